@@ -1,0 +1,57 @@
+// Gotoh scoring under a substitution table on the GPU: scores, recorded decisions, the walk back and
+// the CIGAR, for global and local alignments (reference dinara_align/device_align.mojo,
+// score_groups.mojo, gotoh.mojo).
+#pragma once
+
+#include "internal.cuh"
+
+namespace dinara {
+
+constexpr int kAffineShapes = 5;
+// Lanes a pair and columns a lane of each compiled shape; a pair takes the narrowest shape spanning its
+// columns, the widest in strips of 512 columns (shape 3 is a score-only width: 16 lanes of 20 columns).
+__host__ __device__ inline int affine_lanes(int shape) {
+    return shape == 0 ? 4 : shape == 1 ? 8 : shape == 2 ? 16 : shape == 3 ? 16 : 32;
+}
+__host__ __device__ inline int affine_columns(int shape) { return shape == 3 ? 20 : 16; }
+__host__ __device__ inline int affine_shape_for(uint32_t columns, bool record) {
+    if (columns <= 64) return 0;
+    if (columns <= 128) return 1;
+    if (columns <= 256) return 2;
+    if (!record && columns <= 320) return 3;
+    return 4;
+}
+
+// The substitution table a launch reads, with the gaps in the kernels' terms: `open` a gap's first
+// letter, `extend` each further one (scoring.mojo:202-215 gap_scores).
+struct AffineTable {
+    int32_t size;       // letters in the alphabet
+    int32_t open, extend;
+    int32_t entries[32 * 32];
+    bool packed16;      // size <= 4 and every shifted entry fits 16 bits: the PRMT lookup serves
+};
+
+struct AffineBatch {
+    int64_t pairs;
+    int bits;            // 2 (alphabet of up to 4 letters) or 8 bits a letter on the packed tape
+    bool local;
+    const uint32_t *tape;
+    const PairShape *shapes;
+    uint32_t max_rows, max_columns;
+};
+
+// Scores of a packed batch into `scores` (device): `order` lists the pairs longest first, the classes
+// of affine_shape_for(columns, false) in descending order, `counts[c]` pairs of class c.
+void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
+                   const uint32_t *order, const int64_t counts[kAffineShapes]);
+
+// Alignments of pairs [first_pair, first_pair + count) of a packed batch, ordered as for scores but by
+// affine_shape_for(columns, true): scores into `scores` (indexed by pair), spans (4 per pair of the
+// range: first row, last row, first column, last column of the walk) into `spans`, and each pair's
+// CIGAR: returns the CIGAR bytes' total and leaves their offsets (count + 1, device) in
+// gpu->cigar_offsets and the bytes in gpu->cigar_bytes.
+int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, bool eqx,
+                          int32_t *scores, int64_t *spans, int64_t first_pair, int64_t count, const uint32_t *order,
+                          const int64_t counts[kAffineShapes]);
+
+}  // namespace dinara

@@ -1,0 +1,140 @@
+// Shared definitions of the B200 alignment library: the context, device buffers that grow and are
+// kept between calls, error plumbing from CUDA calls to the C ABI's codes, and the packed pair layout
+// every kernel reads.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "dinara_gpu.h"
+
+namespace dinara {
+
+// A failure carrying one of the C ABI's codes and a message for dinara_gpu_last_error.
+struct Failure : std::runtime_error {
+    int64_t code;
+    Failure(int64_t c, const std::string &message) : std::runtime_error(message), code(c) {}
+};
+
+inline void check_cuda(cudaError_t status, const char *what, const char *file, int line) {
+    if (status != cudaSuccess) {
+        throw Failure(status == cudaErrorMemoryAllocation ? DINARA_OUT_OF_MEMORY : DINARA_DEVICE_FAILURE,
+                      std::string(what) + ": " + cudaGetErrorString(status) + " (" + file + ":" + std::to_string(line) +
+                          ")");
+    }
+}
+
+#define DINARA_CUDA(call) ::dinara::check_cuda((call), #call, __FILE__, __LINE__)
+
+// A device allocation that grows on demand and is reused by later calls.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    template <class T>
+    T *ensure(size_t count) {
+        size_t wanted = count * sizeof(T);
+        if (wanted == 0) wanted = 256;
+        if (wanted > bytes) {
+            if (ptr) cudaFree(ptr);
+            ptr = nullptr;
+            bytes = 0;
+            size_t grown = wanted + wanted / 4;
+            grown = (grown + 255) & ~size_t(255);
+            DINARA_CUDA(cudaMalloc(&ptr, grown));
+            bytes = grown;
+        }
+        return static_cast<T *>(ptr);
+    }
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(ptr);
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Page-locked host memory, so copies run at the bus's rate and asynchronously.
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    template <class T>
+    T *ensure(size_t count) {
+        size_t wanted = count * sizeof(T);
+        if (wanted == 0) wanted = 256;
+        if (wanted > bytes) {
+            if (ptr) cudaFreeHost(ptr);
+            ptr = nullptr;
+            bytes = 0;
+            size_t grown = wanted + wanted / 4;
+            DINARA_CUDA(cudaMallocHost(&ptr, grown));
+            bytes = grown;
+        }
+        return static_cast<T *>(ptr);
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// One pair on the packed tape: each sequence starts on a 16-byte boundary, `letters_per_word` codes a
+// 32-bit word, lowest bits first; rows are the reference's letters, columns the query's.
+struct PairShape {
+    uint32_t first_word;
+    uint32_t rows;
+    uint32_t second_word;
+    uint32_t columns;
+};
+
+// Where a sequence of the ASCII tape lands on the packed tape, in 32-bit words: every sequence takes a
+// 16-byte chunk boundary, and adding one chunk a sequence to its letter offset keeps them apart.
+__host__ __device__ inline uint64_t packed_word_start(int64_t letter_offset, int64_t sequence, int bits) {
+    const int64_t letters_per_chunk = 4 * (32 / bits);
+    return 4ull * uint64_t(letter_offset / letters_per_chunk + sequence);
+}
+
+inline uint64_t packed_words_total(int64_t letters, int64_t sequences, int bits) {
+    const int64_t letters_per_chunk = 4 * (32 / bits);
+    return 4ull * uint64_t(letters / letters_per_chunk + sequences + 2);
+}
+
+}  // namespace dinara
+
+// The context behind the C ABI's opaque handle.
+struct dinara_gpu {
+    int device = 0;
+    int multiprocessors = 0;
+    char name[256] = {0};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    std::string error;
+    // Inputs and their packed form.
+    dinara::DeviceBuffer letters, offsets, code_table, tape, shapes, flags;
+    // Scheduling: bucket keys and the order pairs are taken in.
+    dinara::DeviceBuffer keys, keys_sorted, order, order_sorted, sort_scratch, ranges;
+    // Outputs and per-launch scratch.
+    dinara::DeviceBuffer scores, carry, decisions, decision_offsets, walk_out, cigar_slots, cigar_lengths,
+        cigar_offsets, cigar_bytes, spans;
+    // Unit-cost band state.
+    dinara::DeviceBuffer planes, plane_offsets, thresholds, distances, pending, pending_next, counters, table32;
+    // Learned band predictor.
+    dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations;
+    bool predictor_ready = false;
+    double predictor_margin = 1.25;
+    dinara::PinnedBuffer pinned_in, pinned_out, pinned_small;
+    // Device timing of the sweep kernels, accumulated while `timing` is set.
+    bool timing = false;
+    double kernel_ms = 0.0, record_ms = 0.0;
+    int64_t launches = 0;
+    // The resident batch (capi.cu), if one is loaded.
+    void *resident = nullptr;
+    void (*resident_free)(void *) = nullptr;
+};

@@ -1,0 +1,111 @@
+// Letters to the packed tape on the device: the caller's ASCII tape is copied over as it is and packed
+// here, two bits a letter for an alphabet of up to four letters, else a byte, each sequence from its own
+// 16-byte boundary (the reference packs on host threads into page-locked memory instead,
+// score_groups.mojo:499-537 `packed_into`; its README found that packing dominated its GPU time).
+#include <cub/cub.cuh>
+
+#include "affine.cuh"
+#include "pack.cuh"
+
+namespace dinara {
+
+// A warp a pair: each lane packs 16-byte chunks of the pair's two sequences, translating each byte by
+// `codes` (255 for a byte outside the alphabet, which flags the pair), and writes the pair's shape and
+// its scheduling key (shape class, strips, rows; sorted descending so the longest go first).
+__global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int64_t *__restrict__ offsets,
+                                  int64_t pairs, const uint8_t *__restrict__ codes, int bits,
+                                  uint32_t *__restrict__ tape, PairShape *__restrict__ shapes,
+                                  uint8_t *__restrict__ unknown) {
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= pairs) return;
+    const int per_word = 32 / bits;
+    const int per_chunk = 4 * per_word;
+    const uint32_t mask = bits == 8 ? 0xFFu : ((1u << bits) - 1u);
+    bool bad = false;
+    uint32_t starts[2], lengths[2];
+    for (int side = 0; side < 2; ++side) {
+        const int64_t k = 2 * warp + side;
+        const int64_t start = offsets[k];
+        const int64_t length = offsets[k + 1] - start;
+        const uint64_t word0 = packed_word_start(start, k, bits);
+        starts[side] = uint32_t(word0);
+        lengths[side] = uint32_t(length);
+        const int64_t chunks = (length + per_chunk - 1) / per_chunk;
+        for (int64_t c = lane; c < chunks; c += 32) {
+            uint32_t out[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                uint32_t word = 0;
+                for (int i = 0; i < per_word; ++i) {
+                    const int64_t index = c * per_chunk + w * per_word + i;
+                    if (index < length) {
+                        uint32_t code = codes[letters[start + index]];
+                        if (code == 255u) {
+                            bad = true;
+                            code = 0;
+                        }
+                        word |= (code & mask) << (bits * i);
+                    }
+                }
+                out[w] = word;
+            }
+            *reinterpret_cast<uint4 *>(tape + word0 + 4 * c) = make_uint4(out[0], out[1], out[2], out[3]);
+        }
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+        PairShape shape{starts[0], lengths[0], starts[1], lengths[1]};
+        shapes[warp] = shape;
+        unknown[warp] = bad ? 1 : 0;
+    }
+}
+
+// Scheduling keys of pairs [first, first + count): shape class in the top bits, then strips of its
+// width, then rows, so a descending sort puts each class's longest pairs first and warps hold pairs of
+// like size.
+__global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count, int record,
+                                     uint32_t *__restrict__ keys, uint32_t *__restrict__ order) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const PairShape shape = shapes[first + k];
+    const bool empty = shape.rows == 0 || shape.columns == 0;
+    const int cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);
+    const uint32_t width = uint32_t(affine_lanes(cls) * affine_columns(cls));
+    uint32_t strips = empty ? 0 : (shape.columns + width - 1) / width;
+    if (strips > 255) strips = 255;
+    uint32_t rows = shape.rows >> 2;
+    if (rows > 0xFFFFFu) rows = 0xFFFFFu;
+    keys[k] = (uint32_t(cls) << 28) | (strips << 20) | rows;
+    order[k] = uint32_t(first + k);
+}
+
+void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
+                const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown) {
+    if (pairs <= 0) return;
+    const int threads = 256;
+    const int64_t blocks = (pairs * 32 + threads - 1) / threads;
+    pack_pairs_kernel<<<dim3(unsigned(blocks)), threads, 0, gpu->stream>>>(
+        letters_device, offsets_device, pairs, codes_device, bits, tape, shapes, unknown);
+    DINARA_CUDA(cudaGetLastError());
+}
+
+const uint32_t *schedule(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool record) {
+    uint32_t *keys = gpu->keys.ensure<uint32_t>(count);
+    uint32_t *order = gpu->order.ensure<uint32_t>(count);
+    uint32_t *keys_out = gpu->keys_sorted.ensure<uint32_t>(count);
+    uint32_t *order_out = gpu->order_sorted.ensure<uint32_t>(count);
+    const int threads = 256;
+    schedule_keys_kernel<<<unsigned((count + threads - 1) / threads), threads, 0, gpu->stream>>>(
+        shapes, first, count, record ? 1 : 0, keys, order);
+    DINARA_CUDA(cudaGetLastError());
+    size_t scratch = 0;
+    DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, scratch, keys, keys_out, order, order_out,
+                                                          int(count), 0, 32, gpu->stream));
+    void *space = gpu->sort_scratch.ensure<uint8_t>(scratch);
+    DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(space, scratch, keys, keys_out, order, order_out,
+                                                          int(count), 0, 32, gpu->stream));
+    return order_out;
+}
+
+}  // namespace dinara

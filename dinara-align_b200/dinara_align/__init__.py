@@ -1,0 +1,460 @@
+"""dinara-align's batched alignment path on an NVIDIA B200.
+
+The same Python surface as dinara-align's package (python/dinara_align/__init__.py in the reference) for
+the batched GPU path: `Costs`, `Mode`, `Band`, `Scoring` and `Alignment` with the same fields and
+factories, `distances` and `alignments` with the same signatures, the reference's batch `scores` under a
+`Scoring` (api.mojo:843-892), and a `placement` keyword naming the GPU (api.mojo:1224, :849, :901).
+Everything runs on the GPU through libdinara_gpu.so; a call the GPU path does not serve raises
+ValueError, as the reference's GPU placement does (api.mojo:1240-1246, scoring.mojo:753-757).
+
+>>> import dinara_align as da
+>>> da.distances(["ACGTACGTTTGCA"], ["ACGTCGTTTTGCA"])
+[2]
+>>> da.scores(["ACGTTGCAGGGCATGACGT"], ["ACGTTGCACATGACGT"], da.Scoring.dna())
+[22]
+>>> da.alignments(["ACGTTGCAGGGCATGACGT"], ["ACGTTGCACATGACGT"], da.Scoring.dna())[0].cigar
+'8=3D8='
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, replace
+from typing import Optional, Sequence, Union
+
+import numpy as np
+
+from . import _native as native
+
+__all__ = [
+    "Alignment",
+    "Band",
+    "Costs",
+    "Mode",
+    "Placement",
+    "Scoring",
+    "align",
+    "alignments",
+    "distance",
+    "distances",
+    "score",
+    "scores",
+    "Tape",
+]
+
+UNBOUNDED = 1 << 60
+"""As many free letters as any sequence has, and a band edge past every diagonal (the reference's)."""
+
+Text = Union[str, bytes]
+_ENDS, _EXTENSION, _LOCAL = 0, 1, 2
+
+
+def _text(sequence: Text) -> bytes:
+    """A sequence as ASCII bytes: TypeError unless str or bytes, ValueError unless ASCII."""
+    if isinstance(sequence, (bytes, bytearray)):
+        return bytes(sequence)
+    if not isinstance(sequence, str):
+        raise TypeError(f"a sequence is a str or bytes, not {type(sequence).__name__}")
+    if not sequence.isascii():
+        raise ValueError("a sequence holds ASCII letters alone")
+    return sequence.encode("ascii")
+
+
+def _integers(*values) -> tuple:
+    for value in values:
+        if not isinstance(value, int):
+            raise TypeError(f"an integer, not {type(value).__name__}")
+    return values
+
+
+@dataclass(frozen=True)
+class Costs:
+    """What each edit costs (the reference's `Costs`, fields in `dinara_costs` order). The GPU path
+    measures unit costs, `Costs.edit()`."""
+
+    mismatch: int = 1
+    opening: int = 0
+    extension: int = 1
+    opening2: int = -1
+    extension2: int = 0
+    deletion_opening: int = 0
+    deletion_extension: int = 0
+    deletion_opening2: int = -1
+    deletion_extension2: int = 0
+
+    @staticmethod
+    def edit() -> "Costs":
+        return Costs()
+
+    @staticmethod
+    def linear(mismatch: int, gap: int) -> "Costs":
+        return Costs(mismatch, 0, gap)
+
+    @staticmethod
+    def affine(mismatch: int, opening: int, extension: int) -> "Costs":
+        return Costs(mismatch, opening, extension)
+
+    @staticmethod
+    def two_piece(mismatch: int, opening: int, extension: int, opening2: int, extension2: int) -> "Costs":
+        if _integers(extension2)[0] <= 0 or _integers(opening2)[0] < 0:
+            raise ValueError(f"second piece {opening2}, {extension2}: its extension must cost")
+        return Costs(mismatch, opening, extension, opening2, extension2)
+
+    def unit_scale(self) -> int:
+        """The multiple of the edit distance these costs price every pair at, or 0 if they are not unit
+        costs: a mismatch and a gap letter alike, no opening, one piece (modes.mojo unit_scale)."""
+        one_piece = self.opening2 < 0 and self.deletion_extension == 0
+        if one_piece and self.opening == 0 and self.mismatch == self.extension and self.mismatch > 0:
+            return self.mismatch
+        return 0
+
+
+class Anchor:
+    START = 0
+    END = 1
+
+
+@dataclass(frozen=True)
+class Mode:
+    """Which alignments count (the reference's `Mode`, fields in `dinara_mode` order). The GPU serves
+    `Mode.GLOBAL` and, under a `Scoring`, `Mode.local()`."""
+
+    kind: int = _ENDS
+    reference_start: int = 0
+    reference_end: int = 0
+    query_start: int = 0
+    query_end: int = 0
+    match_score: int = 0
+    anchor: int = Anchor.START
+    zdrop: int = -1
+    end_bonus: int = -1
+
+    GLOBAL = None
+    INFIX = None
+    PREFIX = None
+    SUFFIX = None
+
+    @staticmethod
+    def ends_free(reference_start=0, reference_end=0, query_start=0, query_end=0) -> "Mode":
+        return Mode(_ENDS, reference_start, reference_end, query_start, query_end)
+
+    def with_match_score(self, match_score: int) -> "Mode":
+        return replace(self, match_score=match_score)
+
+    @staticmethod
+    def local(match_score: int = 0) -> "Mode":
+        return Mode(_LOCAL, match_score=match_score)
+
+    def is_global(self) -> bool:
+        return self.kind == _ENDS and not (self.reference_start or self.reference_end or self.query_start
+                                           or self.query_end)
+
+    def _struct(self) -> native.CMode:
+        fields = _integers(self.kind, self.reference_start, self.reference_end, self.query_start, self.query_end,
+                           self.match_score, self.anchor, self.zdrop, self.end_bonus)
+        return native.CMode(*[min(value, UNBOUNDED) for value in fields])
+
+
+Mode.GLOBAL = Mode()
+Mode.INFIX = Mode(_ENDS, UNBOUNDED, UNBOUNDED, 0, 0)
+Mode.PREFIX = Mode(_ENDS, 0, UNBOUNDED, 0, 0)
+Mode.SUFFIX = Mode(_ENDS, UNBOUNDED, 0, 0, 0)
+
+
+@dataclass(frozen=True)
+class Band:
+    low: int = -UNBOUNDED
+    high: int = UNBOUNDED
+
+    @staticmethod
+    def around(width: int) -> "Band":
+        return Band(-width, width)
+
+
+@dataclass(frozen=True)
+class Scoring:
+    """A substitution table over an alphabet, row by row, and a gap of k letters scoring
+    `opening + k * extension` (the reference's `Scoring`)."""
+
+    alphabet: str
+    table: tuple
+    opening: int = -4
+    extension: int = -2
+
+    @staticmethod
+    def dna() -> "Scoring":
+        return Scoring.uniform(2, -4)
+
+    @staticmethod
+    def uniform(match: int, mismatch: int, opening: int = -4, extension: int = -2, alphabet: str = "ACGT") -> "Scoring":
+        size = len(alphabet)
+        table = tuple(match if row == column else mismatch for row in range(size) for column in range(size))
+        return Scoring(alphabet, table, opening, extension)
+
+    @staticmethod
+    def tabulated(alphabet: str, table: Sequence[int], opening: int = -4, extension: int = -2) -> "Scoring":
+        return Scoring(alphabet, tuple(table), opening, extension)
+
+    def _struct(self) -> tuple:
+        if not isinstance(self.alphabet, str) or not self.alphabet.isascii():
+            raise ValueError("an alphabet is a str of ASCII letters")
+        cells = list(_integers(*self.table))
+        if any(cell < -128 or cell > 127 for cell in cells):
+            raise ValueError("a table's cells lie within -128 and 127")
+        size = len(self.alphabet)
+        if len(cells) != size * size:
+            raise ValueError(f"{len(cells)} scores for {size * size} pairs of letters")
+        _integers(self.opening, self.extension)
+        table = np.asarray(cells, dtype=np.int8)
+        alphabet = self.alphabet.encode("ascii")
+        struct = native.CScoring(alphabet, size, native.pointer(table, ctypes.c_int8), self.opening, self.extension)
+        return struct, table, alphabet
+
+
+@dataclass(frozen=True)
+class Alignment:
+    """An alignment of reference[reference_start:reference_end] against query[query_start:query_end] as a
+    CIGAR over those letters ('=' 'X' or 'M', 'D' a reference letter alone, 'I' a query letter alone)."""
+
+    cost: int
+    score: int
+    cigar: str
+    reference_start: int
+    reference_end: int
+    query_start: int
+    query_end: int
+
+    def runs(self) -> list:
+        out, length = [], 0
+        for letter in self.cigar:
+            if letter.isdigit():
+                length = length * 10 + int(letter)
+            else:
+                out.append((length, letter))
+                length = 0
+        return out
+
+    def gapped(self, reference: Text, query: Text) -> tuple:
+        reference, query = _text(reference).decode(), _text(query).decode()
+        top, bottom = [], []
+        column, row = self.reference_start, self.query_start
+        for length, operation in self.runs():
+            if operation == "D":
+                top.append(reference[column:column + length])
+                bottom.append("-" * length)
+                column += length
+            elif operation == "I":
+                top.append("-" * length)
+                bottom.append(query[row:row + length])
+                row += length
+            else:
+                top.append(reference[column:column + length])
+                bottom.append(query[row:row + length])
+                column += length
+                row += length
+        return "".join(top), "".join(bottom)
+
+
+@dataclass(frozen=True)
+class Placement:
+    """Where a batch runs: the GPU `gpu_id` (the reference's `Placement.on_gpu`, common.mojo:130-160)."""
+
+    gpu_id: int = 0
+
+    @staticmethod
+    def on_gpu(gpu_id: int = 0) -> "Placement":
+        return Placement(gpu_id)
+
+
+class Tape:
+    """Pairs laid end to end, the reference's PairTape (scoring.mojo:267-340): pair i's reference is
+    `letters[offsets[2i]:offsets[2i+1]]` and its query `letters[offsets[2i+1]:offsets[2i+2]]`."""
+
+    def __init__(self, letters: np.ndarray, offsets: np.ndarray):
+        self.letters = np.ascontiguousarray(letters, dtype=np.uint8)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        if len(self.letters) == 0:
+            self.letters = np.zeros(1, dtype=np.uint8)
+
+    @property
+    def pairs(self) -> int:
+        return (len(self.offsets) - 1) // 2
+
+    @staticmethod
+    def of(references: Sequence[Text], queries: Sequence[Text]) -> "Tape":
+        if len(references) != len(queries):
+            raise ValueError(f"{len(references)} references against {len(queries)} queries")
+        interleaved = [None] * (2 * len(references))
+        interleaved[0::2] = [_text(item) for item in references]
+        interleaved[1::2] = [_text(item) for item in queries]
+        lengths = np.fromiter((len(item) for item in interleaved), dtype=np.int64, count=len(interleaved))
+        offsets = np.zeros(len(interleaved) + 1, dtype=np.int64)
+        np.cumsum(lengths, out=offsets[1:])
+        letters = np.frombuffer(b"".join(interleaved), dtype=np.uint8)
+        return Tape(letters, offsets)
+
+    def reference(self, pair: int) -> bytes:
+        return self.letters[self.offsets[2 * pair]:self.offsets[2 * pair + 1]].tobytes()
+
+    def query(self, pair: int) -> bytes:
+        return self.letters[self.offsets[2 * pair + 1]:self.offsets[2 * pair + 2]].tobytes()
+
+
+def _placement(placement: Optional[Placement]) -> int:
+    if placement is None:
+        return 0
+    if not isinstance(placement, Placement):
+        raise TypeError("placement: a Placement")
+    return placement.gpu_id
+
+
+def _raise_first(statuses: np.ndarray, what: str) -> None:
+    """Raises the first failing pair's refusal, as a serial loop of single calls would (api.mojo:826-840)."""
+    failed = np.flatnonzero(statuses)
+    if len(failed) == 0:
+        return
+    first = int(failed[0])
+    code = int(statuses[first])
+    if code == native.UNSUPPORTED_SYMBOLS:
+        raise ValueError(f"pair {first}: a letter outside the {what}")
+    if code == native.INVALID_COSTS:
+        raise ValueError(f"pair {first}: scores past 32 bits")
+    raise ValueError(f"pair {first}: code {code}")
+
+
+def scores_tape(tape: Tape, scoring: Scoring, mode: Mode = Mode.GLOBAL, *, placement=None,
+                statuses: bool = False):
+    """Every pair's best score, global or local, on the GPU: an int32 array (and the per-pair statuses)."""
+    handle = native.context(_placement(placement))
+    struct, _table, _alphabet = scoring._struct()
+    mode_struct = mode._struct()
+    pairs = tape.pairs
+    out = np.zeros(max(pairs, 1), dtype=np.int32)
+    codes = np.zeros(max(pairs, 1), dtype=np.int64)
+    code = native.lib().dinara_gpu_scores_tape(handle, pairs, tape.letters.ctypes.data,
+                                                native.pointer(tape.offsets, ctypes.c_int64), ctypes.byref(struct),
+                                                ctypes.byref(mode_struct), native.pointer(out, ctypes.c_int32),
+                                                native.pointer(codes, ctypes.c_int64))
+    native.check(code, handle)
+    if statuses:
+        return out[:pairs], codes[:pairs]
+    _raise_first(codes[:pairs], "Scoring's alphabet")
+    return out[:pairs]
+
+
+def scores(references: Sequence[Text], queries: Sequence[Text], scoring: Scoring, mode: Mode = Mode.GLOBAL, *,
+           placement: Optional[Placement] = None) -> list:
+    """`score` for every pair under `scoring`, globally or locally (api.mojo:843-892)."""
+    return [int(value) for value in scores_tape(Tape.of(references, queries), scoring, mode, placement=placement)]
+
+
+def alignments_tape(tape: Tape, scoring: Scoring, mode: Mode = Mode.GLOBAL, *, eqx: bool = True, placement=None):
+    """Every pair's alignment under `scoring` on the GPU, as arrays: (scores, spans[pairs, 4], cigar
+    offsets, cigar bytes, statuses)."""
+    handle = native.context(_placement(placement))
+    struct, _table, _alphabet = scoring._struct()
+    mode_struct = mode._struct()
+    pairs = tape.pairs
+    out = np.zeros(max(pairs, 1), dtype=np.int32)
+    spans = np.zeros((max(pairs, 1), 4), dtype=np.int64)
+    offsets = np.zeros(pairs + 1, dtype=np.int64)
+    codes = np.zeros(max(pairs, 1), dtype=np.int64)
+    buffer = ctypes.c_void_p()
+    code = native.lib().dinara_gpu_alignments_tape(handle, pairs, tape.letters.ctypes.data,
+                                                    native.pointer(tape.offsets, ctypes.c_int64),
+                                                    ctypes.byref(struct), ctypes.byref(mode_struct), 1 if eqx else 0,
+                                                    native.pointer(out, ctypes.c_int32),
+                                                    native.pointer(spans, ctypes.c_int64),
+                                                    native.pointer(offsets, ctypes.c_int64), ctypes.byref(buffer),
+                                                    native.pointer(codes, ctypes.c_int64))
+    native.check(code, handle)
+    try:
+        total = int(offsets[pairs]) if pairs else 0
+        data = ctypes.string_at(buffer.value, total) if total else b""
+    finally:
+        if buffer.value:
+            native.lib().dinara_free(buffer.value)
+    return out[:pairs], spans[:pairs], offsets, data, codes[:pairs]
+
+
+def alignments(references: Sequence[Text], queries: Sequence[Text], costs: Union[Costs, Scoring] = Costs(),
+               mode: Mode = Mode.GLOBAL, *, band: Optional[Band] = None, max_cost: Optional[int] = None,
+               ties: str = "left", eqx: bool = True, max_memory: Optional[int] = None, threads: int = 0,
+               placement: Optional[Placement] = None) -> list:
+    """Every pair's alignment (the reference's `alignments` signature). On the GPU under a `Scoring`,
+    Gotoh's walk picks among equal alignments, as the reference's device path does (api.mojo:895-1006)."""
+    if not isinstance(costs, Scoring):
+        raise ValueError("on the GPU, alignments under a Scoring")
+    if ties not in ("left", "right"):
+        raise ValueError("ties: 'left' or 'right'")
+    if band is not None or max_cost is not None:
+        raise ValueError("a Scoring takes no band or cap")
+    tape = Tape.of(references, queries)
+    found, spans, offsets, data, codes = alignments_tape(tape, costs, mode, eqx=eqx, placement=placement)
+    _raise_first(codes, "Scoring's alphabet")
+    out = []
+    for pair in range(tape.pairs):
+        cigar = data[offsets[pair]:offsets[pair + 1]].decode("ascii")
+        value = int(found[pair])
+        span = spans[pair]
+        out.append(Alignment(-value, value, cigar, int(span[0]), int(span[1]), int(span[2]), int(span[3])))
+    return out
+
+
+def distances_tape(tape: Tape, *, policy: int = native.BAND_PLAIN, start_thresholds=None, default_start: int = 0,
+                   placement=None, report: bool = False):
+    """Every pair's unit-cost global edit distance by band doubling on the GPU (int64 array; negative
+    entries are the pair's own code), with the band report when asked."""
+    handle = native.context(_placement(placement))
+    pairs = tape.pairs
+    out = np.zeros(max(pairs, 1), dtype=np.int64)
+    plan = native.CBandPlan(policy, None, default_start)
+    starts = None
+    if start_thresholds is not None:
+        starts = np.ascontiguousarray(start_thresholds, dtype=np.int64)
+        plan.start_thresholds = native.pointer(starts, ctypes.c_int64)
+    summary = native.CBandReport()
+    code = native.lib().dinara_gpu_distances_tape(handle, pairs, tape.letters.ctypes.data,
+                                                   native.pointer(tape.offsets, ctypes.c_int64), ctypes.byref(plan),
+                                                   native.pointer(out, ctypes.c_int64), ctypes.byref(summary))
+    native.check(code, handle)
+    if report:
+        return out[:pairs], {name: getattr(summary, name) for name, _ in native.CBandReport._fields_}
+    return out[:pairs]
+
+
+def distances(references: Sequence[Text], queries: Sequence[Text], costs: Costs = Costs(), mode: Mode = Mode.GLOBAL,
+              *, band: Optional[Band] = None, max_cost: Optional[int] = None, threads: int = 0,
+              placement: Optional[Placement] = None) -> list:
+    """Every pair's least cost (the reference's `distances` signature): on the GPU, unit costs
+    globally with no band or cap, as the reference's GPU placement requires (api.mojo:1237-1247)."""
+    if mode.match_score > 0:
+        raise ValueError("a mode with a match score maximizes a score, which `align` finds")
+    scale = costs.unit_scale()
+    if scale == 0 or not mode.is_global() or (band is not None and (band.low > -UNBOUNDED or band.high < UNBOUNDED)):
+        raise ValueError("on the GPU, distances at unit costs, globally, with no band")
+    if max_cost is not None:
+        raise ValueError("on the GPU, distances with no cap")
+    _integers(threads)
+    found = distances_tape(Tape.of(references, queries), placement=placement)
+    if (found < 0).any():
+        first = int(np.flatnonzero(found < 0)[0])
+        raise ValueError(f"pair {first}: a 0xFE or 0xFF byte")
+    return [int(value) * scale for value in found]
+
+
+def distance(reference: Text, query: Text, costs: Costs = Costs(), mode: Mode = Mode.GLOBAL, *, band=None,
+             max_cost=None, placement=None) -> Optional[int]:
+    return distances([reference], [query], costs, mode, band=band, max_cost=max_cost, placement=placement)[0]
+
+
+def score(reference: Text, query: Text, costs: Union[Costs, Scoring], mode: Mode = Mode.GLOBAL, *,
+          placement=None) -> int:
+    if not isinstance(costs, Scoring):
+        raise ValueError("on the GPU, scores under a Scoring")
+    return scores([reference], [query], costs, mode, placement=placement)[0]
+
+
+def align(reference: Text, query: Text, costs: Union[Costs, Scoring], mode: Mode = Mode.GLOBAL, *, eqx=True,
+          placement=None) -> Alignment:
+    return alignments([reference], [query], costs, mode, eqx=eqx, placement=placement)[0]

@@ -1,0 +1,210 @@
+/*
+ * dinara-align's batched alignment path on an NVIDIA B200 (sm_100a), as a C ABI.
+ *
+ * The library scores, aligns and measures batches of pairs on one GPU: global and local Gotoh
+ * scores and CIGARs under a substitution table (a `Scoring`), and global unit-cost edit distances
+ * by banded bit-vectors with band doubling, plain or started from a learned prediction. Every
+ * result is exact: the same integers, and under a `Scoring` the same CIGAR, as dinara-align's own
+ * implementation gives.
+ *
+ * The pair order, the reading of sequences (the first of each pair the reference, read down the
+ * rows; the second the query, across the columns; `D` a reference letter alone, `I` a query letter
+ * alone) and the error codes are dinara-align's (c/dinara.h in the reference). Functions take plain
+ * host pointers; a context (`dinara_gpu`) holds one device's streams and the device buffers it
+ * keeps between calls, and is used by one thread at a time.
+ */
+#ifndef DINARA_GPU_H
+#define DINARA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Codes shared with the reference's C ABI (c/dinara.h:35-49). */
+#define DINARA_UNSUPPORTED_SYMBOLS (-1) /* a letter outside the alphabet (or 0xFE/0xFF at unit cost) */
+#define DINARA_OUT_OF_MEMORY (-2)       /* device or host memory could not be had */
+#define DINARA_INVALID_COSTS (-3)       /* a Scoring or costs that cannot be searched, or scores past 2^28 */
+#define DINARA_ABOVE_MAX (-4)
+#define DINARA_OUTSIDE_BAND (-5)
+#define DINARA_INVALID_MODE (-6)        /* a mode or argument this entry point does not serve */
+#define DINARA_INVALID_LENGTH (-7)      /* a negative length, or lists of different lengths */
+/* GPU additions, distinct from the reference's codes. */
+#define DINARA_DEVICE_FAILURE (-8)      /* a CUDA call failed; dinara_gpu_error() says which */
+#define DINARA_DEVICE_TIMEOUT (-9)      /* a bounded wait (device flag or host wait) ran out */
+
+/* dinara_mode kinds (c/dinara.h:69-76); the GPU serves ENDS_FREE with no free ends (global) and LOCAL. */
+#define DINARA_ENDS_FREE 0
+#define DINARA_EXTENSION 1
+#define DINARA_LOCAL 2
+
+/* The reference's structs, field for field (c/dinara.h:59-138). */
+typedef struct {
+    int64_t mismatch, opening, extension, opening2, extension2;
+    int64_t deletion_opening, deletion_extension, deletion_opening2, deletion_extension2;
+} dinara_costs;
+
+typedef struct {
+    int64_t kind, reference_start, reference_end, query_start, query_end;
+    int64_t match_score, anchor, zdrop, end_bonus;
+} dinara_mode;
+
+typedef struct {
+    int64_t band_low, band_high, max_cost, eqx, right_ties, max_memory;
+} dinara_options;
+
+typedef struct {
+    int64_t cost, score, reference_start, reference_end, query_start, query_end;
+    char *cigar;
+    int64_t cigar_length;
+} dinara_alignment;
+
+/*
+ * A Scoring (reference dinara_align/scoring.mojo:127-215; python Scoring, __init__.py:264-299): an
+ * alphabet of 1 to 32 ASCII letters, its `alphabet_size` x `alphabet_size` table row by row, and a gap
+ * of k letters scoring `opening + k * extension`, both zero or less.
+ */
+typedef struct {
+    const char *alphabet;
+    int64_t alphabet_size;
+    const int8_t *table;
+    int64_t opening;
+    int64_t extension;
+} dinara_scoring;
+
+/* One device's context: streams, kernels' device buffers kept between calls, and the learned band
+ * predictor. Null when the device cannot be opened; `dinara_gpu_last_error` says why. */
+typedef struct dinara_gpu dinara_gpu;
+
+dinara_gpu *dinara_gpu_new(int64_t device);
+void dinara_gpu_free(dinara_gpu *gpu);
+/* The last failure's message on this context (or, for a null context, the last dinara_gpu_new's). */
+const char *dinara_gpu_last_error(const dinara_gpu *gpu);
+/* The device's name and SM count, for reports. */
+int64_t dinara_gpu_device_info(dinara_gpu *gpu, char *name, int64_t name_capacity, int64_t *multiprocessors);
+
+/*
+ * Scores under a Scoring, global or local (replaces the reference's device batch
+ * dinara_align/api.mojo:843-892 `scores` -> scoring.mojo:1294-1409 `device_batch_scores`).
+ * Pair i is references[i] (reference_lengths[i] bytes) against queries[i]. Writes scores[i] and
+ * statuses[i] (0, or the pair's own code: -1 a letter outside the alphabet, -3 scores that could pass
+ * 2^28 as ScoreReach refuses, scoring.mojo:218-249). Returns 0, or a code failing the whole batch
+ * (a bad Scoring or mode), and then writes nothing.
+ */
+int64_t dinara_gpu_scores(dinara_gpu *gpu, int64_t pairs, const char *const *references,
+                          const int64_t *reference_lengths, const char *const *queries, const int64_t *query_lengths,
+                          const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, int64_t *statuses);
+
+/* The same over one tape: pair i's reference is letters[offsets[2i] .. offsets[2i+1]) and its query
+ * letters[offsets[2i+1] .. offsets[2i+2]), the reference's PairTape (scoring.mojo:267-340). */
+int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                               const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores,
+                               int64_t *statuses);
+
+/*
+ * Alignments under a Scoring, global or local, the CIGAR Gotoh's walk picks among equals (replaces
+ * api.mojo:895-1006 `alignments` on the GPU -> scoring.mojo:1436-1478 `device_batch_alignments` ->
+ * device_align.mojo:278-441 `batch_kernel[record]`, and the reference's c/dinara.h:225-228 batch
+ * shape). Each alignment's CIGAR is allocated here and freed with dinara_free; its spans are placed
+ * as scoring.mojo:724-744 `as_alignment` places them. `eqx` nonzero writes '='/'X', else 'M'.
+ */
+int64_t dinara_gpu_alignments(dinara_gpu *gpu, int64_t pairs, const char *const *references,
+                              const int64_t *reference_lengths, const char *const *queries,
+                              const int64_t *query_lengths, const dinara_scoring *scoring, const dinara_mode *mode,
+                              int64_t eqx, dinara_alignment *alignments, int64_t *statuses);
+
+/*
+ * Alignments over one tape with every CIGAR in one buffer: pair i's CIGAR is
+ * cigar_bytes[cigar_offsets[i] .. cigar_offsets[i+1]) (no NULs), its score scores[i], its spans
+ * spans[4i .. 4i+4) = reference_start, reference_end, query_start, query_end. `*cigar_bytes` is
+ * allocated here (dinara_free). Same walk and placement as dinara_gpu_alignments.
+ */
+int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                   const dinara_scoring *scoring, const dinara_mode *mode, int64_t eqx,
+                                   int32_t *scores, int64_t *spans, int64_t *cigar_offsets, char **cigar_bytes,
+                                   int64_t *statuses);
+
+/* Frees a CIGAR or a CIGAR buffer this library allocated (c/dinara.h:207 dinara_free); null is nothing. */
+void dinara_free(char *cigar);
+
+/*
+ * Unit-cost global edit distances (replaces api.mojo:1216-1312 `distances(placement=on_gpu)` ->
+ * `gpu_distances` -> device_edit.mojo:80-173, and the reference's CPU band doubling,
+ * band.mojo:526-657, which its GPU path lacks). Costs must be unit (null, or {1,0,1,-1,0,...}), the
+ * mode global and the options without band or cap, as the reference's GPU placement requires
+ * (api.mojo:1240-1246); otherwise the batch fails with DINARA_INVALID_MODE. Every byte matches only
+ * itself; 0xFE and 0xFF are refused per pair (-1). results[i] is the distance or the pair's code.
+ */
+int64_t dinara_gpu_distances(dinara_gpu *gpu, int64_t pairs, const char *const *references,
+                             const int64_t *reference_lengths, const char *const *queries, const int64_t *query_lengths,
+                             const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options,
+                             int64_t *results);
+
+/* How a band-doubling batch chooses each pair's first threshold. */
+#define DINARA_BAND_PLAIN 0   /* the default: the length difference plus 256 (band.mojo:521 DOUBLING_START) */
+#define DINARA_BAND_LEARNED 1 /* the context's trained predictor's cost, with its margin */
+#define DINARA_BAND_GIVEN 2   /* thresholds the caller gives in `start_thresholds` */
+
+typedef struct {
+    int64_t policy;                  /* DINARA_BAND_PLAIN / _LEARNED / _GIVEN */
+    const int64_t *start_thresholds; /* DINARA_BAND_GIVEN: one per pair */
+    int64_t default_start;           /* added to the length difference for PLAIN; 0 for 256 */
+} dinara_band_plan;
+
+typedef struct {
+    int64_t rounds;          /* launches of the band kernels (all pairs, all rounds) */
+    int64_t pair_rounds;     /* summed over pairs: rounds each took */
+    int64_t words_swept;     /* 64-cell words updated, all rounds (the band cells actually swept / 64) */
+    int64_t full_cells;      /* sum of |A| * |B| (GCUPS denominator) */
+    int64_t first_round_hits;/* pairs settled by their first threshold */
+    int64_t overshoot;       /* pairs whose first threshold was at least twice their distance */
+    int64_t undershoot;      /* pairs whose first threshold was below their distance */
+    double kernel_ms;        /* device time of the band kernels */
+} dinara_band_report;
+
+/* Distances over one tape by band doubling from the plan's first thresholds; `report` may be null. */
+int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                  const dinara_band_plan *plan, int64_t *results, dinara_band_report *report);
+
+/*
+ * Resident batches (no reference counterpart; the reference re-creates its device scope, uploads and
+ * frees on every call, scoring.mojo:1342-1409): a batch's letters uploaded and packed once and kept on
+ * the device, so later calls run the device path alone. One resident batch a context.
+ */
+typedef struct {
+    double total_ms;       /* device time of the whole call, first launch to last */
+    double kernel_ms;      /* device time of the sweep kernels (scores or band rounds) */
+    double record_ms;      /* device time of the recording sweep and walk (alignments) */
+    int64_t launches;      /* kernels this library launched in the call */
+    int64_t cells;         /* matrix cells the sweeps updated */
+} dinara_timing;
+
+/* Uploads and packs `pairs` pairs for a Scoring (or, with `scoring` null, as bytes for unit-cost
+ * distances) and keeps them. Returns 0 or a code; per-pair refusals come back from the runs. */
+int64_t dinara_gpu_resident_load(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                 const dinara_scoring *scoring);
+
+/* Scores (and with `cigars` nonzero the alignments' CIGARs) of the resident batch, results left on the
+ * device until dinara_gpu_resident_fetch. */
+int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int64_t cigars, int64_t eqx,
+                                  dinara_timing *timing);
+
+/* Distances of the resident (unit-cost) batch by band doubling. */
+int64_t dinara_gpu_resident_distances(dinara_gpu *gpu, const dinara_band_plan *plan, dinara_band_report *report,
+                                      dinara_timing *timing);
+
+/* Copies the last resident run's results to the host: `scores` (int32, per pair) for a scoring run or
+ * `distances` (int64) for a distance run; either may be null. */
+int64_t dinara_gpu_resident_fetch(dinara_gpu *gpu, int32_t *scores, int64_t *distances);
+
+/* The device's measured integer issue rate (no reference counterpart: the roofline the sweeps are
+ * judged against): `kind` 0 DPX add-and-max, 1 min/max with an add, 2 three-input add; instructions
+ * per second into *instructions_per_second, from independent chains on every SM. */
+int64_t dinara_gpu_int32_peak(dinara_gpu *gpu, int64_t kind, double *instructions_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,169 @@
+"""Gotoh scores and CIGARs on the GPU against the CPU oracle, bit for bit (the reference's
+tests/test_alignment.mojo:3715-3990 device tests compare scores with the host; here the CIGAR is the
+full-matrix walk's, as the reference's device walk gives it)."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _scoring(da, entry):
+    return da.Scoring(entry["alphabet"], tuple(entry["table"]), entry["opening"], entry["extension"])
+
+
+def _oracle_batch(oracle, da, tape, scoring, local, aligned):
+    size = len(scoring.alphabet)
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    codes = np.full(256, 255, dtype=np.uint8)
+    for k, letter in enumerate(scoring.alphabet.encode()):
+        codes[letter] = k
+    coded = codes[tape.letters[: tape.offsets[-1]]] if tape.offsets[-1] else np.zeros(1, np.uint8)
+    mode = oracle.LOCAL if local else oracle.GLOBAL
+    if aligned:
+        return oracle.batch_alignments(coded, tape.offsets, table, size, op, ex, mode, threads=8)
+    return oracle.batch_scores(coded, tape.offsets, table, size, op, ex, mode, threads=8)
+
+
+def test_known_answers(da):
+    known = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
+    for entry in known:
+        if entry["kind"] != "score":
+            continue
+        scoring = _scoring(da, entry["scoring"])
+        mode = da.Mode.local() if entry["mode"] == "local" else da.Mode.GLOBAL
+        assert da.scores([entry["reference"]], [entry["query"]], scoring, mode) == [entry["score"]], entry
+        found = da.alignments([entry["reference"]], [entry["query"]], scoring, mode)[0]
+        assert found.score == entry["score"], entry
+        if "cigar" in entry:
+            assert found.cigar == entry["cigar"], entry
+        if "reference_start" in entry:
+            assert found.reference_start == entry["reference_start"]
+        if "query_end" in entry:
+            assert found.query_end == entry["query_end"]
+        if "cigar_m" in entry:
+            assert da.alignments([entry["reference"]], [entry["query"]], scoring, mode, eqx=False)[0].cigar == entry[
+                "cigar_m"]
+
+
+def test_random_fixtures(da):
+    data = json.load(open(os.path.join(GOLDEN, "random_pairs.json")))["pairs"]
+    known = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
+    dna = _scoring(da, known[0]["scoring"])
+    config2 = _scoring(da, known[8]["scoring"])
+    refs = [entry["reference"] for entry in data]
+    queries = [entry["query"] for entry in data]
+    for name, scoring in (("dna", dna), ("config2", config2)):
+        assert da.scores(refs, queries, scoring) == [entry[name]["global"] for entry in data]
+        assert da.scores(refs, queries, scoring, da.Mode.local()) == [entry[name]["local"] for entry in data]
+        found = da.alignments(refs, queries, scoring)
+        assert [a.cigar for a in found] == [entry[name]["global_cigar"] for entry in data]
+        local = da.alignments(refs, queries, scoring, da.Mode.local())
+        assert [a.cigar for a in local] == [entry[name]["local_cigar"] for entry in data]
+        assert [a.score for a in local] == [entry[name]["local"] for entry in data]
+
+
+@pytest.mark.parametrize("local", [False, True])
+def test_synthetic_scores_and_cigars(da, oracle, local):
+    """Config-2-shaped pairs (100-300 bp, 5% errors), scores and CIGARs against the oracle."""
+    from dinara_align import workloads
+
+    tape = workloads.affine_global(3000, seed=21)
+    scoring = da.Scoring.uniform(0, -4, -6, -2)
+    mode = da.Mode.local() if local else da.Mode.GLOBAL
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, scoring, local, True)
+    got = da.scores_tape(tape, scoring, mode)
+    np.testing.assert_array_equal(got, expected_scores)
+    scores, spans, offsets, data, codes = da.alignments_tape(tape, scoring, mode)
+    np.testing.assert_array_equal(scores, expected_scores)
+    assert not codes.any()
+    cigars = [data[offsets[p]:offsets[p + 1]].decode() for p in range(tape.pairs)]
+    assert cigars == expected_cigars
+
+
+@pytest.mark.parametrize("local", [False, True])
+def test_shapes_and_strips(da, oracle, local):
+    """Every shape class and multi-strip pairs: widths 1..1500 columns, tall and flat pairs, empties."""
+    rng = np.random.default_rng(8)
+    widths = [0, 1, 2, 15, 16, 17, 63, 64, 65, 127, 128, 129, 255, 256, 257, 319, 320, 321, 511, 512, 513, 700, 1025,
+              1500]
+    refs, queries = [], []
+    for w in widths:
+        for h in (0, 1, 3, 40, 333, 1200):
+            refs.append("".join(rng.choice(list("ACGT"), size=h)))
+            queries.append("".join(rng.choice(list("ACGT"), size=w)))
+    scoring = da.Scoring.dna()
+    mode = da.Mode.local() if local else da.Mode.GLOBAL
+    tape = da.Tape.of(refs, queries)
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, scoring, local, True)
+    assert da.scores(refs, queries, scoring, mode) == list(expected_scores)
+    found = da.alignments(refs, queries, scoring, mode)
+    assert [a.cigar for a in found] == expected_cigars
+    assert [a.score for a in found] == list(expected_scores)
+
+
+def test_local_spans_placed_as_reference(da, oracle):
+    """Local spans by as_alignment's rule (scoring.mojo:724-744): the aligned letters' last place."""
+    refs = ["GGGGACGTACGTGGGG", "ACGTTTTTACGT" * 3, "TTTTACGTACGTTTTT"]
+    queries = ["CCCCACGTTCGTCC", "ACGT", "ACGTACGT"]
+    found = da.alignments(refs, queries, da.Scoring.dna(), da.Mode.local())
+    for a, ref, query in zip(found, refs, queries):
+        top, bottom = a.gapped(ref, query)
+        letters_r = top.replace("-", "")
+        letters_q = bottom.replace("-", "")
+        assert a.reference_start == (ref.rfind(letters_r) if letters_r else 0)
+        assert a.query_start == (query.rfind(letters_q) if letters_q else 0)
+        assert ref[a.reference_start:a.reference_end] == letters_r
+    assert (found[0].cigar, found[0].reference_start) == ("4=1X3=", 4)
+
+
+def test_tables_beyond_four_letters(da, oracle):
+    """A 20-letter table (the shared-memory path) and a table whose shifted entries pass 16 bits."""
+    rng = np.random.default_rng(9)
+    alphabet = "ACDEFGHIKLMNPQRSTVWY"
+    table = tuple(int(v) for v in rng.integers(-6, 8, size=400))
+    protein = da.Scoring.tabulated(alphabet, table, -10, -1)
+    refs = ["".join(rng.choice(list(alphabet), size=rng.integers(0, 600))) for _ in range(80)]
+    queries = ["".join(rng.choice(list(alphabet), size=rng.integers(0, 600))) for _ in range(80)]
+    tape = da.Tape.of(refs, queries)
+    for local in (False, True):
+        mode = da.Mode.local() if local else da.Mode.GLOBAL
+        expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, protein, local, True)
+        assert da.scores(refs, queries, protein, mode) == list(expected_scores)
+        assert [a.cigar for a in da.alignments(refs, queries, protein, mode)] == expected_cigars
+    wide = da.Scoring.uniform(5, -3, -100, -20000)
+    dna_refs = ["".join(rng.choice(list("ACGT"), size=rng.integers(1, 40))) for _ in range(30)]
+    dna_queries = ["".join(rng.choice(list("ACGT"), size=rng.integers(1, 40))) for _ in range(30)]
+    tape = da.Tape.of(dna_refs, dna_queries)
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, wide, False, True)
+    assert da.scores(dna_refs, dna_queries, wide) == list(expected_scores)
+    assert [a.cigar for a in da.alignments(dna_refs, dna_queries, wide)] == expected_cigars
+
+
+def test_refusals(da):
+    """What the reference refuses: letters outside the alphabet (per pair), scores past 2^28, bad
+    Scorings and modes (the whole batch)."""
+    scoring = da.Scoring.dna()
+    scores, statuses = da.scores_tape(da.Tape.of(["ACGT", "ACNT", "A"], ["ACGT", "ACGT", "A"]), scoring,
+                                      statuses=True)
+    assert list(statuses) == [0, -1, 0]
+    assert scores[0] == 8 and scores[2] == 2
+    with pytest.raises(ValueError):
+        da.scores(["ACNT"], ["ACGT"], scoring)
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACGT"], da.Scoring.uniform(2, -4, 3, -2))  # a gap that earns
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACGT"], da.Scoring("AC-T", tuple([1] * 16)))
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.INFIX)
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.local(2))
+    huge = da.Scoring.uniform(2, -4, -4, -100000)
+    _, statuses = da.scores_tape(da.Tape.of(["A" * 3000], ["A" * 3000]), huge, statuses=True)
+    assert list(statuses) == [-3]

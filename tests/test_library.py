@@ -1,0 +1,51 @@
+"""The C-ABI library on the CPU: it loads without a GPU and exports every function include/*.h declares
+(no compute call is made here)."""
+
+import ctypes
+import glob
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBRARY = os.path.join(ROOT, "dinara-align_b200", "dinara_align", "libdinara_gpu.so")
+
+
+def declared_functions():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for match in re.finditer(r"^[A-Za-z_][\w \*]*?\b(dinara_\w+)\s*\(", text, flags=re.M):
+            names.add(match.group(1))
+    return names
+
+
+def test_library_exports_every_declared_function():
+    assert os.path.exists(LIBRARY), "build the library first (make -C dinara-align_b200)"
+    handle = ctypes.CDLL(LIBRARY)
+    names = declared_functions()
+    assert len(names) >= 10
+    missing = [name for name in sorted(names) if not hasattr(handle, name)]
+    assert not missing, missing
+
+
+def test_null_context_is_refused():
+    """A call without a context fails with a code, not a crash, and touches no device."""
+    handle = ctypes.CDLL(LIBRARY)
+    handle.dinara_gpu_scores_tape.restype = ctypes.c_int64
+    code = handle.dinara_gpu_scores_tape(None, 0, None, None, None, None, None, None)
+    assert code == -6
+    handle.dinara_free.restype = None
+    handle.dinara_free(None)
+
+
+def test_python_package_imports_without_gpu():
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "dinara-align_b200"))
+    import dinara_align
+
+    assert dinara_align.Scoring.dna().table[0] == 2
+    assert dinara_align.Tape.of(["AC"], ["G"]).pairs == 1
+    assert dinara_align.Costs.edit().unit_scale() == 1
+    assert dinara_align.Costs.affine(4, 6, 2).unit_scale() == 0

@@ -1,0 +1,204 @@
+"""The CPU oracle pinned against the reference's own known answers, and its formulations against each
+other: the Gotoh walk by exhaustive enumeration on tiny pairs (the reference's
+tests/test_alignment.mojo:93-243 strategy), the unit-cost distance by a plain dynamic program, Myers'
+bit-vectors and band doubling."""
+
+import itertools
+import json
+import os
+import random
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _scoring(entry):
+    table = np.asarray(entry["table"], dtype=np.int8)
+    return table, len(entry["alphabet"]), entry["opening"] + entry["extension"], entry["extension"]
+
+
+def test_known_answers(oracle):
+    """Every known answer the reference's tests give for this path (tests/golden/known_answers.json)."""
+    known = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
+    assert len(known) >= 15
+    for entry in known:
+        a, b = entry["reference"], entry["query"]
+        if entry["kind"] == "distance":
+            assert oracle.edit_distance_dp(a, b) == entry["distance"], entry
+            assert oracle.myers_distance(a, b) == entry["distance"], entry
+            assert oracle.band_doubling(a, b, 0)[0] == entry["distance"], entry
+            continue
+        table, size, op, ex = _scoring(entry["scoring"])
+        mode = oracle.LOCAL if entry["mode"] == "local" else oracle.GLOBAL
+        ca, cb = oracle.codes(a, entry["scoring"]["alphabet"]), oracle.codes(b, entry["scoring"]["alphabet"])
+        score, _, _ = oracle.gotoh_score(ca, cb, table, size, op, ex, mode)
+        assert score == entry["score"], entry
+        aligned, cigar, top, bottom = oracle.gotoh_align(ca, cb, table, size, op, ex, mode)
+        assert aligned == entry["score"], entry
+        if "cigar" in entry:
+            assert cigar == entry["cigar"], entry
+        if "cigar_m" in entry:
+            assert oracle.gotoh_align(ca, cb, table, size, op, ex, mode, eqx=False)[1] == entry["cigar_m"]
+
+
+def _enumerate_best(a, b, table, size, op, ex, local):
+    """The best score of every alignment of two tiny sequences, by listing them all."""
+    best = None
+
+    def rescore(path):
+        total, i, j, run, layer = 0, 0, 0, 0, None
+        for move in path:
+            if move == "M":
+                total += int(table[a[i] * size + b[j]])
+                i, j, layer = i + 1, j + 1, None
+            else:
+                total += ex if layer == move else op
+                layer = move
+                if move == "D":
+                    i += 1
+                else:
+                    j += 1
+        return total
+
+    def walks(i, j):
+        if i == len(a) and j == len(b):
+            yield []
+            return
+        if i < len(a) and j < len(b):
+            for rest in walks(i + 1, j + 1):
+                yield ["M"] + rest
+        if i < len(a):
+            for rest in walks(i + 1, j):
+                yield ["D"] + rest
+        if j < len(b):
+            for rest in walks(i, j + 1):
+                yield ["I"] + rest
+
+    if not local:
+        return max(rescore(path) for path in walks(0, 0))
+    best = 0
+    for i0 in range(len(a) + 1):
+        for i1 in range(i0, len(a) + 1):
+            for j0 in range(len(b) + 1):
+                for j1 in range(j0, len(b) + 1):
+                    sub_a, sub_b = a[i0:i1], b[j0:j1]
+                    value = _enumerate_best(sub_a, sub_b, table, size, op, ex, False) if (sub_a or sub_b) else 0
+                    best = max(best, value)
+    return best
+
+
+def test_gotoh_against_enumeration(oracle):
+    """Every pair over a two-letter alphabet with combined length at most five, global and local."""
+    table = np.array([3, -2, -2, 3], dtype=np.int8)
+    op, ex = oracle.kernel_gaps(-5, -1)
+    words = [()]
+    for n in range(1, 4):
+        words += list(itertools.product((0, 1), repeat=n))
+    for a in words:
+        for b in words:
+            if len(a) + len(b) > 5:
+                continue
+            for local in (False, True):
+                expected = _enumerate_best(list(a), list(b), table, 2, op, ex, local)
+                mode = oracle.LOCAL if local else oracle.GLOBAL
+                got = oracle.gotoh_score(np.array(a, np.uint8), np.array(b, np.uint8), table, 2, op, ex, mode)[0]
+                assert got == expected, (a, b, local)
+
+
+def _rescore_cigar(cigar, a, b, table, size, op, ex, start_a=0, start_b=0):
+    total, i, j = 0, start_a, start_b
+    number = ""
+    for ch in cigar:
+        if ch.isdigit():
+            number += ch
+            continue
+        k = int(number)
+        number = ""
+        if ch in "=XM":
+            for _ in range(k):
+                if ch == "=":
+                    assert a[i] == b[j]
+                if ch == "X":
+                    assert a[i] != b[j]
+                total += int(table[a[i] * size + b[j]])
+                i, j = i + 1, j + 1
+        elif ch == "D":
+            total += op + (k - 1) * ex
+            i += k
+        else:
+            total += op + (k - 1) * ex
+            j += k
+    return total, i, j
+
+
+def test_random_fixtures(oracle):
+    """The seeded fixtures: DP distances agree with Myers and band doubling; each fixture CIGAR rebuilds
+    its pair and rescores to its score."""
+    data = json.load(open(os.path.join(GOLDEN, "random_pairs.json")))["pairs"]
+    dna = json.load(open(os.path.join(GOLDEN, "known_answers.json")))[0]["scoring"]
+    table, size, op, ex = _scoring(dna)
+    for entry in data:
+        a, b = entry["reference"], entry["query"]
+        assert oracle.myers_distance(a, b) == entry["distance"]
+        assert oracle.band_doubling(a, b, 0)[0] == entry["distance"]
+        ca, cb = oracle.codes(a), oracle.codes(b)
+        score, cigar, _, _ = oracle.gotoh_align(ca, cb, table, size, op, ex)
+        assert (score, cigar) == (entry["dna"]["global"], entry["dna"]["global_cigar"])
+        total, i, j = _rescore_cigar(cigar, ca, cb, table, size, op, ex)
+        assert (total, i, j) == (score, len(a), len(b))
+
+
+def test_unit_cost_formulations_agree(oracle):
+    """Plain DP, full-matrix Myers (device_edit.mojo's step) and band doubling from several starts, over
+    lengths across word edges (the reference's 0..513 sweep, tests/test_alignment.mojo:560-586)."""
+    rng = random.Random(11)
+    lengths = [0, 1, 2, 63, 64, 65, 127, 128, 129, 255, 256, 257, 511, 512, 513]
+    for n in lengths:
+        for rate in (0.0, 0.05, 0.3):
+            a = "".join(rng.choice("ACGT") for _ in range(n))
+            b = "".join(ch if rng.random() > rate else rng.choice(["", "A", ch + "C"]) for ch in a)
+            if rng.random() < 0.3:
+                b += "".join(rng.choice("ACGT") for _ in range(rng.randrange(0, 70)))
+            d = oracle.edit_distance_dp(a, b)
+            assert oracle.myers_distance(a, b) == d
+            for start in (0, 1, 7, 64, 256):
+                assert oracle.band_doubling(a, b, start)[0] == d
+            for threshold in (0, 3, 40, 300):
+                assert oracle.banded_round(a, b, threshold) >= d
+
+
+def test_bytes_beyond_dna(oracle):
+    """Unit costs take any byte as a letter matching only itself (c/dinara.h:15-17)."""
+    a, b = b"kitten\x01\x7f", b"sitting\x7f"
+    assert oracle.edit_distance_dp(a, b) == oracle.myers_distance(a, b) == oracle.band_doubling(a, b, 0)[0] == 3
+
+
+def test_score_reach(oracle):
+    """ScoreReach (scoring.mojo:218-249) refuses pairs whose scores could pass 2^28."""
+    table = oracle.dna_table(2, -4)
+    op, ex = oracle.kernel_gaps(-4, -2)
+    assert not oracle.score_reach_refuses(table, 4, op, ex, 50_000, 50_000)
+    assert oracle.score_reach_refuses(table, 4, op, ex, 20_000_000, 20_000_000)
+    assert not oracle.score_reach_refuses(table, 4, op, ex, 40_000_000, 10, oracle.LOCAL)
+
+
+def test_batches_match_singles(oracle):
+    """The threaded batch entry points give each pair's single answer."""
+    rng = np.random.default_rng(5)
+    firsts = [rng.integers(0, 4, rng.integers(0, 90)).astype(np.uint8) for _ in range(60)]
+    seconds = [rng.integers(0, 4, rng.integers(0, 90)).astype(np.uint8) for _ in range(60)]
+    tape, offsets = oracle.tape_of(firsts, seconds)
+    table = oracle.dna_table(2, -4)
+    op, ex = oracle.kernel_gaps(-4, -2)
+    for mode in (oracle.GLOBAL, oracle.LOCAL):
+        scores = oracle.batch_scores(tape, offsets, table, 4, op, ex, mode, threads=4)
+        aligned, cigars = oracle.batch_alignments(tape, offsets, table, 4, op, ex, mode, threads=3)
+        for k, (a, b) in enumerate(zip(firsts, seconds)):
+            single = oracle.gotoh_align(a, b, table, 4, op, ex, mode)
+            assert scores[k] == single[0] == aligned[k]
+            assert cigars[k] == single[1]
+    distances = oracle.batch_distances(tape, offsets, start=0, threads=4)
+    for k, (a, b) in enumerate(zip(firsts, seconds)):
+        assert distances[k] == oracle.edit_distance_dp(a, b)
