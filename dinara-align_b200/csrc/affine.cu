@@ -324,7 +324,7 @@ struct WalkArgs {
     int64_t *spans;               // per pair: first row, last row, first column, last column
     int64_t first_pair, count;
     int bits;
-    bool local, eqx;
+    bool local, eqx, uniform;
 };
 
 __device__ __forceinline__ void emit_run(char *slot, int64_t &written, char op, int64_t count) {
@@ -372,8 +372,7 @@ __global__ void walk_kernel(WalkArgs a) {
         }
     };
     if (rows > 0 && cols > 0) {
-        const int cls = affine_shape_for(uint32_t(cols), true);
-        const int G = affine_lanes(cls);
+        const int G = record_lanes(uint32_t(cols), a.uniform);
         const int W = G * 16;
         const int rows_pad = ((rows + 2) | 3) + 1;
         const int64_t base = a.decision_offsets[k];
@@ -437,15 +436,14 @@ __global__ void gather_cigars_kernel(const char *__restrict__ slots, const int64
     for (int64_t i = lane; i < n; i += 32) to[i] = from[n - 1 - i];
 }
 
-__global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count,
+__global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count, bool uniform,
                                   int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const PairShape sh = shapes[first_pair + k];
     int64_t words = 0;
     if (sh.rows > 0 && sh.columns > 0) {
-        const int cls = affine_shape_for(sh.columns, true);
-        const int G = affine_lanes(cls);
+        const int G = record_lanes(sh.columns, uniform);
         const int W = G * 16;
         const int64_t strips = (sh.columns + W - 1) / W;
         const int64_t rows_pad = ((int64_t(sh.rows) + 2) | 3) + 1;
@@ -636,7 +634,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     int64_t *slot_offsets = slot_bytes + (count + 1);
     const int threads = 256;
     const unsigned blocks = unsigned((count + threads - 1) / threads);
-    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, words, slot_bytes);
+    const bool uniform = !table.packed16 || batch.bits == 8;
+    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, words, slot_bytes);
     DINARA_CUDA(cudaGetLastError());
     size_t scratch = 0;
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, words, word_offsets, int(count + 1), gpu->stream));
@@ -687,6 +686,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.bits = batch.bits;
     w.local = batch.local;
     w.eqx = eqx;
+    w.uniform = uniform;
     if (batch.bits == 8)
         walk_kernel<8><<<blocks, threads, 0, gpu->stream>>>(w);
     else

@@ -22,6 +22,12 @@ __host__ __device__ inline int affine_shape_for(uint32_t columns, bool record) {
     return 4;
 }
 
+// Lanes a pair's recording sweep takes: its shape class's, or 32 for the shared-memory table path,
+// which sweeps every pair with one shape. The decisions' layout, their sizes and the walk all follow it.
+__host__ __device__ inline int record_lanes(uint32_t columns, bool uniform) {
+    return uniform ? 32 : affine_lanes(affine_shape_for(columns, true));
+}
+
 // The substitution table a launch reads, with the gaps in the kernels' terms: `open` a gap's first
 // letter, `extend` each further one (scoring.mojo:202-215 gap_scores).
 struct AffineTable {

@@ -207,6 +207,13 @@ void class_counts(int64_t first, int64_t count, const int64_t *offsets, bool rec
     }
 }
 
+// The 64-bit words a pair's recorded decisions take (the layout affine.cu's record kernels write).
+int64_t record_words(int64_t rows, int64_t columns, bool uniform) {
+    if (rows <= 0 || columns <= 0) return 0;
+    const int64_t lanes = record_lanes(uint32_t(columns), uniform);
+    return (columns + lanes * 16 - 1) / (lanes * 16) * lanes * (((rows + 2) | 3) + 1);
+}
+
 // Per-pair statuses: scores that could pass 2^28 (-3), then a letter outside the alphabet (-1).
 void statuses_of(const CheckedScoring &checked, bool local, int64_t pairs, const int64_t *offsets,
                  const uint8_t *unknown_host, int64_t *statuses) {
@@ -432,6 +439,7 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
         int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
         // Chunks whose recorded decisions stay within a budget of device memory.
         const int64_t budget_words = (int64_t(2) << 30) / 8;
+        const bool uniform = !checked.table.packed16 || checked.bits == 8;
         std::vector<char> bytes;
         std::vector<int64_t> walk_spans(size_t(4 * pairs));
         std::vector<int64_t> ends(size_t(pairs + 1));
@@ -443,12 +451,7 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
                 const int64_t p = first + count;
                 const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
                 const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                int64_t w = 0;
-                if (rows > 0 && columns > 0) {
-                    const int cls = affine_shape_for(uint32_t(columns), true);
-                    const int64_t width = affine_lanes(cls) * 16;
-                    w = (columns + width - 1) / width * affine_lanes(cls) * (((rows + 2) | 3) + 1);
-                }
+                const int64_t w = record_words(rows, columns, uniform);
                 if (count > 0 && words + w > budget_words) break;
                 words += w;
                 ++count;
@@ -680,6 +683,7 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
             affine_scores(gpu, batch, r.checked.table, scores_device, order, counts);
         } else {
             const int64_t budget_words = (int64_t(2) << 30) / 8;
+            const bool uniform = !r.checked.table.packed16 || r.checked.bits == 8;
             int64_t first = 0;
             while (first < r.pairs) {
                 int64_t count = 0, words = 0;
@@ -687,12 +691,7 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
                     const int64_t p = first + count;
                     const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
                     const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                    int64_t w = 0;
-                    if (rows > 0 && columns > 0) {
-                        const int cls = affine_shape_for(uint32_t(columns), true);
-                        const int64_t width = affine_lanes(cls) * 16;
-                        w = (columns + width - 1) / width * affine_lanes(cls) * (((rows + 2) | 3) + 1);
-                    }
+                    const int64_t w = record_words(rows, columns, uniform);
                     if (count > 0 && words + w > budget_words) break;
                     words += w;
                     ++count;
