@@ -134,7 +134,8 @@ def reference_arm(args) -> None:
 
 def cpu_measure(oracle, workload: str, threads: int, steps: int, warmup: int) -> dict:
     """The oracle timed on `threads` host threads over a bounded sample of the workload: pairs/s."""
-    sample_pairs = {"affine": 20_000, "local": 400, "uneven": 2_000, "unit250": 10_000}[workload]
+    # Sized for roughly 10-30 s of CPU work on a 16-core host.
+    sample_pairs = {"affine": 400_000, "local": 400, "uneven": 2_000, "unit250": 10_000}[workload]
     tape = make_workload(workload, sample_pairs, seed=1000)
     letters = tape.letters[: tape.offsets[-1]]
     if workload in ("affine", "local"):
@@ -267,6 +268,19 @@ def main() -> None:
     value = world * pairs / (ms_per_step / 1e3)
 
     # End to end through the C ABI from host buffers, copies inside the timed region.
+    # The scorer alone (scores, no CIGAR) on the same resident batch: the int32 roofline's kernel.
+    scorer = None
+    if not unit:
+        score_timings = []
+        for k in range(args.warmup + args.steps):
+            timing = Timing()
+            native.check(lib.dinara_gpu_resident_align(handle, ctypes.byref(mode_struct), 0, 1, ctypes.byref(timing)),
+                         handle)
+            if k >= args.warmup:
+                score_timings.append(timing)
+        scorer = {"ms_per_step": sum(t.total_ms for t in score_timings) / len(score_timings),
+                  "kernel_ms": sum(t.kernel_ms for t in score_timings) / len(score_timings)}
+
     e2e = None
     if not args.no_e2e:
         times = []
@@ -318,6 +332,12 @@ def main() -> None:
                                 "frac": achieved / peak, "traffic": None,
                                 "ops_per_cell": ops_per_cell, "kernel_ms_per_step": kernel_ms,
                                 "peak_source": "measured here: DPX viaddmax chains on every SM, 2 ops each"}
+        if scorer and "viaddmax" in peaks:
+            achieved = cells * ops_per_cell / (scorer["kernel_ms"] / 1e3)
+            scorer.update({"pairs_per_s": world * pairs / (scorer["ms_per_step"] / 1e3),
+                           "gcups": cells / (scorer["kernel_ms"] / 1e3) / 1e9,
+                           "roofline_frac": achieved / (2 * peaks["viaddmax"])})
+            line["scorer"] = scorer
         line["int32_peaks_instr_per_s"] = peaks
         if not args.no_cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -21,292 +21,13 @@
 #include <vector>
 
 #include "affine.cuh"
+#include "affine_kernel.cuh"
 
 namespace dinara {
 
 namespace {
 
-constexpr int kBlock = 256;
-constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kPadSelector = 0x9999u;  // every byte the sign of entry 0's high byte: 0 or -1
-
-__device__ __forceinline__ int32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
-    uint32_t d;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(s));
-    return int32_t(d);
-}
-
-// The selector that reads letter `x`'s 16-bit entry from a row's two registers, sign-extended.
-__device__ __forceinline__ uint32_t selector_of(uint32_t x) {
-    const uint32_t lo = 2 * x, hi = 2 * x + 1;
-    return lo | (hi << 4) | ((hi | 8u) << 8) | ((hi | 8u) << 12);
-}
-
-template <int BITS>
-__device__ __forceinline__ uint32_t letter_at(const uint32_t *__restrict__ tape, uint32_t word, uint32_t index) {
-    constexpr uint32_t per_word = 32 / BITS;
-    constexpr uint32_t mask = BITS == 8 ? 0xFFu : ((1u << BITS) - 1u);
-    return (__ldg(tape + word + index / per_word) >> (BITS * (index % per_word))) & mask;
-}
-
-__device__ __forceinline__ int warp_max(int v) {
-#pragma unroll
-    for (int span = 16; span > 0; span >>= 1) v = max(v, __shfl_xor_sync(kFull, v, span));
-    return v;
-}
-
-struct KernelArgs {
-    const uint32_t *tape;
-    const PairShape *shapes;
-    const uint32_t *order;
-    uint32_t begin, end;
-    int32_t open, extend;
-    int32_t *scores;
-    int2 *carry;
-    int64_t carry_stride;
-    // Recording.
-    uint64_t *decisions;
-    const int64_t *decision_offsets;
-    int64_t *ends;  // local: (row << 32) | column of the best cell
-    int64_t first_pair;
-};
-
-struct TableArgs {
-    uint2 rows16[4];       // packed 16-bit entries, letter x at bytes 2x..2x+1
-    int32_t size;
-};
-
-// One pair per group of G lanes; see the file's notes. Persistent: each warp takes its next GPW pairs of
-// the bucket until the bucket ends.
-template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE>
-__global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__ table32) {
-    constexpr int W = G * C;
-    constexpr int GPW = 32 / G;
-    __shared__ uint2 rows16[4];
-    __shared__ int32_t big[SMEM_TABLE ? 32 * 33 : 1];
-    if (threadIdx.x < 4) rows16[threadIdx.x] = t.rows16[threadIdx.x];
-    if (SMEM_TABLE) {
-        for (int i = threadIdx.x; i < 32 * 33; i += kBlock) big[i] = table32[i];
-    }
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31;
-    const int member = lane % G;
-    const int group = lane / G;
-    const int warp = int((int64_t(blockIdx.x) * kBlock + threadIdx.x) >> 5);
-    const int warps = int((int64_t(gridDim.x) * kBlock) >> 5);
-    const int32_t open = p.open, extend = p.extend;
-    const int32_t opening = open - extend;  // a shifted cell's gap step
-    const int32_t first_gap = open + extend;
-    const int64_t slot = int64_t(warp) * GPW + group;
-
-    for (uint32_t base = p.begin + uint32_t(warp) * GPW; base < p.end; base += uint32_t(warps) * GPW) {
-        const uint32_t item = base + group;
-        const bool live = item < p.end;
-        uint32_t pair = 0;
-        PairShape sh{0, 0, 0, 0};
-        if (live) {
-            pair = p.order[item];
-            sh = p.shapes[pair];
-        }
-        const int rows = int(sh.rows), cols = int(sh.columns);
-        const bool work = live && rows > 0 && cols > 0;
-        const int strips = work ? (cols + W - 1) / W : 0;
-        const int warp_strips = warp_max(strips);
-        int32_t reported = 0;
-        int32_t best = 0;
-        int64_t best_place = 0;
-        int64_t dec_base = 0;
-        const int rows_pad = ((rows + 2) | 3) + 1;
-        if (RECORD && work) dec_base = p.decision_offsets[pair - p.first_pair];
-
-        for (int s = 0; s < warp_strips; ++s) {
-            const bool strip_live = s < strips;
-            const int first_col = s * W + member * C;
-            const int owned = min(max(cols - first_col, 0), C);
-            uint32_t sel[C];
-#pragma unroll
-            for (int k = 0; k < C; ++k) {
-                const int col = first_col + k;
-                if (strip_live && col < cols) {
-                    const uint32_t x = letter_at<BITS>(p.tape, sh.second_word, uint32_t(col));
-                    sel[k] = SMEM_TABLE ? x : selector_of(x);
-                } else {
-                    sel[k] = SMEM_TABLE ? 32u : kPadSelector;
-                }
-            }
-            const int32_t top = LOCAL ? 0 : opening;
-            int32_t H[C], D[C];
-#pragma unroll
-            for (int k = 0; k < C; ++k) {
-                H[k] = top;
-                D[k] = top + first_gap;
-            }
-            int32_t edgeH = top, edgeI = top + first_gap;
-            int32_t above_left = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
-            const int steps = strip_live ? rows + G : 0;
-            const int warp_steps = warp_max(steps);
-            uint64_t buffered[4] = {0, 0, 0, 0};
-            uint64_t *lane_block = nullptr;
-            if (RECORD) lane_block = p.decisions + dec_base + int64_t(s * G + member) * rows_pad;
-
-            for (int step0 = 1; step0 <= warp_steps; step0 += 4) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int step = step0 + u;
-                    if (step <= warp_steps) {
-                        const int row = step - member;
-                        int32_t leftH = __shfl_up_sync(kFull, edgeH, 1, G);
-                        int32_t leftI = __shfl_up_sync(kFull, edgeI, 1, G);
-                        if (member == 0) {
-                            if (s == 0) {
-                                leftH = LOCAL ? 0 : opening;
-                                leftI = leftH + first_gap;
-                            } else {
-                                const int r = min(max(row, 0), rows);
-                                const int2 c = p.carry[slot * p.carry_stride + r];
-                                leftH = c.x;
-                                leftI = c.y;
-                            }
-                        }
-                        int32_t diag = above_left;
-                        above_left = leftH;
-                        if (strip_live && row >= 1 && row <= rows) {
-                            const uint32_t rl = letter_at<BITS>(p.tape, sh.first_word, uint32_t(row - 1));
-                            uint2 tr = make_uint2(0, 0);
-                            const int32_t *trow = nullptr;
-                            if (SMEM_TABLE)
-                                trow = big + rl * 33;
-                            else
-                                tr = rows16[rl];
-                            int32_t I = 0, Xprev = 0, Hprev = leftH, Iprev = leftI;
-                            uint32_t word_lo = 0, word_hi = 0;
-                            const int64_t row_place = int64_t(row) * (cols + 1) + first_col + 1;
-#pragma unroll
-                            for (int k = 0; k < C; ++k) {
-                                const int32_t sub = SMEM_TABLE ? trow[sel[k]] : prmt(tr.x, tr.y, sel[k]);
-                                const int32_t Hup = H[k], Dup = D[k];
-                                int32_t Dn, X, Hn, Xd = 0;
-                                if (LOCAL) {
-                                    Dn = __viaddmax_s32(Hup, open, Dup + extend);
-                                } else {
-                                    Dn = __viaddmax_s32(Hup, opening, Dup);
-                                }
-                                if (RECORD) {
-                                    Xd = diag + sub;
-                                    X = max(Xd, Dn);
-                                } else {
-                                    X = __viaddmax_s32(diag, sub, Dn);
-                                }
-                                if (k == 0) {
-                                    I = LOCAL ? max(leftH + open, leftI + extend) : __viaddmax_s32(leftH, opening, leftI);
-                                } else {
-                                    I = LOCAL ? __viaddmax_s32(I, extend, Xprev) : __viaddmax_s32(Xprev, opening, I);
-                                }
-                                Hn = LOCAL ? __vimax_s32_relu(X, I) : max(X, I);
-                                if (RECORD) {
-                                    uint32_t source, dext, iext;
-                                    if (LOCAL) {
-                                        dext = Dup + extend > Hup + open;
-                                        iext = Iprev + extend > Hprev + open;
-                                        source = Hn <= 0 ? 3u : (Hn == Xd ? 0u : (Hn == Dn ? 1u : 2u));
-                                    } else {
-                                        dext = Dup > Hup + opening;
-                                        iext = Iprev > Hprev + opening;
-                                        source = Hn == Xd ? 0u : (Hn == Dn ? 1u : 2u);
-                                    }
-                                    const uint32_t nibble = source | (dext << 2) | (iext << 3);
-                                    if (k < 8)
-                                        word_lo |= nibble << (4 * k);
-                                    else
-                                        word_hi |= nibble << (4 * (k - 8));
-                                    // beats(), gotoh.mojo:122-127, as strips visit rows out of order.
-                                    if (LOCAL && k < owned &&
-                                        (Hn > best || (Hn == best && Hn != 0 && row_place + k < best_place))) {
-                                        best = Hn;
-                                        best_place = row_place + k;
-                                    }
-                                } else if (LOCAL) {
-                                    best = max(best, Hn);
-                                }
-                                // Local: the next cell's insertion reads max(X, 0) + open, kept as Xprev.
-                                Xprev = LOCAL ? __viaddmax_s32(X, open, open) : X;
-                                Hprev = Hn;
-                                Iprev = I;
-                                diag = Hup;
-                                H[k] = Hn;
-                                D[k] = Dn;
-                            }
-                            edgeH = H[C - 1];
-                            edgeI = I;
-                            if (member == G - 1 && s + 1 < strips) {
-                                p.carry[slot * p.carry_stride + row] = make_int2(H[C - 1], I);
-                            }
-                            if (!LOCAL && row == rows && owned > 0 && first_col + owned == cols) {
-#pragma unroll
-                                for (int k = 0; k < C; ++k)
-                                    if (k == owned - 1) reported = H[k];
-                            }
-                            if (RECORD) {
-                                buffered[u] = (uint64_t(word_hi) << 32) | word_lo;
-                                if (u == 3 || row == rows) {
-                                    uint64_t *at = lane_block + ((row - 1 + (member & 3)) & ~3);
-                                    reinterpret_cast<uint4 *>(at)[0] = make_uint4(
-                                        uint32_t(buffered[0]), uint32_t(buffered[0] >> 32), uint32_t(buffered[1]),
-                                        uint32_t(buffered[1] >> 32));
-                                    reinterpret_cast<uint4 *>(at)[1] = make_uint4(
-                                        uint32_t(buffered[2]), uint32_t(buffered[2] >> 32), uint32_t(buffered[3]),
-                                        uint32_t(buffered[3] >> 32));
-                                }
-                            }
-                        }
-                    }
-                }
-            }
-            __syncwarp();
-        }
-
-        // Results: a global score is the corner shifted back; a local one the group's best.
-        if (LOCAL) {
-#pragma unroll
-            for (int span = 1; span < G; span <<= 1) {
-                const int32_t theirs = __shfl_xor_sync(kFull, best, span, G);
-                if (RECORD) {
-                    const int64_t their_place = __shfl_xor_sync(kFull, best_place, span, G);
-                    // beats(), gotoh.mojo:122-127: higher, or equal above zero at an earlier place.
-                    if (theirs > best || (theirs == best && theirs != 0 && their_place < best_place)) {
-                        best = theirs;
-                        best_place = their_place;
-                    }
-                } else {
-                    best = max(best, theirs);
-                }
-            }
-            if (live && member == 0) {
-                p.scores[pair] = best;
-                if (RECORD) {
-                    int64_t end = 0;
-                    if (best > 0) {
-                        const int64_t stride = cols + 1;
-                        end = ((best_place / stride) << 32) | (best_place % stride);
-                    }
-                    p.ends[pair - p.first_pair] = end;
-                }
-            }
-        } else if (live) {
-            const int total = rows + cols;
-            if (!work) {
-                if (member == 0) p.scores[pair] = total == 0 ? 0 : open + (total - 1) * extend;
-            } else {
-                const int owner_first = ((cols - 1) % W) / C * C;
-                if (member == ((cols - 1) % W) / C) {
-                    (void)owner_first;
-                    p.scores[pair] = reported + total * extend;
-                }
-            }
-        }
-    }
-}
+using namespace sweep;
 
 // ------------------------------------------------------------------------------------------------
 // The walk back and the CIGAR

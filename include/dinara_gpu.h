@@ -198,6 +198,32 @@ int64_t dinara_gpu_resident_distances(dinara_gpu *gpu, const dinara_band_plan *p
  * `distances` (int64) for a distance run; either may be null. */
 int64_t dinara_gpu_resident_fetch(dinara_gpu *gpu, int32_t *scores, int64_t *distances);
 
+/*
+ * Scores without allocating (no counterpart in the reference). For callers that cannot allocate device
+ * memory themselves or through this library (code inside another framework's memory pool, or under a
+ * budget that forbids growth): the caller passes its own device buffers, a packed batch and the room
+ * for the scores, and the call allocates nothing, keeping its working memory in one fixed device array
+ * of 20 MiB that every device loading this library holds until exit.
+ *
+ * `tape` holds each sequence's letters as 2-bit codes in the Scoring's alphabet order (alphabets of up
+ * to 4 letters), 16 a 32-bit word, lowest bits first, each sequence from a 16-byte boundary; pair i is
+ * described by shapes[i] (word offsets into `tape` and lengths). Writes scores[i] (int32, device) on
+ * `stream` (a cudaStream_t; null is the default stream) and returns once the work is enqueued.
+ * Limits: a pair wider than 512 columns may have at most 8,191 reference letters (else
+ * DINARA_OUT_OF_MEMORY and nothing runs); a shifted table entry must fit 16 bits.
+ * The first call on a device sets its array up (and synchronizes the stream), so make it before any
+ * stream capture. Calls share the array: two calls that overlap on the GPU race, so serialize them.
+ */
+typedef struct {
+    uint32_t first_word; /* the reference's first word in `tape` */
+    uint32_t rows;       /* the reference's letters */
+    uint32_t second_word;/* the query's first word */
+    uint32_t columns;    /* the query's letters */
+} dinara_packed_pair;
+
+int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const uint32_t *tape, const dinara_packed_pair *shapes,
+                                 const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, void *stream);
+
 /* The device's measured integer issue rate (no reference counterpart: the roofline the sweeps are
  * judged against): `kind` 0 DPX add-and-max, 1 min/max with an add, 2 three-input add; instructions
  * per second into *instructions_per_second, from independent chains on every SM. */
