@@ -22,6 +22,8 @@
 
 #include "affine.cuh"
 #include "affine_kernel.cuh"
+#include "banded.cuh"
+#include "pack.cuh"
 
 namespace dinara {
 
@@ -37,6 +39,8 @@ struct WalkArgs {
     const uint32_t *tape;
     const PairShape *shapes;
     const uint64_t *decisions;
+    const uint64_t *decisions_extra;  // the band's leftovers, swept whole afterwards
+    const uint8_t *layouts;           // per pair: 0 whole matrix, 1 band, 2 whole matrix in decisions_extra
     const int64_t *decision_offsets;
     const int64_t *ends;
     const int64_t *slot_offsets;  // per pair: its CIGAR slot, 2 (rows + columns) + 1 bytes
@@ -93,18 +97,34 @@ __global__ void walk_kernel(WalkArgs a) {
         }
     };
     if (rows > 0 && cols > 0) {
+        const int layout = a.layouts[k];
+        const uint64_t *decisions = layout == 2 ? a.decisions_extra : a.decisions;
         const int G = record_lanes(uint32_t(cols), a.uniform);
         const int W = G * 16;
-        const int rows_pad = ((rows + 2) | 3) + 1;
+        const int rows_pad = layout == 1 ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
+        const int low = layout == 1 ? band_low_for(rows, cols) : 0;
         const int64_t base = a.decision_offsets[k];
         int state = 0;  // 0 aligning, 1 deleting, 2 inserting
         while (row > 0 && column > 0) {
-            const int off = column - 1;
-            const int s = off / W;
-            const int within = off % W;
-            const int member = within / 16;
-            const int slot_in = within % 16;
-            const uint64_t word = a.decisions[base + int64_t(s * G + member) * rows_pad + (row - 1 + (member & 3))];
+            int64_t at;
+            int slot_in;
+            if (layout == 1) {
+                // The band's layout: place o = column - row - low, a lane of 16 places a block of rows.
+                const int place = column - row - low;
+                // The proof keeps every optimal path inside the band; a place outside it would read
+                // another pair's decisions, so the walk stops there instead.
+                if (place < 0 || place >= kBandWidth) break;
+                slot_in = place % 16;
+                at = base + int64_t(place / 16) * rows_pad + (row - 1);
+            } else {
+                const int off = column - 1;
+                const int s = off / W;
+                const int within = off % W;
+                const int member = within / 16;
+                slot_in = within % 16;
+                at = base + int64_t(s * G + member) * rows_pad + (row - 1 + (member & 3));
+            }
+            const uint64_t word = decisions[at];
             const uint32_t nibble = uint32_t(word >> (4 * slot_in)) & 15u;
             if (a.local && state == 0 && (nibble & 3u) == 3u) break;
             const int moving = state == 0 ? int(nibble & 3u) : state;
@@ -158,12 +178,17 @@ __global__ void gather_cigars_kernel(const char *__restrict__ slots, const int64
 }
 
 __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count, bool uniform,
-                                  int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes) {
+                                  bool band, int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes,
+                                  uint8_t *__restrict__ layouts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const PairShape sh = shapes[first_pair + k];
     int64_t words = 0;
-    if (sh.rows > 0 && sh.columns > 0) {
+    uint8_t layout = 0;
+    if (band && band_eligible(sh.rows, sh.columns)) {
+        layout = 1;
+        words = int64_t(kBandLanes) * ((int64_t(sh.rows) + 3) & ~int64_t(3));
+    } else if (sh.rows > 0 && sh.columns > 0) {
         const int G = record_lanes(sh.columns, uniform);
         const int W = G * 16;
         const int64_t strips = (sh.columns + W - 1) / W;
@@ -172,6 +197,48 @@ __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t 
     }
     decision_words[k] = words;
     slot_bytes[k] = 2 * (int64_t(sh.rows) + sh.columns) + 8;
+    layouts[k] = layout;
+}
+
+// Cells a batch's sweeps update: 64 a row for a banded pair, the whole matrix for the rest and again for
+// each leftover of the band.
+__global__ void swept_cells_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count, bool band,
+                                   const uint32_t *__restrict__ leftovers, int64_t left,
+                                   unsigned long long *__restrict__ out) {
+    unsigned long long sum = 0;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < count + left;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        const PairShape sh = k < count ? shapes[first + k] : shapes[leftovers[k - count]];
+        if (k < count && band && band_eligible(sh.rows, sh.columns))
+            sum += (unsigned long long)sh.rows * kBandWidth;
+        else
+            sum += (unsigned long long)sh.rows * sh.columns;
+    }
+#pragma unroll
+    for (int span = 16; span > 0; span >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, span);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, sum);
+}
+
+// The whole-matrix words of each leftover pair of the band.
+__global__ void leftover_words_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ leftovers,
+                                      int64_t count, bool uniform, int64_t *__restrict__ words) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const PairShape sh = shapes[leftovers[k]];
+    const int G = record_lanes(sh.columns, uniform);
+    const int W = G * 16;
+    words[k] = (int64_t(sh.columns) + W - 1) / W * G * (((int64_t(sh.rows) + 2) | 3) + 1);
+}
+
+// Points each leftover's decisions at its place in the extra buffer and marks its layout.
+__global__ void leftover_places_kernel(const uint32_t *__restrict__ leftovers, int64_t count, int64_t first_pair,
+                                       const int64_t *__restrict__ offsets, int64_t *__restrict__ decision_offsets,
+                                       uint8_t *__restrict__ layouts) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t pair = int64_t(leftovers[k]) - first_pair;
+    decision_offsets[pair] = offsets[k];
+    layouts[pair] = 2;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -267,36 +334,48 @@ void upload_table32(dinara_gpu *gpu, const AffineTable &table, bool local, int32
     *out = dev;
 }
 
+// The sorted order's ranges per whole-matrix class: the band's pairs first, then classes 4 to 0.
 struct Buckets {
     int64_t begin[kAffineShapes];
     int64_t end[kAffineShapes];
 };
 
-// The sorted order's ranges per shape class: classes in descending order, as the keys put them.
-Buckets buckets_of(const int64_t counts[kAffineShapes]) {
+Buckets buckets_of(const Schedule &schedule) {
     Buckets b;
-    int64_t at = 0;
+    int64_t at = schedule.counts[kBandClass];
     for (int cls = kAffineShapes - 1; cls >= 0; --cls) {
         b.begin[cls] = at;
-        at += counts[cls];
+        at += schedule.counts[cls];
         b.end[cls] = at;
     }
     return b;
 }
 
-}  // namespace
+// Device time of a sweep phase, added to the context's tally while it times.
+struct PhaseTimer {
+    dinara_gpu *gpu;
+    double *into;
+    explicit PhaseTimer(dinara_gpu *g, double *target) : gpu(g), into(target) {
+        if (gpu->timing) DINARA_CUDA(cudaEventRecord(gpu->start, gpu->stream));
+    }
+    void stop() {
+        if (!gpu->timing) return;
+        DINARA_CUDA(cudaEventRecord(gpu->stop, gpu->stream));
+        DINARA_CUDA(cudaEventSynchronize(gpu->stop));
+        float ms = 0.f;
+        DINARA_CUDA(cudaEventElapsedTime(&ms, gpu->start, gpu->stop));
+        *into += ms;
+    }
+};
 
-namespace {
-
-void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const uint32_t *order,
-                       const int64_t counts[kAffineShapes], bool record, KernelArgs args) {
+void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const Schedule &schedule,
+                       bool record, KernelArgs args) {
     const bool smem = !table.packed16 || batch.bits == 8;
     const TableArgs targs = table_args(table, batch.local);
     int32_t *table32 = nullptr;
     if (smem) upload_table32(gpu, table, batch.local, &table32);
-    const Buckets b = buckets_of(counts);
-    args.order = order;
-    if (gpu->timing) DINARA_CUDA(cudaEventRecord(gpu->start, gpu->stream));
+    const Buckets b = buckets_of(schedule);
+    args.order = schedule.order;
     for (int cls = kAffineShapes - 1; cls >= 0; --cls) {
         if (b.end[cls] <= b.begin[cls]) continue;
         KernelFn fn = pick_kernel(cls, batch.local, record, batch.bits, smem);
@@ -322,19 +401,62 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
         DINARA_CUDA(cudaGetLastError());
         gpu->launches += 1;
     }
-    if (gpu->timing) {
-        DINARA_CUDA(cudaEventRecord(gpu->stop, gpu->stream));
-        DINARA_CUDA(cudaEventSynchronize(gpu->stop));
-        float ms = 0.f;
-        DINARA_CUDA(cudaEventElapsedTime(&ms, gpu->start, gpu->stop));
-        (record ? gpu->record_ms : gpu->kernel_ms) += ms;
-    }
+}
+
+// The band's shifted table and best entry for a banded launch.
+BandedBatch banded_batch(const AffineBatch &batch, const AffineTable &table, const Schedule &schedule, int32_t *scores,
+                         uint8_t *proven, uint32_t *leftovers, unsigned int *leftover_count) {
+    BandedBatch band;
+    std::memset(&band, 0, sizeof band);
+    const TableArgs targs = table_args(table, false);
+    for (int r = 0; r < 4; ++r) band.rows16[r] = targs.rows16[r];
+    int32_t best = -128;
+    for (int r = 0; r < table.size; ++r)
+        for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
+    band.tape = batch.tape;
+    band.shapes = batch.shapes;
+    band.order = schedule.order;
+    band.count = schedule.counts[kBandClass];
+    band.open = table.open;
+    band.extend = table.extend;
+    band.best = best;
+    band.scores = scores;
+    band.proven = proven;
+    band.leftovers = leftovers;
+    band.leftover_count = leftover_count;
+    return band;
+}
+
+// Adds the cells a batch's sweeps updated to the context's tally (only while it times).
+void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool band,
+                 const uint32_t *leftovers, int64_t left) {
+    if (!gpu->timing) return;
+    unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(16) + 12);
+    DINARA_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long), gpu->stream));
+    swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, out);
+    DINARA_CUDA(cudaGetLastError());
+    unsigned long long host = 0;
+    DINARA_CUDA(cudaMemcpyAsync(&host, out, sizeof host, cudaMemcpyDeviceToHost, gpu->stream));
+    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    gpu->swept_cells += int64_t(host);
 }
 
 }  // namespace
 
+bool band_serves(const AffineBatch &batch, const AffineTable &table) {
+    if (batch.local || batch.bits != 2 || !table.packed16) return false;
+    int32_t best = -128;
+    for (int r = 0; r < table.size; ++r)
+        for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
+    return 2 * int64_t(table.extend) - best <= 0;
+}
+
 void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
-                   const uint32_t *order, const int64_t counts[kAffineShapes]) {
+                   int64_t first, int64_t count) {
+    if (count <= 0) return;
+    const bool band = band_serves(batch, table);
+    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, band);
+    PhaseTimer timer(gpu, &gpu->kernel_ms);
     KernelArgs args;
     std::memset(&args, 0, sizeof args);
     args.tape = batch.tape;
@@ -342,21 +464,42 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
     args.open = table.open;
     args.extend = table.extend;
     args.scores = scores;
-    affine_launch_all(gpu, batch, table, order, counts, false, args);
+    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(16);
+    unsigned int *leftover_count = counters + 8;
+    uint32_t *leftovers = nullptr;
+    if (schedule_all.counts[kBandClass] > 0) {
+        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(schedule_all.counts[kBandClass]));
+        DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
+        banded_launch(gpu, banded_batch(batch, table, schedule_all, scores, nullptr, leftovers, leftover_count), false);
+    }
+    affine_launch_all(gpu, batch, table, schedule_all, false, args);
+    unsigned int left = 0;
+    if (schedule_all.counts[kBandClass] > 0) {
+        DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        if (left > 0) {
+            const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, false, false);
+            affine_launch_all(gpu, batch, table, again, false, args);
+        }
+    }
+    timer.stop();
+    tally_swept(gpu, batch.shapes, first, count, band, leftovers, left);
 }
 
 int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, bool eqx,
-                          int32_t *scores, int64_t *spans, int64_t first_pair, int64_t count, const uint32_t *order,
-                          const int64_t counts[kAffineShapes]) {
-    // Per pair: its decisions' words and its CIGAR slot, then their offsets by an exclusive scan.
+                          int32_t *scores, int64_t *spans, int64_t first_pair, int64_t count) {
+    const bool band = band_serves(batch, table);
+    const bool uniform = !table.packed16 || batch.bits == 8;
+    // Per pair: its decisions' words, its layout and its CIGAR slot, then the offsets by exclusive scans.
     int64_t *words = gpu->decision_offsets.ensure<int64_t>(2 * (count + 1) + 2);
     int64_t *word_offsets = words + (count + 1);
     int64_t *slot_bytes = gpu->cigar_slots.ensure<int64_t>(2 * (count + 1) + 2);
     int64_t *slot_offsets = slot_bytes + (count + 1);
+    uint8_t *layouts = gpu->layouts.ensure<uint8_t>(size_t(count) + 1);
     const int threads = 256;
     const unsigned blocks = unsigned((count + threads - 1) / threads);
-    const bool uniform = !table.packed16 || batch.bits == 8;
-    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, words, slot_bytes);
+    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, band, words,
+                                                           slot_bytes, layouts);
     DINARA_CUDA(cudaGetLastError());
     size_t scratch = 0;
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, words, word_offsets, int(count + 1), gpu->stream));
@@ -377,7 +520,9 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     char *slots = gpu->walk_out.ensure<char>(size_t(totals[1]) + 8);
     int64_t *ends = gpu->spans.ensure<int64_t>(size_t(count) + 1);
     int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(size_t(count) + 1);
+    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band);
 
+    PhaseTimer timer(gpu, &gpu->record_ms);
     KernelArgs args;
     std::memset(&args, 0, sizeof args);
     args.tape = batch.tape;
@@ -389,13 +534,59 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     args.decision_offsets = word_offsets;
     args.ends = ends;
     args.first_pair = first_pair;
-    affine_launch_all(gpu, batch, table, order, counts, true, args);
+    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(16);
+    unsigned int *leftover_count = counters + 8;
+    uint32_t *leftovers = nullptr;
+    uint64_t *extra = nullptr;
+    if (schedule_all.counts[kBandClass] > 0) {
+        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(schedule_all.counts[kBandClass]));
+        DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
+        BandedBatch band_args = banded_batch(batch, table, schedule_all, scores, nullptr, leftovers, leftover_count);
+        band_args.decisions = decisions;
+        band_args.decision_offsets = word_offsets;
+        band_args.first_pair = first_pair;
+        banded_launch(gpu, band_args, true);
+    }
+    affine_launch_all(gpu, batch, table, schedule_all, true, args);
+    unsigned int left = 0;
+    if (schedule_all.counts[kBandClass] > 0) {
+        DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        if (left > 0) {
+            // The band's leftovers, swept whole: their decisions in the extra buffer.
+            int64_t *left_words = gpu->thresholds.ensure<int64_t>(2 * (size_t(left) + 1) + 2);
+            int64_t *left_offsets = left_words + (left + 1);
+            const unsigned left_blocks = unsigned((left + threads - 1) / threads);
+            leftover_words_kernel<<<left_blocks, threads, 0, gpu->stream>>>(batch.shapes, leftovers, left, uniform,
+                                                                            left_words);
+            DINARA_CUDA(cudaGetLastError());
+            DINARA_CUDA(cudaMemsetAsync(left_words + left, 0, sizeof(int64_t), gpu->stream));
+            size_t bytes = 0;
+            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, left_words, left_offsets, int(left + 1), gpu->stream));
+            space = gpu->sort_scratch.ensure<uint8_t>(bytes + 256);
+            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, bytes, left_words, left_offsets, int(left + 1), gpu->stream));
+            int64_t extra_total = 0;
+            DINARA_CUDA(cudaMemcpyAsync(&extra_total, left_offsets + left, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                        gpu->stream));
+            DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+            extra = gpu->decisions_extra.ensure<uint64_t>(size_t(extra_total) + 8);
+            leftover_places_kernel<<<left_blocks, threads, 0, gpu->stream>>>(leftovers, left, first_pair, left_offsets,
+                                                                             word_offsets, layouts);
+            DINARA_CUDA(cudaGetLastError());
+            const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, true, false);
+            KernelArgs extra_args = args;
+            extra_args.decisions = extra;
+            affine_launch_all(gpu, batch, table, again, true, extra_args);
+        }
+    }
 
     WalkArgs w;
     std::memset(&w, 0, sizeof w);
     w.tape = batch.tape;
     w.shapes = batch.shapes;
     w.decisions = decisions;
+    w.decisions_extra = extra ? extra : decisions;
+    w.layouts = layouts;
     w.decision_offsets = word_offsets;
     w.ends = ends;
     w.slot_offsets = slot_offsets;
@@ -413,6 +604,9 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     else
         walk_kernel<2><<<blocks, threads, 0, gpu->stream>>>(w);
     DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
+    timer.stop();
+    tally_swept(gpu, batch.shapes, first_pair, count, band, leftovers, left);
 
     // The CIGARs' offsets, then each turned round into place.
     int64_t *offsets = gpu->cigar_offsets.ensure<int64_t>(size_t(count) + 2);
@@ -428,6 +622,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     const unsigned gather_blocks = unsigned((count * 32 + threads - 1) / threads);
     gather_cigars_kernel<<<gather_blocks, threads, 0, gpu->stream>>>(slots, slot_offsets, lengths, offsets, out, count);
     DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
     return total;
 }
 

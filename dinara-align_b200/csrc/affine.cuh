@@ -46,18 +46,20 @@ struct AffineBatch {
     uint32_t max_rows, max_columns;
 };
 
-// Scores of a packed batch into `scores` (device): `order` lists the pairs longest first, the classes
-// of affine_shape_for(columns, false) in descending order, `counts[c]` pairs of class c.
-void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
-                   const uint32_t *order, const int64_t counts[kAffineShapes]);
+// Whether a batch's global pairs may be swept over proven bands (a 2-bit alphabet, the 16-bit table and
+// a bound that holds for its table): pairs the band does not prove are swept whole.
+bool band_serves(const AffineBatch &batch, const AffineTable &table);
 
-// Alignments of pairs [first_pair, first_pair + count) of a packed batch, ordered as for scores but by
-// affine_shape_for(columns, true): scores into `scores` (indexed by pair), spans (4 per pair of the
-// range: first row, last row, first column, last column of the walk) into `spans`, and each pair's
-// CIGAR: returns the CIGAR bytes' total and leaves their offsets (count + 1, device) in
+// Scores of pairs [first, first + count) of a packed batch into `scores` (device, indexed by pair): the
+// proven band where it serves, every other pair over its whole matrix, longest first.
+void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
+                   int64_t first, int64_t count);
+
+// Alignments of pairs [first_pair, first_pair + count): scores into `scores` (indexed by pair), spans (4
+// per pair of the range: first row, last row, first column, last column of the walk) into `spans`, and
+// each pair's CIGAR; returns the CIGAR bytes' total and leaves their offsets (count + 1, device) in
 // gpu->cigar_offsets and the bytes in gpu->cigar_bytes.
 int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, bool eqx,
-                          int32_t *scores, int64_t *spans, int64_t first_pair, int64_t count, const uint32_t *order,
-                          const int64_t counts[kAffineShapes]);
+                          int32_t *scores, int64_t *spans, int64_t first_pair, int64_t count);
 
 }  // namespace dinara

@@ -1,0 +1,223 @@
+// Global Gotoh over a band of 64 diagonals a pair, proven by the pair's own score.
+//
+// Four lanes hold a pair's band, 16 diagonals each, and sweep its rows together: a cell at band place o
+// on row r is column r + low + o, so the cell diagonally before it sits at the same place a row up, the
+// one above at place o + 1 (the next lane's first, by shuffle, at a lane's edge), and the one to its
+// left at o - 1 on the same row. The insertion layer along a row is a running maximum (cells shifted by
+// (row + column) * extend, as score_groups.mojo:114-120 holds them), so the four lanes take it as a
+// prefix maximum: each lane's own, then a two-step shuffle scan across the four. Cells left of column 0
+// start below every score and stay there; the first column's cells come out of the recurrence as the
+// border the reference sets; cells right of the last column are never read by a real one. So no cell is
+// masked.
+//
+// The query's letters move one place along the band each row: a lane keeps the selectors of 32
+// consecutive letters and reads them at a place that advances with the row, the rows unrolled sixteen at
+// a time so every place is a constant, and refills the 32 every sixteen rows.
+//
+// The band's score is accepted when every path leaving the band provably scores below it
+// (band_proves); then every optimal path lies inside it, so the band's cells on those paths hold the
+// whole matrix's values and its recorded decisions walk back the same CIGAR as the whole matrix's.
+// Pairs the band does not prove go on a leftover list for the whole-matrix sweep.
+#include "affine_kernel.cuh"
+#include "banded.cuh"
+
+namespace dinara {
+namespace {
+
+using namespace sweep;
+
+constexpr int32_t kUnreached = -(1 << 28);  // below every score a sweep can hold (ScoreReach bounds them)
+
+template <bool RECORD>
+__global__ void __launch_bounds__(kBlock) banded_kernel(BandedBatch b) {
+    constexpr int G = kBandLanes, C = kBandColumns;
+    constexpr int GPW = 32 / G;
+    __shared__ uint2 rows16[4];
+    if (threadIdx.x < 4) rows16[threadIdx.x] = b.rows16[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int member = lane % G;
+    const int group = lane / G;
+    const int warp = int((int64_t(blockIdx.x) * kBlock + threadIdx.x) >> 5);
+    const int warps = int((int64_t(gridDim.x) * kBlock) >> 5);
+    const int32_t open = b.open, extend = b.extend;
+    const int32_t opening = open - extend;
+
+    for (int64_t base = int64_t(warp) * GPW; base < b.count; base += int64_t(warps) * GPW) {
+        const int64_t item = base + group;
+        const bool live = item < b.count;
+        uint32_t pair = 0;
+        PairShape sh{0, 0, 0, 0};
+        if (live) {
+            pair = b.order[item];
+            sh = b.shapes[pair];
+        }
+        const int rows = int(sh.rows), cols = int(sh.columns);
+        const int low = live ? band_low_for(rows, cols) : 0;
+        const int first_place = member * C;  // this lane's first place in the band
+        int warp_rows = live ? rows : 0;
+#pragma unroll
+        for (int span = 16; span > 0; span >>= 1) warp_rows = max(warp_rows, __shfl_xor_sync(kFull, warp_rows, span));
+
+        // Row 0: the origin 0, the first row's shifted border `opening`, left of the matrix unreached.
+        int32_t H[C], D[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = low + first_place + k;
+            H[k] = c < 0 ? kUnreached : (c == 0 ? 0 : opening);
+            D[k] = kUnreached;
+        }
+        const int end_place = cols - rows - low;  // the corner's place in the band
+        int32_t reported = kUnreached;
+        int64_t dec_base = 0;
+        const int rows_pad = (rows + 3) & ~3;
+        if (RECORD && live) dec_base = b.decision_offsets[pair - b.first_pair] + int64_t(member) * rows_pad;
+        uint64_t buffered[4] = {0, 0, 0, 0};
+
+        for (int r0 = 1; r0 <= warp_rows; r0 += 16) {
+            // Selectors of the 32 letters from column r0 + low + first_place on (letter index one less).
+            uint32_t window[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int column = r0 + low + first_place + j;  // the column whose letter place j holds
+                window[j] = (live && column >= 1 && column <= cols)
+                                ? selector_of(letter_at<2>(b.tape, sh.second_word, uint32_t(column - 1)))
+                                : 0x9999u;
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int row = r0 + u;
+                if (row <= warp_rows) {
+                    const bool active = live && row <= rows;
+                    // The row above's cell at the next place: this lane's next, or the next lane's first.
+                    const int32_t nextH = __shfl_down_sync(kFull, H[0], 1, G);
+                    const int32_t nextD = __shfl_down_sync(kFull, D[0], 1, G);
+                    uint2 tr = make_uint2(0, 0);
+                    if (active) tr = rows16[letter_at<2>(b.tape, sh.first_word, uint32_t(row - 1))];
+                    int32_t X[C];
+                    int32_t S = kUnreached;  // running max of X + opening along this lane's places
+                    uint32_t word_lo = 0, word_hi = 0;
+                    // Pass 1: the deletion layer and the best of the diagonal and deletion moves. Only D[k] is
+                    // rewritten here, after place k-1 has read it, so every read is of the row above.
+#pragma unroll
+                    for (int k = 0; k < C; ++k) {
+                        const int32_t Hup = k + 1 < C ? H[k + 1] : (member == G - 1 ? kUnreached : nextH);
+                        const int32_t Dup = k + 1 < C ? D[k + 1] : (member == G - 1 ? kUnreached : nextD);
+                        const int32_t sub = prmt(tr.x, tr.y, window[k + u]);
+                        if (RECORD) {
+                            const int32_t opened = Hup + opening;
+                            const int32_t dn = max(opened, Dup);
+                            const int32_t xd = H[k] + sub;
+                            const int32_t x = max(xd, dn);
+                            // gotoh.mojo:173-186 decide: a deletion run extends only where extending beats
+                            // opening; the source is the diagonal unless the deletion beats it.
+                            const uint32_t bits = (x != xd ? 1u : 0u) | (Dup > opened ? 4u : 0u);
+                            if (k < 8)
+                                word_lo |= bits << (4 * k);
+                            else
+                                word_hi |= bits << (4 * (k - 8));
+                            D[k] = dn;
+                            X[k] = x;
+                        } else {
+                            D[k] = __viaddmax_s32(Hup, opening, Dup);
+                            X[k] = __viaddmax_s32(H[k], sub, D[k]);
+                        }
+                        S = __viaddmax_s32(X[k], opening, S);
+                    }
+                    // Exclusive prefix maximum of the four lanes' running maxima.
+                    int32_t reach = __shfl_up_sync(kFull, S, 1, G);
+                    if (member == 0) reach = kUnreached;
+                    {
+                        const int32_t further = __shfl_up_sync(kFull, reach, 1, G);
+                        if (member >= 1) reach = max(reach, further);
+                        const int32_t further2 = __shfl_up_sync(kFull, reach, 2, G);
+                        if (member >= 2) reach = max(reach, further2);
+                    }
+                    // Pass 2: the insertion layer (the best earlier X plus an opening) and the scores.
+                    int32_t S2 = reach;
+                    uint32_t ins_lo = 0, ins_hi = 0;
+#pragma unroll
+                    for (int k = 0; k < C; ++k) {
+                        const int32_t I = S2;
+                        S2 = __viaddmax_s32(X[k], opening, S2);
+                        if (RECORD) {
+                            const int32_t Hn = max(X[k], I);
+                            // The insertion beats both: the source is inserting (ties go to the diagonal,
+                            // then the deletion, as decide() orders them).
+                            if (k < 8)
+                                ins_lo |= (I > X[k] ? 2u : 0u) << (4 * k);
+                            else
+                                ins_hi |= (I > X[k] ? 2u : 0u) << (4 * (k - 8));
+                            H[k] = Hn;
+                            X[k] = I;
+                        } else {
+                            H[k] = max(X[k], I);
+                        }
+                    }
+                    if (RECORD) {
+                        word_lo = (word_lo & ~(ins_lo >> 1)) | ins_lo;
+                        word_hi = (word_hi & ~(ins_hi >> 1)) | ins_hi;
+                        // Pass 3: an insertion run extends where the left cell's insertion layer beats its
+                        // score plus an opening; the left of place 0 is the previous lane's last place.
+                        int32_t leftH = __shfl_up_sync(kFull, H[C - 1], 1, G);
+                        int32_t leftI = __shfl_up_sync(kFull, X[C - 1], 1, G);
+                        if (member == 0) {
+                            leftH = kUnreached;
+                            leftI = kUnreached;
+                        }
+#pragma unroll
+                        for (int k = 0; k < C; ++k) {
+                            const int32_t lh = k == 0 ? leftH : H[k - 1];
+                            const int32_t li = k == 0 ? leftI : X[k - 1];
+                            const uint32_t bit = li > lh + opening ? 8u : 0u;
+                            if (k < 8)
+                                word_lo |= bit << (4 * k);
+                            else
+                                word_hi |= bit << (4 * (k - 8));
+                        }
+                        buffered[u & 3] = (uint64_t(word_hi) << 32) | word_lo;
+                        if (active && ((u & 3) == 3 || row == rows)) {
+                            uint4 *at = reinterpret_cast<uint4 *>(b.decisions + dec_base + ((row - 1) & ~3));
+                            at[0] = make_uint4(uint32_t(buffered[0]), uint32_t(buffered[0] >> 32),
+                                               uint32_t(buffered[1]), uint32_t(buffered[1] >> 32));
+                            at[1] = make_uint4(uint32_t(buffered[2]), uint32_t(buffered[2] >> 32),
+                                               uint32_t(buffered[3]), uint32_t(buffered[3] >> 32));
+                        }
+                    }
+                    if (active && row == rows) {
+#pragma unroll
+                        for (int k = 0; k < C; ++k)
+                            if (first_place + k == end_place) reported = H[k];
+                    }
+                }
+            }
+        }
+        // The corner's lane reports; the band's score is accepted when the band proves it.
+        const bool holder = live && end_place >= first_place && end_place < first_place + C;
+        if (holder) {
+            const int64_t score = (rows == 0 && cols == 0) ? 0 : int64_t(reported) + int64_t(rows + cols) * extend;
+            const bool proven = band_proves(score, rows, cols, low, b.best, open, extend);
+            b.scores[pair] = int32_t(score);
+            if (b.proven) b.proven[pair] = proven ? 1 : 0;
+            if (!proven) b.leftovers[atomicAdd(b.leftover_count, 1u)] = pair;
+        }
+    }
+}
+
+}  // namespace
+
+void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record) {
+    if (batch.count <= 0) return;
+    auto fn = record ? &banded_kernel<true> : &banded_kernel<false>;
+    int per_sm = 0;
+    DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+    const int64_t pairs_per_block = kBlock / kBandLanes;
+    int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
+    const int64_t needed = (batch.count + pairs_per_block - 1) / pairs_per_block;
+    if (blocks > needed) blocks = needed;
+    fn<<<unsigned(blocks), kBlock, 0, gpu->stream>>>(batch);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
+}
+
+}  // namespace dinara

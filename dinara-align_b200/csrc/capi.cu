@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "affine.cuh"
+#include "banded.cuh"
 #include "edit.cuh"
 #include "internal.cuh"
 #include "pack.cuh"
@@ -197,19 +198,13 @@ Packed pack_batch(dinara_gpu *gpu, int64_t pairs, const char *letters, const int
     return out;
 }
 
-void class_counts(int64_t first, int64_t count, const int64_t *offsets, bool record, int64_t counts[kAffineShapes]) {
-    for (int c = 0; c < kAffineShapes; ++c) counts[c] = 0;
-    for (int64_t p = first; p < first + count; ++p) {
-        const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-        const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-        const int cls = (rows == 0 || columns == 0) ? 0 : affine_shape_for(uint32_t(columns), record);
-        counts[cls] += 1;
-    }
-}
+// Device memory a launch's recorded decisions may take before the batch is cut into chunks.
+constexpr int64_t kDecisionBudget = int64_t(8) << 30;
 
 // The 64-bit words a pair's recorded decisions take (the layout affine.cu's record kernels write).
-int64_t record_words(int64_t rows, int64_t columns, bool uniform) {
+int64_t record_words(int64_t rows, int64_t columns, bool uniform, bool band) {
     if (rows <= 0 || columns <= 0) return 0;
+    if (band && band_eligible(uint32_t(rows), uint32_t(columns))) return int64_t(kBandLanes) * ((rows + 3) & ~int64_t(3));
     const int64_t lanes = record_lanes(uint32_t(columns), uniform);
     return (columns + lanes * 16 - 1) / (lanes * 16) * lanes * (((rows + 2) | 3) + 1);
 }
@@ -295,6 +290,7 @@ struct Timer {
         gpu->timing = true;
         gpu->kernel_ms = gpu->record_ms = 0.0;
         gpu->launches = 0;
+        gpu->swept_cells = 0;
     }
     void finish(dinara_timing *timing, int64_t cells) {
         DINARA_CUDA(cudaEventRecord(end, gpu->stream));
@@ -306,7 +302,7 @@ struct Timer {
             timing->kernel_ms = gpu->kernel_ms;
             timing->record_ms = gpu->record_ms;
             timing->launches = gpu->launches;
-            timing->cells = cells;
+            timing->cells = gpu->swept_cells > 0 ? gpu->swept_cells : cells;
         }
     }
     ~Timer() {
@@ -387,12 +383,9 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
         if (pairs == 0) return 0;
         DINARA_CUDA(cudaSetDevice(gpu->device));
         Packed packed = pack_batch(gpu, pairs, letters, offsets, checked.codes, checked.bits);
-        int64_t counts[kAffineShapes];
-        class_counts(0, pairs, offsets, false, counts);
-        const uint32_t *order = schedule(gpu, packed.shapes, 0, pairs, false);
         AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
         int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
-        affine_scores(gpu, batch, checked.table, scores_device, order, counts);
+        affine_scores(gpu, batch, checked.table, scores_device, 0, pairs);
         std::vector<uint8_t> unknown(static_cast<size_t>(pairs));
         to_host(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
         to_host(gpu, unknown.data(), packed.unknown, size_t(pairs));
@@ -438,9 +431,12 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
         AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
         int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
         // Chunks whose recorded decisions stay within a budget of device memory.
-        const int64_t budget_words = (int64_t(2) << 30) / 8;
+        const int64_t budget_words = kDecisionBudget / 8;
         const bool uniform = !checked.table.packed16 || checked.bits == 8;
-        std::vector<char> bytes;
+        const bool band = band_serves(batch, checked.table);
+        // Every chunk's CIGAR bytes go straight into the caller's buffer, grown a chunk at a time.
+        char *bytes = nullptr;
+        size_t size = 0;
         std::vector<int64_t> walk_spans(size_t(4 * pairs));
         std::vector<int64_t> ends(size_t(pairs + 1));
         ends[0] = 0;
@@ -451,21 +447,24 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
                 const int64_t p = first + count;
                 const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
                 const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                const int64_t w = record_words(rows, columns, uniform);
+                const int64_t w = record_words(rows, columns, uniform, band);
                 if (count > 0 && words + w > budget_words) break;
                 words += w;
                 ++count;
             }
-            int64_t counts[kAffineShapes];
-            class_counts(first, count, offsets, true, counts);
-            const uint32_t *order = schedule(gpu, packed.shapes, first, count, true);
             int64_t *spans_device = gpu->ranges.ensure<int64_t>(size_t(4 * count));
             const int64_t total = affine_alignments(gpu, batch, checked.table, eqx != 0, scores_device, spans_device,
-                                                    first, count, order, counts);
-            const size_t at = bytes.size();
-            bytes.resize(at + size_t(total));
+                                                    first, count);
+            const size_t at = size;
+            char *grown = static_cast<char *>(std::realloc(bytes, at + size_t(total) + 1));
+            if (!grown) {
+                std::free(bytes);
+                throw std::bad_alloc();
+            }
+            bytes = grown;
+            size = at + size_t(total);
             std::vector<int64_t> chunk_offsets(size_t(count + 1));
-            to_host(gpu, bytes.data() + at, gpu->cigar_bytes.as<char>(), size_t(total));
+            to_host(gpu, bytes + at, gpu->cigar_bytes.as<char>(), size_t(total));
             to_host(gpu, chunk_offsets.data(), gpu->cigar_offsets.as<int64_t>(), size_t(count + 1) * sizeof(int64_t));
             to_host(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
             DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
@@ -499,13 +498,13 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
             }
         }
         if (cigar_offsets) std::memcpy(cigar_offsets, ends.data(), size_t(pairs + 1) * sizeof(int64_t));
-        if (cigar_bytes) {
-            char *out = static_cast<char *>(std::malloc(bytes.size() + 1));
-            if (!out) throw std::bad_alloc();
-            if (!bytes.empty()) std::memcpy(out, bytes.data(), bytes.size());
-            out[bytes.size()] = 0;
-            *cigar_bytes = out;
-        }
+        if (!bytes) bytes = static_cast<char *>(std::malloc(1));
+        if (!bytes) throw std::bad_alloc();
+        bytes[size] = 0;
+        if (cigar_bytes)
+            *cigar_bytes = bytes;
+        else
+            std::free(bytes);
         return 0;
     });
 }
@@ -677,13 +676,11 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(r.pairs));
         const int64_t *offsets = r.offsets.data();
         if (!cigars) {
-            int64_t counts[kAffineShapes];
-            class_counts(0, r.pairs, offsets, false, counts);
-            const uint32_t *order = schedule(gpu, r.packed.shapes, 0, r.pairs, false);
-            affine_scores(gpu, batch, r.checked.table, scores_device, order, counts);
+            affine_scores(gpu, batch, r.checked.table, scores_device, 0, r.pairs);
         } else {
-            const int64_t budget_words = (int64_t(2) << 30) / 8;
+            const int64_t budget_words = kDecisionBudget / 8;
             const bool uniform = !r.checked.table.packed16 || r.checked.bits == 8;
+            const bool band = band_serves(batch, r.checked.table);
             int64_t first = 0;
             while (first < r.pairs) {
                 int64_t count = 0, words = 0;
@@ -691,17 +688,13 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
                     const int64_t p = first + count;
                     const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
                     const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                    const int64_t w = record_words(rows, columns, uniform);
+                    const int64_t w = record_words(rows, columns, uniform, band);
                     if (count > 0 && words + w > budget_words) break;
                     words += w;
                     ++count;
                 }
-                int64_t counts[kAffineShapes];
-                class_counts(first, count, offsets, true, counts);
-                const uint32_t *order = schedule(gpu, r.packed.shapes, first, count, true);
                 int64_t *spans_device = gpu->ranges.ensure<int64_t>(size_t(4 * count));
-                affine_alignments(gpu, batch, r.checked.table, eqx != 0, scores_device, spans_device, first, count,
-                                  order, counts);
+                affine_alignments(gpu, batch, r.checked.table, eqx != 0, scores_device, spans_device, first, count);
                 first += count;
             }
         }

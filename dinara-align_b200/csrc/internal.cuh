@@ -119,7 +119,8 @@ struct dinara_gpu {
     // Inputs and their packed form.
     dinara::DeviceBuffer letters, offsets, code_table, tape, shapes, flags;
     // Scheduling: bucket keys and the order pairs are taken in.
-    dinara::DeviceBuffer keys, keys_sorted, order, order_sorted, sort_scratch, ranges;
+    dinara::DeviceBuffer keys, keys_sorted, order, order_sorted, sort_scratch, ranges, class_counts, layouts,
+        leftovers, decisions_extra;
     // Outputs and per-launch scratch.
     dinara::DeviceBuffer scores, carry, decisions, decision_offsets, walk_out, cigar_slots, cigar_lengths,
         cigar_offsets, cigar_bytes, spans;
@@ -134,6 +135,7 @@ struct dinara_gpu {
     bool timing = false;
     double kernel_ms = 0.0, record_ms = 0.0;
     int64_t launches = 0;
+    int64_t swept_cells = 0;  // cells the sweeps updated (bands, whole matrices, leftovers)
     // The resident batch (capi.cu), if one is loaded.
     void *resident = nullptr;
     void (*resident_free)(void *) = nullptr;

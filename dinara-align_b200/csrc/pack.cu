@@ -5,6 +5,7 @@
 #include <cub/cub.cuh>
 
 #include "affine.cuh"
+#include "banded.cuh"
 #include "pack.cuh"
 
 namespace dinara {
@@ -61,23 +62,32 @@ __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int
     }
 }
 
-// Scheduling keys of pairs [first, first + count): shape class in the top bits, then strips of its
-// width, then rows, so a descending sort puts each class's longest pairs first and warps hold pairs of
-// like size.
-__global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count, int record,
-                                     uint32_t *__restrict__ keys, uint32_t *__restrict__ order) {
+// Scheduling keys: the pair's class in the top bits (the whole-matrix shape class, or the proven band,
+// the highest), then strips of its width, then rows, so a descending sort puts each class's longest pairs
+// first and warps hold pairs of like size. Counts each class.
+__global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ list,
+                                     int64_t first, int64_t count, int record, int band, uint32_t *__restrict__ keys,
+                                     uint32_t *__restrict__ order, unsigned int *__restrict__ class_counts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
-    const PairShape shape = shapes[first + k];
+    const uint32_t pair = list ? list[k] : uint32_t(first + k);
+    const PairShape shape = shapes[pair];
     const bool empty = shape.rows == 0 || shape.columns == 0;
-    const int cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);
-    const uint32_t width = uint32_t(affine_lanes(cls) * affine_columns(cls));
-    uint32_t strips = empty ? 0 : (shape.columns + width - 1) / width;
-    if (strips > 255) strips = 255;
+    int cls;
+    uint32_t strips = 0;
+    if (band && band_eligible(shape.rows, shape.columns)) {
+        cls = kBandClass;
+    } else {
+        cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);
+        const uint32_t width = uint32_t(affine_lanes(cls) * affine_columns(cls));
+        strips = empty ? 0 : (shape.columns + width - 1) / width;
+        if (strips > 255) strips = 255;
+    }
     uint32_t rows = shape.rows >> 2;
     if (rows > 0xFFFFFu) rows = 0xFFFFFu;
     keys[k] = (uint32_t(cls) << 28) | (strips << 20) | rows;
-    order[k] = uint32_t(first + k);
+    order[k] = pair;
+    atomicAdd(&class_counts[cls], 1u);
 }
 
 void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
@@ -90,22 +100,35 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
     DINARA_CUDA(cudaGetLastError());
 }
 
-const uint32_t *schedule(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool record) {
+Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
+                   bool record, bool band) {
+    Schedule out;
+    for (int c = 0; c < kClasses; ++c) out.counts[c] = 0;
+    out.order = nullptr;
+    if (count <= 0) return out;
     uint32_t *keys = gpu->keys.ensure<uint32_t>(count);
     uint32_t *order = gpu->order.ensure<uint32_t>(count);
     uint32_t *keys_out = gpu->keys_sorted.ensure<uint32_t>(count);
     uint32_t *order_out = gpu->order_sorted.ensure<uint32_t>(count);
+    unsigned int *class_counts = gpu->class_counts.ensure<unsigned int>(kClasses);
+    DINARA_CUDA(cudaMemsetAsync(class_counts, 0, kClasses * sizeof(unsigned int), gpu->stream));
     const int threads = 256;
     schedule_keys_kernel<<<unsigned((count + threads - 1) / threads), threads, 0, gpu->stream>>>(
-        shapes, first, count, record ? 1 : 0, keys, order);
+        shapes, list, first, count, record ? 1 : 0, band ? 1 : 0, keys, order, class_counts);
     DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
     size_t scratch = 0;
     DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, scratch, keys, keys_out, order, order_out,
                                                           int(count), 0, 32, gpu->stream));
     void *space = gpu->sort_scratch.ensure<uint8_t>(scratch);
     DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(space, scratch, keys, keys_out, order, order_out,
                                                           int(count), 0, 32, gpu->stream));
-    return order_out;
+    unsigned int host_counts[kClasses];
+    DINARA_CUDA(cudaMemcpyAsync(host_counts, class_counts, sizeof host_counts, cudaMemcpyDeviceToHost, gpu->stream));
+    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    for (int c = 0; c < kClasses; ++c) out.counts[c] = host_counts[c];
+    out.order = order_out;
+    return out;
 }
 
 }  // namespace dinara

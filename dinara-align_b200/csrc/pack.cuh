@@ -11,8 +11,18 @@ namespace dinara {
 void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
                 const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown);
 
-// The order pairs [first, first + count) are swept in: by shape class (affine_shape_for with
-// `record`), descending, then strips and rows, descending (device; valid until the next call).
-const uint32_t *schedule(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool record);
+// A batch's sweep order: pairs by class (the whole-matrix shape classes 0-4, affine_shape_for with
+// `record`, and with `band` the proven band, kBandClass), classes in descending order, then strips and rows
+// descending. `order` is valid on the device until the next call.
+constexpr int kClasses = 6;
+constexpr int kBandClass = 5;
+struct Schedule {
+    const uint32_t *order;
+    int64_t counts[kClasses];
+};
+
+// The order of pairs [first, first + count), or of the `count` pairs listed in `list` (device) when given.
+Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
+                  bool record, bool band);
 
 }  // namespace dinara

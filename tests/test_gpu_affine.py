@@ -167,3 +167,36 @@ def test_refusals(da):
     huge = da.Scoring.uniform(2, -4, -4, -100000)
     _, statuses = da.scores_tape(da.Tape.of(["A" * 3000], ["A" * 3000]), huge, statuses=True)
     assert list(statuses) == [-3]
+
+
+@pytest.mark.parametrize("scoring_name", ["config2", "dna"])
+def test_band_proofs_and_leftovers(da, oracle, scoring_name):
+    """Global pairs the proven band serves and pairs it leaves to the whole matrix: error rates from 0 to
+    40%, length differences up to and past the band's 63 diagonals, long pairs; scores and CIGARs must
+    equal the whole-matrix oracle's either way."""
+    from dinara_align import workloads
+
+    rng = np.random.default_rng(41)
+    scoring = da.Scoring.uniform(0, -4, -6, -2) if scoring_name == "config2" else da.Scoring.dna()
+    tapes = []
+    for rate in (0.0, 0.02, 0.1, 0.25, 0.4):
+        tapes.append(workloads.pairs_with_errors(rng, rng.integers(20, 700, size=120), rate,
+                                                 workloads.HALF_QUARTERS))
+    refs, queries = [], []
+    for tape in tapes:
+        for p in range(tape.pairs):
+            refs.append(tape.reference(p).decode())
+            queries.append(tape.query(p).decode())
+    for extra in (30, 31, 32, 60, 62, 63, 64, 65, 90):
+        a = "".join(rng.choice(list("ACGT"), size=300))
+        refs.append(a)
+        queries.append(a[: 300 - extra] if extra % 2 else a + "".join(rng.choice(list("ACGT"), size=extra)))
+    a = "".join(rng.choice(list("ACGT"), size=4000))
+    refs.append(a)
+    queries.append(a[:1000] + a[1100:])
+    tape = da.Tape.of(refs, queries)
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, scoring, False, True)
+    assert da.scores(refs, queries, scoring) == list(expected_scores)
+    found = da.alignments(refs, queries, scoring)
+    assert [a.score for a in found] == list(expected_scores)
+    assert [a.cigar for a in found] == expected_cigars
