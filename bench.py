@@ -135,7 +135,7 @@ def reference_arm(args) -> None:
 def cpu_measure(oracle, workload: str, threads: int, steps: int, warmup: int) -> dict:
     """The oracle timed on `threads` host threads over a bounded sample of the workload: pairs/s."""
     # Sized for roughly 10-30 s of CPU work on a 16-core host.
-    sample_pairs = {"affine": 400_000, "local": 400, "uneven": 2_000, "unit250": 10_000}[workload]
+    sample_pairs = {"affine": 400_000, "local": 20_000, "uneven": 40_000, "unit250": 10_000}[workload]
     tape = make_workload(workload, sample_pairs, seed=1000)
     letters = tape.letters[: tape.offsets[-1]]
     if workload in ("affine", "local"):
@@ -234,6 +234,8 @@ def main() -> None:
                                         None if unit else ctypes.byref(struct))
     native.check(code, handle)
 
+    band_report = {}
+
     def step() -> Timing:
         timing = Timing()
         if unit:
@@ -241,6 +243,7 @@ def main() -> None:
             report = native.CBandReport()
             native.check(lib.dinara_gpu_resident_distances(handle, ctypes.byref(plan), ctypes.byref(report),
                                                            ctypes.byref(timing)), handle)
+            band_report.update({name: getattr(report, name) for name, _ in native.CBandReport._fields_})
         else:
             native.check(lib.dinara_gpu_resident_align(handle, ctypes.byref(mode_struct), 1 if args.workload ==
                                                        "affine" else 0, 1, ctypes.byref(timing)), handle)
@@ -348,6 +351,8 @@ def main() -> None:
                            "roofline_frac": achieved / (2 * peaks["viaddmax"]),
                            "achieved_gops": achieved / 1e9})
             line["scorer"] = scorer
+        if band_report:
+            line["band_report"] = band_report
         line["int32_peaks_instr_per_s"] = peaks
         if not args.no_cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))

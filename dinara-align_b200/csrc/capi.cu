@@ -1,6 +1,7 @@
 // The C ABI (include/dinara_gpu.h): checks what the reference checks, moves the caller's letters to the
 // device, packs and schedules them there, runs the kernels and brings the results back.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <new>
@@ -11,6 +12,7 @@
 #include "banded.cuh"
 #include "edit.cuh"
 #include "internal.cuh"
+#include "learned.cuh"
 #include "pack.cuh"
 
 using namespace dinara;
@@ -329,6 +331,11 @@ dinara_gpu *dinara_gpu_new(int64_t device) {
         DINARA_CUDA(cudaStreamCreateWithFlags(&gpu->stream, cudaStreamNonBlocking));
         DINARA_CUDA(cudaEventCreate(&gpu->start));
         DINARA_CUDA(cudaEventCreate(&gpu->stop));
+        DINARA_CUDA(cudaEventCreateWithFlags(&gpu->fork, cudaEventDisableTiming));
+        for (int k = 0; k < dinara_gpu::kSideStreams; ++k) {
+            DINARA_CUDA(cudaStreamCreateWithFlags(&gpu->side[k], cudaStreamNonBlocking));
+            DINARA_CUDA(cudaEventCreateWithFlags(&gpu->joins[k], cudaEventDisableTiming));
+        }
         return gpu;
     } catch (const std::exception &error) {
         new_error = error.what();
@@ -357,6 +364,11 @@ void dinara_gpu_free(dinara_gpu *gpu) {
     gpu->pinned_small.release();
     if (gpu->start) cudaEventDestroy(gpu->start);
     if (gpu->stop) cudaEventDestroy(gpu->stop);
+    if (gpu->fork) cudaEventDestroy(gpu->fork);
+    for (int k = 0; k < dinara_gpu::kSideStreams; ++k) {
+        if (gpu->side[k]) cudaStreamDestroy(gpu->side[k]);
+        if (gpu->joins[k]) cudaEventDestroy(gpu->joins[k]);
+    }
     if (gpu->stream) cudaStreamDestroy(gpu->stream);
     delete gpu;
 }
@@ -741,6 +753,142 @@ int64_t dinara_gpu_resident_fetch(dinara_gpu *gpu, int32_t *scores, int64_t *dis
         if (r.last == 1 && scores) to_host(gpu, scores, gpu->scores.as<int32_t>(), size_t(r.pairs) * sizeof(int32_t));
         if (r.last == 2 && distances)
             to_host(gpu, distances, gpu->scores.as<int64_t>(), size_t(r.pairs) * sizeof(int64_t));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        return 0;
+    });
+}
+
+namespace {
+
+// A tape's letters and offsets (rebased to its first letter) on the device.
+void upload_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets, const uint8_t **letters_out,
+                 const int64_t **offsets_out) {
+    const int64_t first = offsets[0];
+    const int64_t total = offsets[2 * pairs] - first;
+    std::vector<int64_t> relative(size_t(2 * pairs + 1));
+    for (int64_t k = 0; k <= 2 * pairs; ++k) relative[size_t(k)] = offsets[k] - first;
+    uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
+    int64_t *offsets_device = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
+    to_device(gpu, letters_device, letters + first, size_t(total), gpu->pinned_in);
+    to_device(gpu, offsets_device, relative.data(), relative.size() * sizeof(int64_t), gpu->pinned_small);
+    *letters_out = letters_device;
+    *offsets_out = offsets_device;
+}
+
+}  // namespace
+
+int64_t dinara_gpu_predictor_train(dinara_gpu *gpu, const dinara_train_options *options, dinara_train_report *report) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !options) throw Failure(DINARA_INVALID_MODE, "no context or options");
+        if (options->pairs < 100 || options->batch < 16 || options->batch > 65536 || options->epochs < 1 ||
+            options->length_low < 1 || options->length_high < options->length_low || options->rate_low < 0 ||
+            options->rate_high < options->rate_low || options->rate_high > 1 || options->learning_rate <= 0)
+            throw Failure(DINARA_INVALID_MODE, "training options out of range");
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        dinara_train_report local;
+        std::memset(&local, 0, sizeof local);
+        const auto begin = std::chrono::steady_clock::now();
+        predictor_train(gpu, *options, local);
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        local.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+        if (report) *report = local;
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_set(dinara_gpu *gpu, const float *parameters, double margin, double slack) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !parameters) throw Failure(DINARA_INVALID_MODE, "no context or parameters");
+        if (!(margin >= 0.0) || !(slack >= 0.0)) throw Failure(DINARA_INVALID_MODE, "a negative margin or slack");
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        float *weights = gpu->weights.ensure<float>(kPredictorParameters);
+        DINARA_CUDA(cudaMemcpyAsync(weights, parameters, kPredictorParameters * sizeof(float), cudaMemcpyHostToDevice,
+                                    gpu->stream));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        gpu->predictor_margin = margin;
+        for (int k = 0; k < 4; ++k) gpu->predictor_margins[k] = margin;
+        gpu->predictor_slack = slack;
+        gpu->predictor_ready = true;
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_get(dinara_gpu *gpu, float *parameters, double *margin, double *slack) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !gpu->predictor_ready) throw Failure(DINARA_INVALID_MODE, "no trained band predictor on this context");
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        if (parameters) {
+            DINARA_CUDA(cudaMemcpyAsync(parameters, gpu->weights.as<float>(), kPredictorParameters * sizeof(float),
+                                        cudaMemcpyDeviceToHost, gpu->stream));
+            DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        }
+        if (margin) *margin = gpu->predictor_margin;
+        if (slack) *slack = gpu->predictor_slack;
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_features(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                      float *features) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+        check_offsets(pairs, offsets);
+        if (pairs == 0) return 0;
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        const uint8_t *letters_device;
+        const int64_t *offsets_device;
+        upload_tape(gpu, pairs, letters, offsets, &letters_device, &offsets_device);
+        float *matrix = gpu->features.ensure<float>(size_t(pairs) * kPredictorInputs);
+        predictor_features(gpu, pairs, letters_device, offsets_device, matrix);
+        std::vector<float> host(size_t(pairs) * kPredictorInputs);
+        to_host(gpu, host.data(), matrix, host.size() * sizeof(float));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        for (int64_t p = 0; p < pairs; ++p)
+            for (int f = 0; f < kPredictorInputs; ++f)
+                features[p * kPredictorInputs + f] = host[size_t(int64_t(f) * pairs + p)];
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_gradients(dinara_gpu *gpu, int64_t batch, const float *features, const float *targets,
+                                       float *gradients, double *loss) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !gpu->predictor_ready) throw Failure(DINARA_INVALID_MODE, "no parameters on this context");
+        if (batch < 1 || batch > 65536) throw Failure(DINARA_INVALID_LENGTH, "a batch of 1 to 65,536 samples");
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        std::vector<float> matrix(size_t(batch) * kPredictorInputs);
+        for (int64_t s = 0; s < batch; ++s)
+            for (int f = 0; f < kPredictorInputs; ++f)
+                matrix[size_t(int64_t(f) * batch + s)] = features[s * kPredictorInputs + f];
+        float *x = gpu->features.ensure<float>(matrix.size());
+        float *t = gpu->targets.ensure<float>(size_t(batch));
+        float *g = gpu->gradients.ensure<float>(kPredictorParameters);
+        float *l = gpu->counters.ensure<float>(64) + 60;
+        DINARA_CUDA(cudaMemcpyAsync(x, matrix.data(), matrix.size() * sizeof(float), cudaMemcpyHostToDevice, gpu->stream));
+        DINARA_CUDA(cudaMemcpyAsync(t, targets, size_t(batch) * sizeof(float), cudaMemcpyHostToDevice, gpu->stream));
+        predictor_gradients(gpu, int(batch), x, t, g, l);
+        float summed = 0.f;
+        to_host(gpu, gradients, g, kPredictorParameters * sizeof(float));
+        to_host(gpu, &summed, l, sizeof summed);
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        if (loss) *loss = double(summed) / double(batch);
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_predict(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                     float *predicted, int64_t *thresholds) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+        check_offsets(pairs, offsets);
+        if (pairs == 0) return 0;
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        const uint8_t *letters_device;
+        const int64_t *offsets_device;
+        upload_tape(gpu, pairs, letters, offsets, &letters_device, &offsets_device);
+        const int64_t *starts = predict_thresholds(gpu, pairs, letters_device, offsets_device);
+        if (thresholds) to_host(gpu, thresholds, starts, size_t(pairs) * sizeof(int64_t));
+        if (predicted) to_host(gpu, predicted, gpu->targets.as<float>(), size_t(pairs) * sizeof(float));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         return 0;
     });

@@ -17,6 +17,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "edit.cuh"
@@ -71,14 +72,6 @@ struct BandArgs {
     unsigned long long *swept;
 };
 
-// The window's first word at column c (c >= 1): the band's first row's word, held at most `last` so
-// the window stays inside the pattern.
-__device__ __forceinline__ int window_base(int c, int delta, int64_t e, int last) {
-    int64_t low = int64_t(c) - delta - e;
-    if (low < 1) low = 1;
-    int base = int((low - 1) >> 6);
-    return base < last ? base : last;
-}
 
 template <int G, int K>
 __global__ void __launch_bounds__(kBlock) band_kernel(BandArgs a) {
@@ -105,9 +98,12 @@ __global__ void __launch_bounds__(kBlock) band_kernel(BandArgs a) {
         const int words = info.words;
         const int delta = m - n;
         if (t < delta) t = delta;
-        const int64_t e = (t - delta) / 2;
+        const int64_t half = (t - delta) / 2;
+        const int e = int(half < int64_t(n) + m ? half : int64_t(n) + m);
         const int last = words > W ? words - W : 0;
-        const int final_base = live ? window_base(m, delta, e, last) : 0;
+        // The window's first word at column c is min(max(c - delta - e - 1, 0) / 64, last): it slides at
+        // columns delta + e + 1 + 64 k, k = 1 .. last, known in advance.
+        const int final_base = live ? min(max(m - delta - e - 1, 0) >> 6, last) : 0;
         // Lane m takes column c at step c + m + base(c): one stall for each word the window slides.
         const int steps = live ? m + G - 1 + final_base : 0;
         int warp_steps = steps;
@@ -117,24 +113,26 @@ __global__ void __launch_bounds__(kBlock) band_kernel(BandArgs a) {
         const uint8_t *text = a.letters + info.text;
         const uint8_t *pattern = a.letters + info.pattern;
         const bool dna = info.dna != 0;
-        const uint64_t *planes = dna && live ? a.planes + a.plane_offsets[pair] : nullptr;
+        // This lane's words: base + member * K + i; `mine` points at the first one's four planes.
+        const uint64_t *mine = dna && live ? a.planes + a.plane_offsets[pair] + 4 * int64_t(member * K) : nullptr;
+        int held = words - member * K;  // words of this lane's K that lie inside the pattern
         uint64_t P[K], M[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             P[i] = ~0ull;
             M[i] = 0ull;
         }
-        int64_t above = 0;  // lane 0: the score of the row above the window
-        int base = 0;       // the window's first word at this lane's last column
+        int above = 0;  // lane 0: the score of the row above the window
+        int base = 0;   // the window's first word at this lane's last column
+        int next_slide = last > 0 ? delta + e + 1 + 64 : INT_MAX;
         int next_col = 1;
-        int next_time = 1 + member;
+        int next_time = 1 + member + (next_slide == 1 ? 1 : 0);
+        uint32_t letter = live && m > 0 ? __ldg(text) : 0u;
         int hout = 0;
         for (int step = 1; step <= warp_steps; ++step) {
             const int from_above = __shfl_up_sync(kFull, hout, 1, G);
             const bool due = live && next_col <= m && step == next_time;
-            int new_base = base;
-            if (due) new_base = window_base(next_col, delta, e, last);
-            const bool slides = due && new_base > base;
+            const bool slides = due && next_col == next_slide;
             uint64_t belowP = 0, belowM = 0;
             if (G > 1 && __any_sync(kFull, slides)) {
                 belowP = shfl_down64(P[0], G);
@@ -156,22 +154,26 @@ __global__ void __launch_bounds__(kBlock) band_kernel(BandArgs a) {
                         P[K - 1] = belowP;
                         M[K - 1] = belowM;
                     }
-                    base = new_base;
+                    base += 1;
+                    held -= 1;
+                    mine += 4;
+                    next_slide = base < last ? next_slide + 64 : INT_MAX;
                 }
-                const uint32_t letter = text[c - 1];
+                const uint32_t here = letter;
+                if (c < m) letter = __ldg(text + c);  // the next column's letter, early
                 int carry = member == 0 ? 1 : from_above;
+                const uint32_t code = dna_code(here);
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    const int w = base + member * K + i;
-                    if (w < words) {
+                    if (i < held) {
                         uint64_t eq;
                         if (dna) {
-                            eq = __ldg(planes + 4 * int64_t(w) + dna_code(letter));
+                            eq = __ldg(mine + 4 * i + code);
                         } else {
                             eq = 0;
-                            const int first = w * 64;
+                            const int first = (base + member * K + i) * 64;
                             const int count = min(64, n - first);
-                            for (int j = 0; j < count; ++j) eq |= uint64_t(pattern[first + j] == letter) << j;
+                            for (int j = 0; j < count; ++j) eq |= uint64_t(pattern[first + j] == here) << j;
                         }
                         carry = myers_word(eq, P[i], M[i], carry);
                     }
@@ -179,13 +181,11 @@ __global__ void __launch_bounds__(kBlock) band_kernel(BandArgs a) {
                 hout = carry;
                 if (member == 0) above += 1;
                 next_col = c + 1;
-                int slide_next = 0;
-                if (next_col <= m) slide_next = window_base(next_col, delta, e, last) > base ? 1 : 0;
-                next_time = step + 1 + slide_next;
+                next_time = step + 1 + (next_col == next_slide ? 1 : 0);
             }
         }
         // The distance: the row above the window plus every vertical step down to the pattern's last row.
-        int64_t sum = member == 0 ? above : 0;
+        int64_t sum = member == 0 ? int64_t(above) : 0;
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             const int w = base + member * K + i;
@@ -333,13 +333,21 @@ BandFn pick_band(int shape) {
     switch (shape) {
         case 0: return &band_kernel<1, 1>;
         case 1: return &band_kernel<1, 2>;
-        case 2: return &band_kernel<1, 4>;
-        case 3: return &band_kernel<4, 2>;
-        case 4: return &band_kernel<8, 2>;
-        case 5: return &band_kernel<16, 2>;
-        case 6: return &band_kernel<32, 2>;
-        case 7: return &band_kernel<32, 4>;
-        case 8: return &band_kernel<32, 8>;
+        case 2: return &band_kernel<1, 3>;
+        case 3: return &band_kernel<1, 4>;
+        case 4: return &band_kernel<2, 3>;
+        case 5: return &band_kernel<4, 2>;
+        case 6: return &band_kernel<4, 3>;
+        case 7: return &band_kernel<8, 2>;
+        case 8: return &band_kernel<8, 3>;
+        case 9: return &band_kernel<16, 2>;
+        case 10: return &band_kernel<16, 3>;
+        case 11: return &band_kernel<32, 2>;
+        case 12: return &band_kernel<32, 3>;
+        case 13: return &band_kernel<32, 4>;
+        case 14: return &band_kernel<32, 6>;
+        case 15: return &band_kernel<32, 8>;
+        case 16: return &band_kernel<32, 12>;
         default: return &band_kernel<32, 16>;
     }
 }
@@ -427,6 +435,11 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
                                     cudaMemcpyDeviceToHost, stream));
         DINARA_CUDA(cudaStreamSynchronize(stream));
         DINARA_CUDA(cudaEventRecord(gpu->start, stream));
+        // Each shape's launch on a side stream, all forked from and joined back to the context's stream:
+        // a launch lasts as long as its longest pair, so running the shapes at once overlaps those tails.
+        DINARA_CUDA(cudaEventRecord(gpu->fork, stream));
+        bool used[dinara_gpu::kSideStreams] = {false};
+        int next_side = 0;
         // Shapes in descending order, as the keys sort them.
         int64_t at = 0;
         for (int shape = kBandShapes - 1; shape >= 0; --shape) {
@@ -451,10 +464,19 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
             int64_t grid = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
             const int64_t needed = (n_shape + groups_per_block - 1) / groups_per_block;
             if (grid > needed) grid = needed;
-            fn<<<unsigned(grid), kBlock, 0, stream>>>(args);
+            const int side = next_side;
+            next_side = (next_side + 1) % dinara_gpu::kSideStreams;
+            if (!used[side]) DINARA_CUDA(cudaStreamWaitEvent(gpu->side[side], gpu->fork, 0));
+            used[side] = true;
+            fn<<<unsigned(grid), kBlock, 0, gpu->side[side]>>>(args);
             DINARA_CUDA(cudaGetLastError());
             at += n_shape;
             ++launches;
+        }
+        for (int side = 0; side < dinara_gpu::kSideStreams; ++side) {
+            if (!used[side]) continue;
+            DINARA_CUDA(cudaEventRecord(gpu->joins[side], gpu->side[side]));
+            DINARA_CUDA(cudaStreamWaitEvent(stream, gpu->joins[side], 0));
         }
         DINARA_CUDA(cudaEventRecord(gpu->stop, stream));
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned int), stream));

@@ -18,15 +18,18 @@ struct EditPair {
     int32_t words;  // ceil(n / 64)
 };
 
-constexpr int kBandShapes = 10;
+constexpr int kBandShapes = 18;
+// Window shapes (lanes x 64-bit words a lane), narrowest first: 1 to 512 words, each at most half again
+// the last, so a tight first threshold gets a tight window.
 __host__ __device__ inline int band_lanes(int shape) {
-    const int lanes[kBandShapes] = {1, 1, 1, 4, 8, 16, 32, 32, 32, 32};
+    const int lanes[kBandShapes] = {1, 1, 1, 1, 2, 4, 4, 8, 8, 16, 16, 32, 32, 32, 32, 32, 32, 32};
     return lanes[shape];
 }
 __host__ __device__ inline int band_words_per_lane(int shape) {
-    const int words[kBandShapes] = {1, 2, 4, 2, 2, 2, 2, 4, 8, 16};
+    const int words[kBandShapes] = {1, 2, 3, 4, 3, 2, 3, 2, 3, 2, 3, 2, 3, 4, 6, 8, 12, 16};
     return words[shape];
 }
+
 // The narrowest window (lanes x words) that covers the band of threshold t: every cell of diagonal d
 // with |d| + |d - delta| <= t, at most delta + 2e + 1 rows a column, e = (t - delta) / 2.
 __host__ __device__ inline int band_shape_for(int64_t n, int64_t m, int64_t t) {

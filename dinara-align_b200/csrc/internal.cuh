@@ -115,6 +115,10 @@ struct dinara_gpu {
     char name[256] = {0};
     cudaStream_t stream = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
+    // Side streams that let a round's launches of different shapes run at once, joined by events.
+    static constexpr int kSideStreams = 8;
+    cudaStream_t side[kSideStreams] = {nullptr};
+    cudaEvent_t fork = nullptr, joins[kSideStreams] = {nullptr};
     std::string error;
     // Inputs and their packed form.
     dinara::DeviceBuffer letters, offsets, code_table, tape, shapes, flags;
@@ -129,7 +133,9 @@ struct dinara_gpu {
     // Learned band predictor.
     dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations;
     bool predictor_ready = false;
-    double predictor_margin = 1.25;
+    double predictor_margin = 1.25;    // the largest of the classes' margins (reported)
+    double predictor_margins[4] = {1.25, 1.25, 1.25, 1.25};  // by mean length: < 300, < 1000, < 4096, more
+    double predictor_slack = 0.0;
     dinara::PinnedBuffer pinned_in, pinned_out, pinned_small;
     // Device timing of the sweep kernels, accumulated while `timing` is set.
     bool timing = false;

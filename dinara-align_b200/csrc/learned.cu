@@ -1,14 +1,626 @@
-// The learned band predictor (placeholder until its kernels land).
+// The learned band: a small network that reads a pair's 4-mer sketch and predicts its edit distance, so
+// band doubling starts near the answer instead of at the default threshold (band.mojo:521 starts an
+// untrusted band 256 past what it knows). The network is 257 -> 64 -> 64 -> 1, fp32, ReLU: its input the
+// 256 counts of each 4-mer in the reference less those in the query, over the pair's mean length, and
+// the length ratio; its output the distance over the mean length. Nothing about the answer depends on
+// it: a low guess costs extra doublings, a high one a wider band, and the doubling that follows is the
+// reference's.
+//
+// Everything runs on the device and is written here: a generator of training pairs (the benchmark's
+// uneven distribution, from a counter-based hash so the lengths pass and the letters pass agree), their
+// exact distances by the band kernels, the sketch, the training step (tiled fp32 products forward and
+// back, Adam), and inference inside the scheduling kernel that sets each pair's first threshold.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "edit.cuh"
+#include "learned.cuh"
 
 namespace dinara {
 
+namespace {
+
+constexpr int kIn = kPredictorInputs, kH = kPredictorHidden;
+// The parameters' room in the inference kernel's shared memory, rounded up to 4 floats.
+constexpr int kParamsRoom = (kPredictorParameters + 3) & ~3;
+
+// ------------------------------------------------------------------------------------------------
+// Counter-based randomness
+// ------------------------------------------------------------------------------------------------
+
+__host__ __device__ inline uint64_t mix64(uint64_t x) {
+    // SplitMix64's finalizer (Steele, Lea and Flood, 2014).
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+__host__ __device__ inline uint64_t draw(uint64_t seed, uint64_t pair, uint64_t index) {
+    return mix64(seed ^ mix64(pair * 0x9e3779b97f4a7c15ull + index * 0xd1b54a32d192ed03ull + 0x632be59bd9b4e019ull));
+}
+
+__host__ __device__ inline double unit(uint64_t h) { return double(h >> 11) * (1.0 / 9007199254740992.0); }
+
+struct PairDraw {
+    int64_t length;
+    double rate;
+};
+
+// A pair's reference length (log-uniform) and error rate (uniform).
+__device__ inline PairDraw pair_draw(uint64_t seed, uint64_t pair, double low, double high, double rate_low,
+                                     double rate_high) {
+    const double u = unit(draw(seed, pair, 0));
+    const double v = unit(draw(seed, pair, 1));
+    PairDraw d;
+    d.length = int64_t(llround(exp(log(low) + u * (log(high) - log(low)))));
+    d.rate = rate_low + v * (rate_high - rate_low);
+    return d;
+}
+
+// Letter i's fate: 0 kept, 1 substituted, 2 deleted, 3 kept with a letter inserted after it (50/25/25).
+__device__ inline int fate(uint64_t h, double rate) {
+    const double roll = unit(h);
+    if (roll < rate * 0.5) return 1;
+    if (roll < rate * 0.75) return 2;
+    if (roll < rate) return 3;
+    return 0;
+}
+
+__global__ void generate_lengths_kernel(uint64_t seed, int64_t pairs, double low, double high, double rate_low,
+                                        double rate_high, int64_t *lengths) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= pairs) return;
+    const PairDraw d = pair_draw(seed, uint64_t(p), low, high, rate_low, rate_high);
+    int64_t b = 0;
+    for (int64_t i = 0; i < d.length; ++i) {
+        const int f = fate(draw(seed, uint64_t(p), uint64_t(i) + 16), d.rate);
+        b += f == 2 ? 0 : (f == 3 ? 2 : 1);
+    }
+    lengths[2 * p] = d.length;
+    lengths[2 * p + 1] = b;
+}
+
+__global__ void generate_letters_kernel(uint64_t seed, int64_t pairs, double low, double high, double rate_low,
+                                        double rate_high, const int64_t *offsets, uint8_t *letters) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= pairs) return;
+    const PairDraw d = pair_draw(seed, uint64_t(p), low, high, rate_low, rate_high);
+    const char *acgt = "ACGT";
+    uint8_t *a = letters + offsets[2 * p];
+    uint8_t *b = letters + offsets[2 * p + 1];
+    int64_t at = 0;
+    for (int64_t i = 0; i < d.length; ++i) {
+        const uint64_t h = draw(seed, uint64_t(p), uint64_t(i) + 16);
+        const uint32_t letter = uint32_t(h) & 3u;
+        a[i] = uint8_t(acgt[letter]);
+        const int f = fate(h, d.rate);
+        if (f == 1) {
+            b[at++] = uint8_t(acgt[(letter + 1 + (uint32_t(h >> 2) % 3u)) & 3u]);
+        } else if (f == 0) {
+            b[at++] = uint8_t(acgt[letter]);
+        } else if (f == 3) {
+            b[at++] = uint8_t(acgt[letter]);
+            b[at++] = uint8_t(acgt[uint32_t(h >> 4) & 3u]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// The sketch
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ int base_code(uint32_t byte) {
+    switch (byte) {
+        case 'A': return 0;
+        case 'C': return 1;
+        case 'G': return 2;
+        case 'T': return 3;
+        default: return -1;
+    }
+}
+
+// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints), `sign` +1 or -1: each lane
+// takes a stretch, rolling its 4-mer across letters; a k-mer holding another letter is skipped.
+__device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, int *counts) {
+    const int lane = threadIdx.x & 31;
+    const int64_t stretch = (length + 31) / 32;
+    const int64_t begin = lane * stretch, end = min(length, begin + stretch);
+    // The k-mers starting in [begin, end) each need the 3 letters after them.
+    int valid = 0;
+    uint32_t code = 0;
+    for (int64_t i = begin - 3 < 0 ? 0 : begin - 3; i < end + 3 && i < length; ++i) {
+        const int c = base_code(sequence[i]);
+        if (c < 0) {
+            valid = 0;
+            code = 0;
+            continue;
+        }
+        code = ((code << 2) | uint32_t(c)) & 0xFFu;
+        valid = valid < 4 ? valid + 1 : 4;
+        const int64_t start = i - 3;
+        if (valid == 4 && start >= begin && start < end) atomicAdd(&counts[code], sign);
+    }
+}
+
+// Writes a pair's 257 features, scaled as the network reads them: the count differences over the root of
+// the mean length, since each error moves a handful of 4-mers between bins and the differences' squares
+// then sum to about the errors a letter whatever the length; and the length ratio.
+__device__ void features_of(const int *counts, int64_t reference, int64_t query, float *out, int stride) {
+    const int lane = threadIdx.x & 31;
+    const float mean = 0.5f * float(reference + query);
+    const float scale = rsqrtf(mean > 1.0f ? mean : 1.0f);
+    for (int k = lane; k < 256; k += 32) out[int64_t(k) * stride] = float(counts[k]) * scale;
+    if (lane == 0) {
+        const int64_t low = min(reference, query), high = max(reference, query);
+        out[int64_t(256) * stride] = high > 0 ? float(low) / float(high) : 1.0f;
+    }
+}
+
+// A warp a pair: the features into a feature-major matrix (feature f of pair p at f * pairs + p).
+__global__ void features_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs, float *features) {
+    __shared__ int counts[8][256];
+    const int warp_in_block = threadIdx.x >> 5;
+    const int64_t pair = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp_in_block;
+    const int lane = threadIdx.x & 31;
+    int *mine = counts[warp_in_block];
+    for (int k = lane; k < 256; k += 32) mine[k] = 0;
+    __syncwarp();
+    if (pair < pairs) {
+        const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
+        count_kmers(letters + r0, q0 - r0, 1, mine);
+        count_kmers(letters + q0, q1 - q0, -1, mine);
+    }
+    __syncwarp();
+    if (pair < pairs) features_of(mine, offsets[2 * pair + 1] - offsets[2 * pair],
+                                  offsets[2 * pair + 2] - offsets[2 * pair + 1], features + pair, int(pairs));
+}
+
+// ------------------------------------------------------------------------------------------------
+// Training: tiled fp32 products
+// ------------------------------------------------------------------------------------------------
+
+// C[m x n] (+)= op(A)[m x k] * op(B)[k x n], all row-major with leading dimensions; op transposes when
+// asked. A 64 x 64 tile a block of 256 threads, 4 x 4 outputs a thread, k in steps of 16 through shared
+// memory. `accumulate` adds to C; `bias` (length m) and `relu` finish the tile when given.
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) product_kernel(int m, int n, int k, const float *A, int lda, const float *B,
+                                                      int ldb, float *C, int ldc, const float *bias, bool relu,
+                                                      bool accumulate) {
+    __shared__ float As[16][64 + 1];
+    __shared__ float Bs[16][64 + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int row0 = blockIdx.y * 64, col0 = blockIdx.x * 64;
+    float acc[4][4] = {{0.f}};
+    for (int kk = 0; kk < k; kk += 16) {
+        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+            const int kq = e / 64, i = e % 64;
+            const int r = row0 + i, kc = kk + kq;
+            float a = 0.f;
+            if (r < m && kc < k) a = TA ? A[int64_t(kc) * lda + r] : A[int64_t(r) * lda + kc];
+            As[kq][i] = a;
+            const int c = col0 + i;
+            float bv = 0.f;
+            if (c < n && kc < k) bv = TB ? B[int64_t(c) * ldb + kc] : B[int64_t(kc) * ldb + c];
+            Bs[kq][i] = bv;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[q][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[q][tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = row0 + ty * 4 + i;
+        if (r >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = col0 + tx * 4 + j;
+            if (c >= n) continue;
+            float v = acc[i][j];
+            if (accumulate) v += C[int64_t(r) * ldc + c];
+            if (bias) v += bias[r];
+            if (relu) v = fmaxf(v, 0.f);
+            C[int64_t(r) * ldc + c] = v;
+        }
+    }
+}
+
+template <bool TA, bool TB>
+void product(cudaStream_t stream, int m, int n, int k, const float *A, int lda, const float *B, int ldb, float *C,
+             int ldc, const float *bias = nullptr, bool relu = false, bool accumulate = false) {
+    dim3 grid(unsigned((n + 63) / 64), unsigned((m + 63) / 64));
+    product_kernel<TA, TB><<<grid, 256, 0, stream>>>(m, n, k, A, lda, B, ldb, C, ldc, bias, relu, accumulate);
+    DINARA_CUDA(cudaGetLastError());
+}
+
+// The output layer and the loss: y = w3 . h2 + b3 for each sample; dy = 2 (y - target) / batch, and
+// the summed squared error into `loss`.
+__global__ void output_kernel(const float *h2, int batch, const float *w3, const float *b3, const float *targets,
+                              float *y, float *dy, float *loss) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= batch) return;
+    float v = b3[0];
+    for (int j = 0; j < kH; ++j) v = fmaf(w3[j], h2[int64_t(j) * batch + s], v);
+    y[s] = v;
+    if (targets) {
+        const float e = v - targets[s];
+        dy[s] = 2.f * e / float(batch);
+        atomicAdd(loss, e * e);
+    }
+}
+
+// dH2 = w3 dy masked by h2 > 0; db3 = sum dy; dw3 = sum dy h2.
+__global__ void output_backward_kernel(const float *h2, const float *dy, int batch, const float *w3, float *dh2,
+                                       float *dw3, float *db3) {
+    const int j = blockIdx.x;  // a hidden unit a block
+    float sum = 0.f, dsum = 0.f;
+    for (int s = threadIdx.x; s < batch; s += blockDim.x) {
+        const float h = h2[int64_t(j) * batch + s];
+        dh2[int64_t(j) * batch + s] = h > 0.f ? w3[j] * dy[s] : 0.f;
+        sum += dy[s] * h;
+        if (j == 0) dsum += dy[s];
+    }
+    __shared__ float part[2][256];
+    part[0][threadIdx.x] = sum;
+    part[1][threadIdx.x] = dsum;
+    __syncthreads();
+    for (int span = blockDim.x / 2; span > 0; span >>= 1) {
+        if (threadIdx.x < span) {
+            part[0][threadIdx.x] += part[0][threadIdx.x + span];
+            part[1][threadIdx.x] += part[1][threadIdx.x + span];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        dw3[j] = part[0][0];
+        if (j == 0) db3[0] = part[1][0];
+    }
+}
+
+// Masks dH by H > 0 in place, and sums each row into `dbias`.
+__global__ void relu_backward_kernel(const float *h, float *dh, int batch, float *dbias) {
+    const int j = blockIdx.x;
+    float sum = 0.f;
+    for (int s = threadIdx.x; s < batch; s += blockDim.x) {
+        const int64_t at = int64_t(j) * batch + s;
+        const float g = h[at] > 0.f ? dh[at] : 0.f;
+        dh[at] = g;
+        sum += g;
+    }
+    __shared__ float part[256];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int span = blockDim.x / 2; span > 0; span >>= 1) {
+        if (threadIdx.x < span) part[threadIdx.x] += part[threadIdx.x + span];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) dbias[j] = part[0];
+}
+
+// Adam (Kingma and Ba, 2015) over every parameter.
+__global__ void adam_kernel(float *params, const float *grads, float *m, float *v, int count, float rate, float beta1,
+                            float beta2, float eps, float correction1, float correction2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float g = grads[i];
+    const float mi = beta1 * m[i] + (1.f - beta1) * g;
+    const float vi = beta2 * v[i] + (1.f - beta2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    params[i] -= rate * (mi / correction1) / (sqrtf(vi / correction2) + eps);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Inference inside the scheduling kernel
+// ------------------------------------------------------------------------------------------------
+
+// A warp a pair: the sketch, the network with every weight in shared memory, and the first threshold:
+// the predicted distance widened by the margin and the slack, never below the length difference.
+struct Margins {
+    float by_length[4];  // mean length < 300, < 1000, < 4096, longer
+};
+
+__device__ __host__ inline int length_class(double mean) { return mean < 300 ? 0 : mean < 1000 ? 1 : mean < 4096 ? 2 : 3; }
+
+__global__ void __launch_bounds__(256) predict_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs,
+                                                      const float *params, Margins margins, float slack,
+                                                      int64_t *thresholds, float *predicted) {
+    extern __shared__ float shared[];
+    float *w1 = shared;                 // [kIn][kH]
+    float *b1 = w1 + kIn * kH;
+    float *w2 = b1 + kH;                // [kH][kH]
+    float *b2 = w2 + kH * kH;
+    float *w3 = b2 + kH;
+    float *b3 = w3 + kH;
+    float *inputs = shared + kParamsRoom;  // 8 warps x 260 (kIn and padding)
+    int *counts = reinterpret_cast<int *>(inputs + 8 * 260);  // 8 warps x 256
+    for (int i = threadIdx.x; i < kPredictorParameters; i += blockDim.x) shared[i] = params[i];
+    const int warp_in_block = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *mine = counts + warp_in_block * 256;
+    float *x = inputs + warp_in_block * 260;
+    __syncthreads();
+    for (int64_t pair = int64_t(blockIdx.x) * 8 + warp_in_block; pair < pairs; pair += int64_t(gridDim.x) * 8) {
+        for (int k = lane; k < 256; k += 32) mine[k] = 0;
+        __syncwarp();
+        const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
+        count_kmers(letters + r0, q0 - r0, 1, mine);
+        count_kmers(letters + q0, q1 - q0, -1, mine);
+        __syncwarp();
+        features_of(mine, q0 - r0, q1 - q0, x, 1);
+        __syncwarp();
+        // Hidden layers: lane j computes units j and j + 32.
+        float h[2];
+        for (int u = 0; u < 2; ++u) {
+            const int j = lane + 32 * u;
+            float v = b1[j];
+            for (int i = 0; i < kIn; ++i) v = fmaf(x[i], w1[i * kH + j], v);
+            h[u] = fmaxf(v, 0.f);
+        }
+        float g[2];
+        for (int u = 0; u < 2; ++u) {
+            const int j = lane + 32 * u;
+            float v = b2[j];
+            for (int i = 0; i < kH; ++i) {
+                const float hi = __shfl_sync(0xffffffffu, h[i / 32], i % 32);
+                v = fmaf(hi, w2[i * kH + j], v);
+            }
+            g[u] = fmaxf(v, 0.f);
+        }
+        float y = g[0] * w3[lane] + g[1] * w3[lane + 32];
+        for (int span = 16; span > 0; span >>= 1) y += __shfl_xor_sync(0xffffffffu, y, span);
+        y += b3[0];
+        if (lane == 0) {
+            const int64_t n = q0 - r0, m = q1 - q0;
+            const double mean = 0.5 * double(n + m);
+            const double guess = fmax(0.0, double(y)) * mean;
+            const int64_t delta = n > m ? n - m : m - n;
+            const double margin = double(margins.by_length[length_class(mean)]);
+            int64_t t = int64_t(ceil(guess * margin + double(slack)));
+            if (t < delta) t = delta;
+            if (t < 1) t = 1;
+            thresholds[pair] = t;
+            if (predicted) predicted[pair] = float(guess);
+        }
+        __syncwarp();
+    }
+}
+
+size_t predict_shared_bytes() { return size_t(kParamsRoom + 8 * 260) * sizeof(float) + 8 * 256 * sizeof(int); }
+
+// Parameter offsets in the flat vector: w1 [kIn][kH], b1, w2 [kH][kH], b2, w3, b3.
+constexpr int kW1 = 0, kB1 = kW1 + kIn * kH, kW2 = kB1 + kH, kB2 = kW2 + kH * kH, kW3 = kB2 + kH, kB3 = kW3 + kH;
+
+// One training step's forward and backward over `batch` samples whose features are the columns of X
+// (feature-major, leading dimension ldx): gradients into `grads` (flat, like the parameters), the
+// squared error summed into `loss`.
+void forward_backward(cudaStream_t stream, const float *params, const float *X, int ldx, const float *targets,
+                      int batch, float *work, float *grads, float *loss) {
+    float *h1 = work, *h2 = h1 + int64_t(kH) * batch, *y = h2 + int64_t(kH) * batch, *dy = y + batch;
+    float *dh2 = dy + batch, *dh1 = dh2 + int64_t(kH) * batch;
+    // h1 = relu(W1^T X + b1): [kH x batch]; W1 is [kIn x kH] row-major, so op(A) = W1^T.
+    product<true, false>(stream, kH, batch, kIn, params + kW1, kH, X, ldx, h1, batch, params + kB1, true);
+    product<true, false>(stream, kH, batch, kH, params + kW2, kH, h1, batch, h2, batch, params + kB2, true);
+    output_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(h2, batch, params + kW3, params + kB3, targets, y, dy, loss);
+    DINARA_CUDA(cudaGetLastError());
+    output_backward_kernel<<<kH, 256, 0, stream>>>(h2, dy, batch, params + kW3, dh2, grads + kW3, grads + kB3);
+    DINARA_CUDA(cudaGetLastError());
+    // dW2[i][j] = sum_s h1[i][s] dh2[j][s]: [kH x kH] = h1 [kH x batch] * dh2^T.
+    product<false, true>(stream, kH, kH, batch, h1, batch, dh2, batch, grads + kW2, kH);
+    // db2: the rows of dh2.
+    relu_backward_kernel<<<kH, 256, 0, stream>>>(h2, dh2, batch, grads + kB2);
+    DINARA_CUDA(cudaGetLastError());
+    // dh1 = W2 dh2: [kH x batch] = W2 [kH x kH] * dh2, then masked by h1 > 0 with db1 its row sums.
+    product<false, false>(stream, kH, batch, kH, params + kW2, kH, dh2, batch, dh1, batch);
+    relu_backward_kernel<<<kH, 256, 0, stream>>>(h1, dh1, batch, grads + kB1);
+    DINARA_CUDA(cudaGetLastError());
+    // dW1[i][j] = sum_s X[i][s] dh1[j][s]: [kIn x kH].
+    product<false, true>(stream, kIn, kH, batch, X, ldx, dh1, batch, grads + kW1, kH);
+}
+
+size_t work_floats(int batch) { return size_t(batch) * (4 * kH + 2) + 64; }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Entry points used by capi.cu
+// ------------------------------------------------------------------------------------------------
+
+void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
+                        float *features) {
+    const int threads = 256;
+    features_kernel<<<unsigned((pairs + 7) / 8), threads, 0, gpu->stream>>>(letters, offsets, pairs, features);
+    DINARA_CUDA(cudaGetLastError());
+}
+
+void predictor_gradients(dinara_gpu *gpu, int batch, const float *features, const float *targets, float *grads,
+                         float *loss) {
+    float *params = gpu->weights.as<float>();
+    float *work = gpu->activations.ensure<float>(work_floats(batch));
+    DINARA_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), gpu->stream));
+    forward_backward(gpu->stream, params, features, batch, targets, batch, work, grads, loss);
+}
+
 const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets) {
-    (void)pairs;
-    (void)letters;
-    (void)offsets;
-    throw Failure(DINARA_INVALID_MODE, "no trained band predictor on this context");
-    return gpu ? nullptr : nullptr;
+    if (!gpu->predictor_ready) throw Failure(DINARA_INVALID_MODE, "no trained band predictor on this context");
+    int64_t *thresholds = gpu->predictions.ensure<int64_t>(size_t(pairs));
+    float *predicted = gpu->targets.ensure<float>(size_t(pairs));
+    static bool configured = false;
+    const size_t shared = predict_shared_bytes();
+    if (!configured) {
+        DINARA_CUDA(cudaFuncSetAttribute(predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared)));
+        configured = true;
+    }
+    int per_sm = 0;
+    DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, predict_kernel, 256, shared));
+    int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
+    blocks = std::min<int64_t>(blocks, (pairs + 7) / 8);
+    Margins margins;
+    for (int k = 0; k < 4; ++k) margins.by_length[k] = float(gpu->predictor_margins[k]);
+    predict_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), 256, shared, gpu->stream>>>(
+        letters, offsets, pairs, gpu->weights.as<float>(), margins, float(gpu->predictor_slack), thresholds, predicted);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
+    return thresholds;
+}
+
+void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinara_train_report &report) {
+    cudaStream_t stream = gpu->stream;
+    const int64_t pairs = options.pairs;
+    // The training pairs: lengths, offsets, letters, all on the device.
+    int64_t *lengths = gpu->thresholds.ensure<int64_t>(size_t(2 * pairs + 1));
+    const int threads = 256;
+    const unsigned pair_blocks = unsigned((pairs + threads - 1) / threads);
+    generate_lengths_kernel<<<pair_blocks, threads, 0, stream>>>(options.seed, pairs, options.length_low,
+                                                                 options.length_high, options.rate_low,
+                                                                 options.rate_high, lengths);
+    DINARA_CUDA(cudaGetLastError());
+    int64_t *offsets = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
+    DINARA_CUDA(cudaMemsetAsync(lengths + 2 * pairs, 0, sizeof(int64_t), stream));
+    size_t scratch = 0;
+    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, lengths, offsets, int(2 * pairs + 1), stream));
+    void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
+    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, lengths, offsets, int(2 * pairs + 1), stream));
+    int64_t total = 0;
+    DINARA_CUDA(cudaMemcpyAsync(&total, offsets + 2 * pairs, sizeof total, cudaMemcpyDeviceToHost, stream));
+    DINARA_CUDA(cudaStreamSynchronize(stream));
+    uint8_t *letters = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
+    generate_letters_kernel<<<pair_blocks, threads, 0, stream>>>(options.seed, pairs, options.length_low,
+                                                                 options.length_high, options.rate_low,
+                                                                 options.rate_high, offsets, letters);
+    DINARA_CUDA(cudaGetLastError());
+    // Their exact distances: the method's own, plain band doubling.
+    int64_t *distances = gpu->features.ensure<int64_t>(size_t(pairs));
+    band_doubling(gpu, pairs, letters, offsets, nullptr, 0, distances, nullptr);
+    // Targets (distance over mean length) and features.
+    std::vector<int64_t> host_distances(static_cast<size_t>(pairs)), host_offsets(size_t(2 * pairs + 1));
+    DINARA_CUDA(cudaMemcpyAsync(host_distances.data(), distances, size_t(pairs) * sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, stream));
+    DINARA_CUDA(cudaMemcpyAsync(host_offsets.data(), offsets, host_offsets.size() * sizeof(int64_t),
+                                cudaMemcpyDeviceToHost, stream));
+    DINARA_CUDA(cudaStreamSynchronize(stream));
+    std::vector<float> host_targets(static_cast<size_t>(pairs));
+    for (int64_t p = 0; p < pairs; ++p) {
+        const double mean = 0.5 * double(host_offsets[size_t(2 * p + 2)] - host_offsets[size_t(2 * p)]);
+        host_targets[size_t(p)] = mean > 0 ? float(double(host_distances[size_t(p)]) / mean) : 0.f;
+    }
+    float *targets = gpu->targets.ensure<float>(size_t(pairs));
+    DINARA_CUDA(cudaMemcpyAsync(targets, host_targets.data(), size_t(pairs) * sizeof(float), cudaMemcpyHostToDevice,
+                                stream));
+    // The features, feature-major, into gpu->gradients' room after the parameters' gradients.
+    float *features = gpu->planes.ensure<float>(size_t(pairs) * kIn);
+    predictor_features(gpu, pairs, letters, offsets, features);
+
+    // Parameters: He initialisation from the seed, biases zero; Adam's moments zero.
+    std::vector<float> init(kPredictorParameters, 0.f);
+    uint64_t state = options.seed ^ 0x5bd1e995u;
+    auto gaussian = [&]() {
+        const double u1 = std::max(1e-12, unit(mix64(++state)));
+        const double u2 = unit(mix64(++state));
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+    };
+    for (int i = 0; i < kIn * kH; ++i) init[size_t(kW1 + i)] = float(gaussian() * std::sqrt(2.0 / kIn));
+    for (int i = 0; i < kH * kH; ++i) init[size_t(kW2 + i)] = float(gaussian() * std::sqrt(2.0 / kH));
+    for (int i = 0; i < kH; ++i) init[size_t(kW3 + i)] = float(gaussian() * std::sqrt(1.0 / kH));
+    float *params = gpu->weights.ensure<float>(kPredictorParameters);
+    float *grads = gpu->gradients.ensure<float>(kPredictorParameters);
+    float *moments = gpu->optimizer.ensure<float>(2 * kPredictorParameters);
+    DINARA_CUDA(cudaMemcpyAsync(params, init.data(), init.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+    DINARA_CUDA(cudaMemsetAsync(moments, 0, 2 * kPredictorParameters * sizeof(float), stream));
+    const int batch = int(options.batch);
+    float *work = gpu->activations.ensure<float>(work_floats(batch));
+    float *loss = work + work_floats(batch) - 8;
+    // The last tenth of the pairs is held out for validation.
+    const int64_t held = std::max<int64_t>(pairs / 10, 1);
+    const int64_t trained = pairs - held;
+    int64_t step = 0;
+    double last_loss = 0.0;
+    for (int64_t epoch = 0; epoch < options.epochs; ++epoch) {
+        double epoch_loss = 0.0;
+        int64_t batches = 0;
+        for (int64_t first = 0; first + batch <= trained; first += batch) {
+            DINARA_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), stream));
+            forward_backward(stream, params, features + first, int(pairs), targets + first, batch, work, grads, loss);
+            ++step;
+            const float beta1 = 0.9f, beta2 = 0.999f;
+            adam_kernel<<<(kPredictorParameters + 255) / 256, 256, 0, stream>>>(
+                params, grads, moments, moments + kPredictorParameters, kPredictorParameters, float(options.learning_rate),
+                beta1, beta2, 1e-8f, 1.f - std::pow(beta1, float(step)), 1.f - std::pow(beta2, float(step)));
+            DINARA_CUDA(cudaGetLastError());
+            if ((batches & 63) == 63 || first + 2 * batch > trained) {
+                float host_loss = 0.f;
+                DINARA_CUDA(cudaMemcpyAsync(&host_loss, loss, sizeof host_loss, cudaMemcpyDeviceToHost, stream));
+                DINARA_CUDA(cudaStreamSynchronize(stream));
+                epoch_loss = host_loss / batch;
+            }
+            ++batches;
+        }
+        last_loss = epoch_loss;
+    }
+    report.steps = step;
+    report.train_loss = last_loss;
+    // Validation: predicted distances on the held-out pairs, and the margin that covers the asked share
+    // of them (a first threshold at or above the distance).
+    gpu->predictor_ready = true;
+    for (int k = 0; k < 4; ++k) gpu->predictor_margins[k] = 1.0;
+    gpu->predictor_slack = 0.0;
+    int64_t *held_offsets = gpu->pending.ensure<int64_t>(size_t(2 * held + 1));
+    std::vector<int64_t> rebased(size_t(2 * held + 1));
+    for (int64_t k = 0; k <= 2 * held; ++k) rebased[size_t(k)] = host_offsets[size_t(2 * trained + k)];
+    DINARA_CUDA(cudaMemcpyAsync(held_offsets, rebased.data(), rebased.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                stream));
+    predict_thresholds(gpu, held, letters, held_offsets);
+    std::vector<float> guesses(static_cast<size_t>(held));
+    DINARA_CUDA(cudaMemcpyAsync(guesses.data(), gpu->targets.as<float>(), size_t(held) * sizeof(float),
+                                cudaMemcpyDeviceToHost, stream));
+    DINARA_CUDA(cudaStreamSynchronize(stream));
+    // Each held-out pair's ratio of distance (less the slack) to guess, by length class; a class's margin
+    // reaches the asked share of its pairs. A long pair that undershoots costs a whole extra round, a short
+    // one that overshoots only a wider band, so every class is held to the same coverage of its own pairs.
+    std::vector<double> ratios[4];
+    double squared = 0.0;
+    for (int64_t k = 0; k < held; ++k) {
+        const int64_t p = trained + k;
+        const double d = double(host_distances[size_t(p)]);
+        const double g = double(guesses[size_t(k)]);
+        const double mean = 0.5 * double(host_offsets[size_t(2 * p + 2)] - host_offsets[size_t(2 * p)]);
+        ratios[length_class(mean)].push_back((d - options.slack) / std::max(g, 1.0));
+        const double e = (mean > 0 ? d / mean : 0.0) - (mean > 0 ? g / mean : 0.0);
+        squared += e * e;
+    }
+    const double coverage = std::min(std::max(options.coverage, 0.5), 0.999);
+    double widest = 1.0;
+    for (int c = 0; c < 4; ++c) {
+        double margin = 1.0;
+        if (!ratios[c].empty()) {
+            std::sort(ratios[c].begin(), ratios[c].end());
+            margin = std::max(1.0, ratios[c][size_t(double(ratios[c].size() - 1) * coverage)]);
+        }
+        gpu->predictor_margins[c] = margin;
+        widest = std::max(widest, margin);
+    }
+    gpu->predictor_margin = widest;
+    gpu->predictor_slack = options.slack;
+    const double margin = widest;
+    report.validation_loss = squared / double(held);
+    report.margin = margin;
+    report.slack = options.slack;
+    report.held_out = held;
 }
 
 }  // namespace dinara

@@ -1,0 +1,26 @@
+// The learned band predictor's shapes and the entry points capi.cu calls (learned.cu).
+#pragma once
+
+#include "internal.cuh"
+
+namespace dinara {
+
+constexpr int kPredictorInputs = 257;  // 256 4-mer count differences and the length ratio
+constexpr int kPredictorHidden = 64;
+// w1 [257][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3 [1], flat in that order.
+constexpr int kPredictorParameters =
+    kPredictorInputs * kPredictorHidden + kPredictorHidden + kPredictorHidden * kPredictorHidden + kPredictorHidden +
+    kPredictorHidden + 1;
+
+// Features of pairs on the device into a feature-major matrix (feature f of pair p at f * pairs + p).
+void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets, float *features);
+
+// One batch's gradients of the summed squared error over the mean, for the context's parameters: the
+// features feature-major ([257][batch]), targets, gradients and the squared error's sum on the device.
+void predictor_gradients(dinara_gpu *gpu, int batch, const float *features, const float *targets, float *grads,
+                         float *loss);
+
+// Trains the context's predictor on device-generated pairs and sets its margin.
+void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinara_train_report &report);
+
+}  // namespace dinara

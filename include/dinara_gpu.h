@@ -168,6 +168,57 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
                                   const dinara_band_plan *plan, int64_t *results, dinara_band_report *report);
 
 /*
+ * The learned band predictor (no reference counterpart): a 257 -> 64 -> 64 -> 1 fp32 network over a
+ * pair's 4-mer count differences and length ratio, predicting its distance over its mean length; band
+ * doubling with DINARA_BAND_LEARNED starts each pair at the prediction times the margin plus the slack,
+ * never below the length difference. Parameters are one flat vector of DINARA_PREDICTOR_PARAMETERS
+ * floats: w1 [257][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3.
+ */
+#define DINARA_PREDICTOR_PARAMETERS 20737
+
+typedef struct {
+    uint64_t seed;          /* the training pairs' generator seed */
+    int64_t pairs;          /* training pairs generated on the device (a tenth held out) */
+    double length_low;      /* reference lengths log-uniform in [length_low, length_high] */
+    double length_high;
+    double rate_low;        /* per-pair error rate uniform in [rate_low, rate_high], 50/25/25 */
+    double rate_high;
+    int64_t epochs;
+    int64_t batch;
+    double learning_rate;   /* Adam's */
+    double coverage;        /* share of held-out pairs the first threshold should reach (0.5-0.999) */
+    double slack;           /* letters added to every first threshold */
+} dinara_train_options;
+
+typedef struct {
+    int64_t steps;
+    double train_loss;      /* mean squared error of the last batch, distance over mean length */
+    double validation_loss; /* the held-out pairs' */
+    double margin;          /* the multiplier chosen for the coverage */
+    double slack;
+    int64_t held_out;
+    double seconds;         /* wall time of generation, exact distances and training */
+} dinara_train_report;
+
+/* Trains the context's predictor on the device: generates the pairs, measures their exact distances by
+ * plain band doubling, trains with Adam, and sets the margin from the held-out pairs. */
+int64_t dinara_gpu_predictor_train(dinara_gpu *gpu, const dinara_train_options *options, dinara_train_report *report);
+/* Installs parameters (and the margin and slack) on the context, or reads them back. */
+int64_t dinara_gpu_predictor_set(dinara_gpu *gpu, const float *parameters, double margin, double slack);
+int64_t dinara_gpu_predictor_get(dinara_gpu *gpu, float *parameters, double *margin, double *slack);
+/* The 257 features of each pair of a tape, pair-major into `features` (pairs x 257 floats). */
+int64_t dinara_gpu_predictor_features(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                      float *features);
+/* One batch's gradients for the installed parameters: features pair-major (batch x 257), targets
+ * (distance over mean length); the gradient of the mean squared error into `gradients`, and the mean
+ * squared error into *loss. For checking the training kernels against another implementation. */
+int64_t dinara_gpu_predictor_gradients(dinara_gpu *gpu, int64_t batch, const float *features, const float *targets,
+                                       float *gradients, double *loss);
+/* Each pair's predicted distance and first threshold. */
+int64_t dinara_gpu_predictor_predict(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                     float *predicted, int64_t *thresholds);
+
+/*
  * Resident batches (no reference counterpart; the reference re-creates its device scope, uploads and
  * frees on every call, scoring.mojo:1342-1409): a batch's letters uploaded and packed once and kept on
  * the device, so later calls run the device path alone. One resident batch a context.

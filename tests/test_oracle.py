@@ -202,3 +202,30 @@ def test_batches_match_singles(oracle):
     distances = oracle.batch_distances(tape, offsets, start=0, threads=4)
     for k, (a, b) in enumerate(zip(firsts, seconds)):
         assert distances[k] == oracle.edit_distance_dp(a, b)
+
+
+def test_mlp_oracle_gradients_by_finite_differences():
+    """The predictor's CPU oracle: its analytic gradients against central differences."""
+    import mlp_oracle
+
+    rng = np.random.default_rng(2)
+    flat = rng.normal(0, 0.2, size=mlp_oracle.PARAMETERS)
+    x = rng.normal(0, 1, size=(7, 257))
+    t = rng.uniform(0, 1, size=7)
+    grads, _ = mlp_oracle.gradients(flat, x, t)
+    for index in list(rng.integers(0, mlp_oracle.PARAMETERS, size=40)) + [mlp_oracle.PARAMETERS - 1]:
+        step = 1e-6
+        up, down = flat.copy(), flat.copy()
+        up[index] += step
+        down[index] -= step
+        numeric = (mlp_oracle.gradients(up, x, t)[1] - mlp_oracle.gradients(down, x, t)[1]) / (2 * step)
+        assert abs(numeric - grads[index]) <= 1e-5 + 1e-4 * abs(numeric)
+
+
+def test_mlp_oracle_kmer_features():
+    import mlp_oracle
+
+    counts = mlp_oracle.kmer_counts(b"AAAACNAAAA")
+    assert counts[0] == 2 and counts.sum() == 3  # AAAA twice, AAAC once; k-mers over N skipped
+    f = mlp_oracle.features(b"AAAAA", b"AAAA")
+    assert abs(f[0] - (2 - 1) / np.sqrt(4.5)) < 1e-12 and abs(f[256] - 0.8) < 1e-12
