@@ -49,6 +49,7 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--pairs", type=int, default=0, help="override the workload's pair count")
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-cpu", action="store_true")
+    parser.add_argument("--no-extras", action="store_true", help="skip the learned-band and serving sections")
     return parser.parse_args()
 
 
@@ -172,6 +173,61 @@ def cpu_measure(oracle, workload: str, threads: int, steps: int, warmup: int) ->
                           f"{len(times)} runs of {seconds:.2f} s"}}
 
 
+def learned_band_section(da, native, lib, handle, steps: int) -> dict:
+    """The uneven unit-cost batch (200,000 pairs, log-uniform 100 bp-20 kbp, 0.5-15% errors) swept by plain
+    band doubling and by the learned band, each timed on the device with the letters resident; the
+    predictor first trained on the GPU on 1,000,000 pairs of the same distribution."""
+    from dinara_align import learned, workloads
+
+    predictor = learned.Predictor()
+    training = predictor.train(pairs=1_000_000, epochs=4, batch=4096, seed=2024)
+    tape = workloads.uneven_unit_cost(200_000, seed=7)
+    cells = int(((tape.offsets[1::2] - tape.offsets[0:-1:2]) * (tape.offsets[2::2] - tape.offsets[1::2])).sum())
+    native.check(lib.dinara_gpu_resident_load(handle, tape.pairs, tape.letters.ctypes.data,
+                                              tape.offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), None),
+                 handle)
+    out = {"workload": WORKLOADS["uneven"], "pairs": tape.pairs, "full_matrix_cells": cells, "training": training}
+    results = {}
+    for name, policy in (("plain", native.BAND_PLAIN), ("learned", native.BAND_LEARNED)):
+        times, report = [], native.CBandReport()
+        for k in range(2 + steps):
+            timing = Timing()
+            plan = native.CBandPlan(policy, None, 0)
+            report = native.CBandReport()
+            native.check(lib.dinara_gpu_resident_distances(handle, ctypes.byref(plan), ctypes.byref(report),
+                                                           ctypes.byref(timing)), handle)
+            if k >= 2:
+                times.append(timing.total_ms)
+        found = np.zeros(tape.pairs, dtype=np.int64)
+        lib.dinara_gpu_resident_fetch(handle, None, found.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        results[name] = found
+        ms = statistics.median(times)
+        out[name] = {"ms": ms, "pairs_per_s": tape.pairs / (ms / 1e3), "gcups": cells / (ms / 1e3) / 1e9,
+                     "report": {field: getattr(report, field) for field, _ in native.CBandReport._fields_}}
+    out["identical_distances"] = bool((results["plain"] == results["learned"]).all())
+    out["speedup"] = out["learned"]["pairs_per_s"] / out["plain"]["pairs_per_s"]
+    return out
+
+
+def serving_section(da) -> dict:
+    """Open-loop serving: Poisson arrivals at 2,000 requests/s, each 1-4,096 pairs (log-uniform), lengths
+    log-uniform 100 bp-50 kbp, 1-10% errors, global gap-affine (4,6,2) scores, a 40 GB device budget; a bounded
+    run of 40 requests, far past what the device sustains, so latency is mostly queueing."""
+    from dinara_align import serving, workloads
+
+    rng = np.random.default_rng(55)
+    requests = [workloads.serving_request(rng) for _ in range(40)]
+    scoring = da.Scoring.uniform(0, -4, -6, -2)
+    with serving.Server(slots=4, device_bytes=40 << 30) as server:
+        out = serving.open_loop(server, requests, 2000.0, scoring)
+        out["stats"] = server.stats()
+    out["cells"] = int(sum(((t.offsets[1::2] - t.offsets[0:-1:2]) * (t.offsets[2::2] - t.offsets[1::2])).sum()
+                           for t in requests))
+    out["gcups"] = out["cells"] / out["seconds"] / 1e9
+    out["offered_pairs_per_s"] = 2000.0 * float(np.mean([t.pairs for t in requests]))
+    return out
+
+
 def int32_peak(handle, lib) -> dict:
     lib.dinara_gpu_int32_peak.restype = ctypes.c_int64
     lib.dinara_gpu_int32_peak.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]
@@ -227,6 +283,9 @@ def main() -> None:
     lib.dinara_gpu_resident_distances.restype = ctypes.c_int64
     lib.dinara_gpu_resident_distances.argtypes = [ctypes.c_void_p, ctypes.POINTER(native.CBandPlan),
                                                   ctypes.POINTER(native.CBandReport), ctypes.POINTER(Timing)]
+    lib.dinara_gpu_resident_fetch.restype = ctypes.c_int64
+    lib.dinara_gpu_resident_fetch.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.POINTER(ctypes.c_int64)]
     struct, _table, _alphabet = scoring._struct()
     mode_struct = mode._struct()
     code = lib.dinara_gpu_resident_load(handle, pairs, tape.letters.ctypes.data,
@@ -353,6 +412,9 @@ def main() -> None:
             line["scorer"] = scorer
         if band_report:
             line["band_report"] = band_report
+        if world == 1 and not args.no_extras and args.workload == "affine":
+            line["learned_band"] = learned_band_section(da, native, lib, handle, max(1, min(args.steps, 3)))
+            line["serving"] = serving_section(da)
         line["int32_peaks_instr_per_s"] = peaks
         if not args.no_cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -434,6 +434,7 @@ void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_
     unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(16) + 12);
     DINARA_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long), gpu->stream));
     swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, out);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     unsigned long long host = 0;
     DINARA_CUDA(cudaMemcpyAsync(&host, out, sizeof host, cudaMemcpyDeviceToHost, gpu->stream));
@@ -500,6 +501,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     const unsigned blocks = unsigned((count + threads - 1) / threads);
     slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, band, words,
                                                            slot_bytes, layouts);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     size_t scratch = 0;
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, words, word_offsets, int(count + 1), gpu->stream));
@@ -559,6 +561,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
             const unsigned left_blocks = unsigned((left + threads - 1) / threads);
             leftover_words_kernel<<<left_blocks, threads, 0, gpu->stream>>>(batch.shapes, leftovers, left, uniform,
                                                                             left_words);
+            gpu->launches += 1;
             DINARA_CUDA(cudaGetLastError());
             DINARA_CUDA(cudaMemsetAsync(left_words + left, 0, sizeof(int64_t), gpu->stream));
             size_t bytes = 0;
@@ -572,6 +575,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
             extra = gpu->decisions_extra.ensure<uint64_t>(size_t(extra_total) + 8);
             leftover_places_kernel<<<left_blocks, threads, 0, gpu->stream>>>(leftovers, left, first_pair, left_offsets,
                                                                              word_offsets, layouts);
+            gpu->launches += 1;
             DINARA_CUDA(cudaGetLastError());
             const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, true, false);
             KernelArgs extra_args = args;

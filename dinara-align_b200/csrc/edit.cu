@@ -382,6 +382,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     const unsigned warp_blocks = unsigned((pairs * 32 + threads - 1) / threads);
     const unsigned thread_blocks = unsigned((pairs + threads - 1) / threads);
     prepare_kernel<<<warp_blocks, threads, 0, stream>>>(letters, offsets, pairs, info, plane_words, results, status);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     DINARA_CUDA(cudaMemsetAsync(plane_words + pairs, 0, sizeof(int64_t), stream));
     size_t scratch = 0;
@@ -393,6 +394,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     DINARA_CUDA(cudaStreamSynchronize(stream));
     uint64_t *planes = gpu->planes.ensure<uint64_t>(size_t(plane_total) + 4);
     planes_kernel<<<warp_blocks, threads, 0, stream>>>(letters, info, pairs, plane_offsets, planes);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 
     int64_t *thresholds = gpu->thresholds.ensure<int64_t>(3 * size_t(pairs));
@@ -409,6 +411,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     start_kernel<<<thread_blocks, threads, 0, stream>>>(info, pairs, first_thresholds_device,
                                                         default_start > 0 ? default_start : 256, status, thresholds,
                                                         firsts, pending, counters);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     uint32_t *keys = gpu->keys.ensure<uint32_t>(size_t(pairs));
     uint32_t *keys_sorted = gpu->keys_sorted.ensure<uint32_t>(size_t(pairs));
@@ -424,6 +427,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, (1 + kBandShapes) * sizeof(unsigned int), stream));
         const unsigned blocks = unsigned((count + threads - 1) / threads);
         band_keys_kernel<<<blocks, threads, 0, stream>>>(info, pending, counters, thresholds, keys, counters + 2);
+        gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         size_t sort_bytes = 0;
         DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_bytes, keys, keys_sorted, pending,
@@ -469,6 +473,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
             if (!used[side]) DINARA_CUDA(cudaStreamWaitEvent(gpu->side[side], gpu->fork, 0));
             used[side] = true;
             fn<<<unsigned(grid), kBlock, 0, gpu->side[side]>>>(args);
+            gpu->launches += 1;
             DINARA_CUDA(cudaGetLastError());
             at += n_shape;
             ++launches;
@@ -482,6 +487,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned int), stream));
         settle_kernel<<<blocks, threads, 0, stream>>>(info, order_sorted, counters, thresholds, banded, results, rounds,
                                                       next, counters + 1);
+        gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         DINARA_CUDA(cudaMemcpyAsync(counters, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToDevice, stream));
         DINARA_CUDA(cudaMemcpyAsync(host_counts, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
@@ -496,6 +502,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         unsigned long long *tallies = swept + 1;
         DINARA_CUDA(cudaMemsetAsync(tallies, 0, 4 * sizeof(unsigned long long), stream));
         tally_kernel<<<thread_blocks, threads, 0, stream>>>(info, pairs, status, firsts, rounds, results, tallies);
+        gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         unsigned long long host[5] = {0, 0, 0, 0, 0};
         DINARA_CUDA(cudaMemcpyAsync(host, swept, sizeof(host), cudaMemcpyDeviceToHost, stream));

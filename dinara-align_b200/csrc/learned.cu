@@ -445,6 +445,7 @@ void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, 
                         float *features) {
     const int threads = 256;
     features_kernel<<<unsigned((pairs + 7) / 8), threads, 0, gpu->stream>>>(letters, offsets, pairs, features);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 }
 

@@ -97,6 +97,7 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
     const int64_t blocks = (pairs * 32 + threads - 1) / threads;
     pack_pairs_kernel<<<dim3(unsigned(blocks)), threads, 0, gpu->stream>>>(
         letters_device, offsets_device, pairs, codes_device, bits, tape, shapes, unknown);
+    gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 }
 

@@ -250,6 +250,43 @@ int64_t dinara_gpu_resident_distances(dinara_gpu *gpu, const dinara_band_plan *p
 int64_t dinara_gpu_resident_fetch(dinara_gpu *gpu, int32_t *scores, int64_t *distances);
 
 /*
+ * A serving loop (no reference counterpart; the reference opens a device scope, uploads and frees on
+ * every call, scoring.mojo:1342-1409). Requests, each a batch of pairs under a Scoring, are submitted at
+ * any time and admitted first in first out as a worker slot and device memory free up; each slot keeps its
+ * stream and device buffers between requests, and admitted requests run at once on the device. Waits are
+ * bounded and return DINARA_DEVICE_TIMEOUT when they run out.
+ */
+typedef struct dinara_server dinara_server;
+
+typedef struct {
+    int64_t slots;        /* requests that may run at once (1 to 32; 0 for 4) */
+    int64_t device_bytes; /* the device memory budget for the slots' buffers (0 for 40 GiB) */
+} dinara_server_options;
+
+typedef struct {
+    double submitted, admitted, finished; /* seconds since the server started */
+    int64_t pairs;
+    int64_t device_bytes;                 /* the request's estimated device memory */
+} dinara_request_timing;
+
+typedef struct {
+    int64_t queued, running, admitted, completed, refused, pairs_done;
+    int64_t resident_bytes, budget_bytes;
+    double clock; /* seconds since the server started */
+} dinara_server_stats_t;
+
+dinara_server *dinara_server_new(dinara_gpu *gpu, const dinara_server_options *options);
+void dinara_server_free(dinara_server *server);
+/* Queues a request (its letters and Scoring copied); its ticket into *ticket. */
+int64_t dinara_server_submit(dinara_server *server, int64_t pairs, const char *letters, const int64_t *offsets,
+                             const dinara_scoring *scoring, const dinara_mode *mode, int64_t *ticket);
+/* Waits up to `timeout_ms` for a request: its scores and statuses (each `pairs` long) and timing; the
+ * request's code (DINARA_OUT_OF_MEMORY when it cannot fit the budget) or DINARA_DEVICE_TIMEOUT. */
+int64_t dinara_server_wait(dinara_server *server, int64_t ticket, int64_t timeout_ms, int32_t *scores,
+                           int64_t *statuses, dinara_request_timing *timing);
+int64_t dinara_server_stats(dinara_server *server, dinara_server_stats_t *stats);
+
+/*
  * Scores without allocating (no counterpart in the reference). For callers that cannot allocate device
  * memory themselves or through this library (code inside another framework's memory pool, or under a
  * budget that forbids growth): the caller passes its own device buffers, a packed batch and the room
@@ -276,8 +313,10 @@ int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const uint32_t *
                                  const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, void *stream);
 
 /* The device's measured integer issue rate (no reference counterpart: the roofline the sweeps are
- * judged against): `kind` 0 DPX add-and-max, 1 min/max with an add, 2 three-input add; instructions
- * per second into *instructions_per_second, from independent chains on every SM. */
+ * judged against): `kind` 0 DPX add-and-max, 1 min/max with an add (counted as two), 2 three-input add,
+ * 3 DPX add-and-max on 16-bit pairs, 4 three-way max, 5 three-way max on 16-bit pairs, 6 byte permute,
+ * 7 max alone, 8 16-bit pair compare to a mask, 9 16-bit pair max with predicates, 10 kind 3 floored at
+ * zero, 11 16-bit pair subtraction; instructions per second into *instructions_per_second, from independent chains on every SM. */
 int64_t dinara_gpu_int32_peak(dinara_gpu *gpu, int64_t kind, double *instructions_per_second);
 
 #ifdef __cplusplus
