@@ -203,7 +203,7 @@ def learned_band_section(da, native, lib, handle, steps: int) -> dict:
         results[name] = found
         ms = statistics.median(times)
         out[name] = {"ms": ms, "pairs_per_s": tape.pairs / (ms / 1e3), "gcups": cells / (ms / 1e3) / 1e9,
-                     "report": {field: getattr(report, field) for field, _ in native.CBandReport._fields_}}
+                     "report": report.as_dict()}
     out["identical_distances"] = bool((results["plain"] == results["learned"]).all())
     out["speedup"] = out["learned"]["pairs_per_s"] / out["plain"]["pairs_per_s"]
     return out
@@ -302,7 +302,7 @@ def main() -> None:
             report = native.CBandReport()
             native.check(lib.dinara_gpu_resident_distances(handle, ctypes.byref(plan), ctypes.byref(report),
                                                            ctypes.byref(timing)), handle)
-            band_report.update({name: getattr(report, name) for name, _ in native.CBandReport._fields_})
+            band_report.update(report.as_dict())
         else:
             native.check(lib.dinara_gpu_resident_align(handle, ctypes.byref(mode_struct), 1 if args.workload ==
                                                        "affine" else 0, 1, ctypes.byref(timing)), handle)

@@ -342,7 +342,7 @@ struct Buckets {
 
 Buckets buckets_of(const Schedule &schedule) {
     Buckets b;
-    int64_t at = schedule.counts[kBandClass];
+    int64_t at = schedule.counts[kBandPairsClass] + schedule.counts[kBandClass];
     for (int cls = kAffineShapes - 1; cls >= 0; --cls) {
         b.begin[cls] = at;
         at += schedule.counts[cls];
@@ -403,20 +403,43 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
     }
 }
 
-// The band's shifted table and best entry for a banded launch.
+// The largest rows + columns of a pair the 16-bit pair sweep takes under a table (band_pair_limit): the
+// largest step a shifted cell takes is a shifted entry or a gap's opening.
+int32_t pair_limit_of(const AffineTable &table) {
+    int32_t step = std::abs(table.open - table.extend);
+    bool bytes_fit = true;
+    for (int r = 0; r < table.size; ++r)
+        for (int c = 0; c < table.size; ++c) {
+            const int32_t v = table.entries[r * 32 + c] - 2 * table.extend;
+            step = std::max(step, std::abs(v));
+            bytes_fit = bytes_fit && v >= -128 && v <= 127;
+        }
+    return band_pair_limit(step, bytes_fit);
+}
+
+// The band's shifted table and best entry for a banded launch: the band's pairs of the 16-bit pair sweep
+// (`pairs_of_16`), which come first in the order, or the rest after them.
 BandedBatch banded_batch(const AffineBatch &batch, const AffineTable &table, const Schedule &schedule, int32_t *scores,
-                         uint8_t *proven, uint32_t *leftovers, unsigned int *leftover_count) {
+                         uint8_t *proven, uint32_t *leftovers, unsigned int *leftover_count, bool pairs_of_16) {
     BandedBatch band;
     std::memset(&band, 0, sizeof band);
     const TableArgs targs = table_args(table, false);
     for (int r = 0; r < 4; ++r) band.rows16[r] = targs.rows16[r];
+    for (int r = 0; r < 4; ++r) {
+        uint32_t row = 0;
+        for (int c = 0; c < 4; ++c) {
+            const int32_t v = r < table.size && c < table.size ? table.entries[r * 32 + c] - 2 * table.extend : 0;
+            row |= uint32_t(uint8_t(int8_t(v))) << (8 * c);
+        }
+        band.rows8[r] = row;
+    }
     int32_t best = -128;
     for (int r = 0; r < table.size; ++r)
         for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
     band.tape = batch.tape;
     band.shapes = batch.shapes;
-    band.order = schedule.order;
-    band.count = schedule.counts[kBandClass];
+    band.order = pairs_of_16 ? schedule.order : schedule.order + schedule.counts[kBandPairsClass];
+    band.count = schedule.counts[pairs_of_16 ? kBandPairsClass : kBandClass];
     band.open = table.open;
     band.extend = table.extend;
     band.best = best;
@@ -444,6 +467,30 @@ void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_
 
 }  // namespace
 
+namespace {
+
+// The proven band's pairs of a schedule: the 16-bit pair sweep's and the rest.
+int64_t band_pairs(const Schedule &schedule) {
+    return schedule.counts[kBandPairsClass] + schedule.counts[kBandClass];
+}
+
+// Sweeps the band's pairs, the 16-bit pair sweep's first, every unproven pair onto one leftover list.
+void launch_bands(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const Schedule &schedule,
+                  int32_t *scores, uint32_t *leftovers, unsigned int *leftover_count, bool record, uint64_t *decisions,
+                  const int64_t *decision_offsets, int64_t first_pair) {
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool pairs_of_16 = pass == 0;
+        BandedBatch b = banded_batch(batch, table, schedule, scores, nullptr, leftovers, leftover_count, pairs_of_16);
+        if (b.count == 0) continue;
+        b.decisions = decisions;
+        b.decision_offsets = decision_offsets;
+        b.first_pair = first_pair;
+        banded_launch(gpu, b, record, pairs_of_16);
+    }
+}
+
+}  // namespace
+
 bool band_serves(const AffineBatch &batch, const AffineTable &table) {
     if (batch.local || batch.bits != 2 || !table.packed16) return false;
     int32_t best = -128;
@@ -456,7 +503,8 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
                    int64_t first, int64_t count) {
     if (count <= 0) return;
     const bool band = band_serves(batch, table);
-    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, band);
+    const Schedule schedule_all =
+        dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, band, band ? pair_limit_of(table) : 0);
     PhaseTimer timer(gpu, &gpu->kernel_ms);
     KernelArgs args;
     std::memset(&args, 0, sizeof args);
@@ -468,14 +516,14 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
     unsigned int *counters = gpu->class_counts.ensure<unsigned int>(16);
     unsigned int *leftover_count = counters + 8;
     uint32_t *leftovers = nullptr;
-    if (schedule_all.counts[kBandClass] > 0) {
-        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(schedule_all.counts[kBandClass]));
+    if (band_pairs(schedule_all) > 0) {
+        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(band_pairs(schedule_all)));
         DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
-        banded_launch(gpu, banded_batch(batch, table, schedule_all, scores, nullptr, leftovers, leftover_count), false);
+        launch_bands(gpu, batch, table, schedule_all, scores, leftovers, leftover_count, false, nullptr, nullptr, 0);
     }
     affine_launch_all(gpu, batch, table, schedule_all, false, args);
     unsigned int left = 0;
-    if (schedule_all.counts[kBandClass] > 0) {
+    if (band_pairs(schedule_all) > 0) {
         DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         if (left > 0) {
@@ -522,7 +570,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     char *slots = gpu->walk_out.ensure<char>(size_t(totals[1]) + 8);
     int64_t *ends = gpu->spans.ensure<int64_t>(size_t(count) + 1);
     int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(size_t(count) + 1);
-    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band);
+    const Schedule schedule_all =
+        dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band, band ? pair_limit_of(table) : 0);
 
     PhaseTimer timer(gpu, &gpu->record_ms);
     KernelArgs args;
@@ -540,18 +589,15 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     unsigned int *leftover_count = counters + 8;
     uint32_t *leftovers = nullptr;
     uint64_t *extra = nullptr;
-    if (schedule_all.counts[kBandClass] > 0) {
-        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(schedule_all.counts[kBandClass]));
+    if (band_pairs(schedule_all) > 0) {
+        leftovers = gpu->leftovers.ensure<uint32_t>(size_t(band_pairs(schedule_all)));
         DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
-        BandedBatch band_args = banded_batch(batch, table, schedule_all, scores, nullptr, leftovers, leftover_count);
-        band_args.decisions = decisions;
-        band_args.decision_offsets = word_offsets;
-        band_args.first_pair = first_pair;
-        banded_launch(gpu, band_args, true);
+        launch_bands(gpu, batch, table, schedule_all, scores, leftovers, leftover_count, true, decisions, word_offsets,
+                     first_pair);
     }
     affine_launch_all(gpu, batch, table, schedule_all, true, args);
     unsigned int left = 0;
-    if (schedule_all.counts[kBandClass] > 0) {
+    if (band_pairs(schedule_all) > 0) {
         DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         if (left > 0) {

@@ -204,14 +204,263 @@ __global__ void __launch_bounds__(kBlock) banded_kernel(BandedBatch b) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// The 16-bit pair sweep: two pairs a lane group, pair A in every register's low half and pair B in its
+// high half, so each DPX instruction on 16-bit pairs (full rate on this part, as the 32-bit ones) moves
+// two cells. The layout and the recurrence are the 32-bit sweep's; values are held as kPairBias plus the
+// shifted cell (unreached cells from kPairUnreached), all within [0, 0x8000) by band_pair_limit, so a
+// half never overflows and an add across the whole register never carries from one half to the other.
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t pack2(int32_t low, int32_t high) {
+    return (uint32_t(low) & 0xFFFFu) | (uint32_t(high) << 16);
+}
+__device__ __forceinline__ int32_t low_half(uint32_t v) { return int32_t(int16_t(uint16_t(v & 0xFFFFu))); }
+__device__ __forceinline__ int32_t high_half(uint32_t v) { return int32_t(int16_t(uint16_t(v >> 16))); }
+
+// The halves' maximum: the DPX maximum floored at zero, which every value here already is at or above.
+__device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) { return __vimax_s16x2_relu(a, b); }
+
+// Sets bit `at` (and bit 16 + at) of `acc` where a half of `v` has bit 15 clear. `v` = b - a + 0x8000 per
+// half (halves in [0, 0x8000), so nothing crosses between them) has bit 15 set exactly where b >= a: a
+// clear bit records a > b.
+template <int AT>
+__device__ __forceinline__ uint32_t place_clear(uint32_t acc, uint32_t v) {
+    constexpr uint32_t mask = (1u << AT) | (1u << (16 + AT));
+    return acc | (~(v >> (15 - AT)) & mask);
+}
+
+template <bool RECORD>
+__global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) {
+    constexpr int G = kBandLanes, C = kBandColumns;
+    constexpr int GPW = 32 / G;      // lane groups a warp
+    constexpr int PPW = 2 * GPW;     // pairs a warp
+    __shared__ uint32_t rows8[4];
+    if (threadIdx.x < 4) rows8[threadIdx.x] = b.rows8[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int member = lane % G;
+    const int group = lane / G;
+    const int warp = int((int64_t(blockIdx.x) * kBlock + threadIdx.x) >> 5);
+    const int warps = int((int64_t(gridDim.x) * kBlock) >> 5);
+    const int32_t opening = b.open - b.extend;
+    const uint32_t opening2 = pack2(opening, opening);
+    const uint32_t unreached2 = pack2(kPairUnreached, kPairUnreached);
+    const uint32_t at_least = 0x80008000u;                             // b - a + this: bit 15 where b >= a
+    const uint32_t at_least_open = pack2(0x8000 + opening, 0x8000 + opening);  // b + opening >= a
+
+    for (int64_t base = int64_t(warp) * PPW; base < b.count; base += int64_t(warps) * PPW) {
+        const int64_t item = base + 2 * group;
+        bool live[2];
+        uint32_t pair[2] = {0, 0};
+        PairShape sh[2] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        int rows[2], cols[2], low[2], end_place[2], rows_pad[2];
+        int64_t dec_base[2] = {0, 0};
+        int group_rows = 0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            live[h] = item + h < b.count;
+            if (live[h]) {
+                pair[h] = b.order[item + h];
+                sh[h] = b.shapes[pair[h]];
+            }
+            rows[h] = int(sh[h].rows);
+            cols[h] = int(sh[h].columns);
+            low[h] = live[h] ? band_low_for(rows[h], cols[h]) : 0;
+            end_place[h] = cols[h] - rows[h] - low[h];
+            rows_pad[h] = (rows[h] + 3) & ~3;
+            if (RECORD && live[h])
+                dec_base[h] = b.decision_offsets[pair[h] - b.first_pair] + int64_t(member) * rows_pad[h];
+            group_rows = max(group_rows, live[h] ? rows[h] : 0);
+        }
+        const int first_place = member * C;
+        int warp_rows = group_rows;
+#pragma unroll
+        for (int span = 16; span > 0; span >>= 1) warp_rows = max(warp_rows, __shfl_xor_sync(kFull, warp_rows, span));
+
+        // Row 0: the origin, the first row's shifted border `opening`, left of the matrix unreached.
+        uint32_t H[C], D[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            int32_t v[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = low[h] + first_place + k;
+                v[h] = c < 0 ? kPairUnreached : (c == 0 ? kPairBias : kPairBias + opening);
+            }
+            H[k] = pack2(v[0], v[1]);
+            D[k] = unreached2;
+        }
+        int32_t reported[2] = {0, 0};
+        uint2 buffered[2][2];  // [pair][row of two]: the rows' 64-bit words, low and high 32 bits
+
+        for (int r0 = 1; r0 <= warp_rows; r0 += 16) {
+            // Selectors of 32 consecutive columns from r0 + low + first_place, both pairs in one: bytes 0-1
+            // pick pair A's entry (sign-extended to 16 bits) from its row, bytes 2-3 pair B's.
+            uint32_t window[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                uint32_t y[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int column = r0 + low[h] + first_place + j;
+                    y[h] = (live[h] && column >= 1 && column <= cols[h])
+                               ? letter_at<2>(b.tape, sh[h].second_word, uint32_t(column - 1))
+                               : 0u;
+                }
+                window[j] = (17u * y[0] + 128u) | ((17u * y[1] + 196u) << 8);
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int row = r0 + u;
+                if (row <= warp_rows) {
+                    const uint32_t nextH = __shfl_down_sync(kFull, H[0], 1, G);
+                    const uint32_t nextD = __shfl_down_sync(kFull, D[0], 1, G);
+                    uint32_t x_letter[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        x_letter[h] = (live[h] && row <= rows[h])
+                                          ? letter_at<2>(b.tape, sh[h].first_word, uint32_t(row - 1))
+                                          : 0u;
+                    const uint32_t trA = rows8[x_letter[0]], trB = rows8[x_letter[1]];
+                    uint32_t X[C];
+                    uint32_t S = unreached2;  // running max of X + opening along this lane's places
+                    uint32_t acc[4] = {0, 0, 0, 0};
+                    // Pass 1: the deletion layer, the best of the diagonal and deletion moves, and (scores)
+                    // each place's best insertion from this lane's earlier places.
+#pragma unroll
+                    for (int k = 0; k < C; ++k) {
+                        const uint32_t Hup = k + 1 < C ? H[k + 1] : (member == G - 1 ? unreached2 : nextH);
+                        const uint32_t Dup = k + 1 < C ? D[k + 1] : (member == G - 1 ? unreached2 : nextD);
+                        const uint32_t sub = uint32_t(prmt(trA, trB, window[k + u]));
+                        const uint32_t dn = __viaddmax_s16x2(Hup, opening2, Dup);
+                        if (RECORD) {
+                            const uint32_t xd = __viaddmax_s16x2(H[k], sub, 0u);  // H + sub: never below 0
+                            X[k] = max2(xd, dn);
+                            // gotoh.mojo:173-186 decide: the source leaves the diagonal only where the
+                            // deletion beats it; a deletion run extends only where extending beats opening.
+                            const uint32_t del = xd - dn + at_least;         // bit 15 clear: dn > xd
+                            const uint32_t ext = Hup - Dup + at_least_open;  // clear: Dup > Hup + opening
+                            switch (k & 3) {
+                                case 0: acc[k >> 2] = place_clear<2>(place_clear<0>(acc[k >> 2], del), ext); break;
+                                case 1: acc[k >> 2] = place_clear<6>(place_clear<4>(acc[k >> 2], del), ext); break;
+                                case 2: acc[k >> 2] = place_clear<10>(place_clear<8>(acc[k >> 2], del), ext); break;
+                                default: acc[k >> 2] = place_clear<14>(place_clear<12>(acc[k >> 2], del), ext); break;
+                            }
+                            S = __viaddmax_s16x2(X[k], opening2, S);
+                        } else {
+                            const uint32_t x = __viaddmax_s16x2(H[k], sub, dn);
+                            X[k] = S;  // the insertion from this lane's earlier places
+                            S = __viaddmax_s16x2(x, opening2, S);
+                            H[k] = x;
+                        }
+                        D[k] = dn;
+                    }
+                    // Exclusive prefix maximum of the four lanes' running maxima.
+                    uint32_t reach = __shfl_up_sync(kFull, S, 1, G);
+                    if (member == 0) reach = unreached2;
+                    {
+                        const uint32_t further = __shfl_up_sync(kFull, reach, 1, G);
+                        if (member >= 1) reach = max2(reach, further);
+                        const uint32_t further2 = __shfl_up_sync(kFull, reach, 2, G);
+                        if (member >= 2) reach = max2(reach, further2);
+                    }
+                    if (RECORD) {
+                        // Pass 2: the insertion layer (the best earlier X plus an opening), the scores, and the
+                        // insertion decisions: the source is inserting where the insertion beats both moves (ties
+                        // go to the diagonal, then the deletion), and an insertion run extends where the left
+                        // cell's insertion beats its score plus an opening.
+                        uint32_t S2 = reach;
+                        uint32_t prevH = 0, prevI = 0;
+#pragma unroll
+                        for (int k = 0; k < C; ++k) {
+                            const uint32_t I = S2;
+                            S2 = __viaddmax_s16x2(X[k], opening2, S2);
+                            H[k] = max2(X[k], I);
+                            const uint32_t ins = X[k] - I + at_least;  // bit 15 clear: I > X
+                            // The inserting bit at 4k + 1, and the deleting bit below it cleared where set.
+                            uint32_t y = 0;
+                            switch (k & 3) {
+                                case 0: y = place_clear<1>(0u, ins); break;
+                                case 1: y = place_clear<5>(0u, ins); break;
+                                case 2: y = place_clear<9>(0u, ins); break;
+                                default: y = place_clear<13>(0u, ins); break;
+                            }
+                            acc[k >> 2] = (acc[k >> 2] & ~(y >> 1)) | y;
+                            if (k > 0) {
+                                const uint32_t grow = prevH - prevI + at_least_open;  // clear: I > H + opening
+                                switch (k & 3) {
+                                    case 0: acc[k >> 2] = place_clear<3>(acc[k >> 2], grow); break;
+                                    case 1: acc[k >> 2] = place_clear<7>(acc[k >> 2], grow); break;
+                                    case 2: acc[k >> 2] = place_clear<11>(acc[k >> 2], grow); break;
+                                    default: acc[k >> 2] = place_clear<15>(acc[k >> 2], grow); break;
+                                }
+                            }
+                            prevH = H[k];
+                            prevI = I;
+                        }
+                        // Place 0's insertion-run bit: the left cell is the previous lane's last place.
+                        uint32_t leftH = __shfl_up_sync(kFull, prevH, 1, G);
+                        uint32_t leftI = __shfl_up_sync(kFull, prevI, 1, G);
+                        if (member == 0) {
+                            leftH = unreached2;
+                            leftI = unreached2;
+                        }
+                        acc[0] = place_clear<3>(acc[0], leftH - leftI + at_least_open);
+                        // Each pair's 64-bit word of the row: places 0-7 from acc[0..1], 8-15 from acc[2..3].
+                        const int slot = u & 1;
+                        buffered[0][slot] = make_uint2(uint32_t(prmt(acc[0], acc[1], 0x5410u)),
+                                                       uint32_t(prmt(acc[2], acc[3], 0x5410u)));
+                        buffered[1][slot] = make_uint2(uint32_t(prmt(acc[0], acc[1], 0x7632u)),
+                                                       uint32_t(prmt(acc[2], acc[3], 0x7632u)));
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            if (live[h] && row <= rows[h] && (slot == 1 || row == rows[h])) {
+                                uint4 *at = reinterpret_cast<uint4 *>(b.decisions + dec_base[h] + ((row - 1) & ~1));
+                                *at = make_uint4(buffered[h][0].x, buffered[h][0].y, buffered[h][1].x,
+                                                 buffered[h][1].y);
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < C; ++k) H[k] = __vimax3_s16x2(H[k], X[k], reach);
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        if (live[h] && row == rows[h]) {
+#pragma unroll
+                            for (int k = 0; k < C; ++k)
+                                if (first_place + k == end_place[h])
+                                    reported[h] = (h == 0 ? low_half(H[k]) : high_half(H[k])) - kPairBias;
+                        }
+                    }
+                }
+            }
+        }
+        // The corner's lane reports each pair; the band's score is accepted when the band proves it.
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const bool holder = live[h] && end_place[h] >= first_place && end_place[h] < first_place + C;
+            if (holder) {
+                const int64_t score = int64_t(reported[h]) + int64_t(rows[h] + cols[h]) * b.extend;
+                const bool proven = band_proves(score, rows[h], cols[h], low[h], b.best, b.open, b.extend);
+                b.scores[pair[h]] = int32_t(score);
+                if (b.proven) b.proven[pair[h]] = proven ? 1 : 0;
+                if (!proven) b.leftovers[atomicAdd(b.leftover_count, 1u)] = pair[h];
+            }
+        }
+    }
+}
+
 }  // namespace
 
-void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record) {
+void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16) {
     if (batch.count <= 0) return;
-    auto fn = record ? &banded_kernel<true> : &banded_kernel<false>;
+    auto fn = pairs_of_16 ? (record ? &banded_pairs_kernel<true> : &banded_pairs_kernel<false>)
+                          : (record ? &banded_kernel<true> : &banded_kernel<false>);
     int per_sm = 0;
     DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
-    const int64_t pairs_per_block = kBlock / kBandLanes;
+    const int64_t pairs_per_block = (pairs_of_16 ? 2 : 1) * kBlock / kBandLanes;
     int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
     const int64_t needed = (batch.count + pairs_per_block - 1) / pairs_per_block;
     if (blocks > needed) blocks = needed;

@@ -50,6 +50,26 @@ __host__ __device__ inline bool band_proves(int64_t score, int64_t rows, int64_t
     return true;
 }
 
+// The 16-bit pair sweep (banded_pairs_kernel) holds every value a pair's band takes as a 16-bit half of a
+// register: real cells plus kPairBias, cells no path reaches from kPairUnreached up. With K the largest
+// step a cell takes from its neighbour (the largest shifted table entry, or a gap's opening), a real
+// value lies within (rows + columns + 2) K of the bias; the sweep also runs a few columns right of a
+// pair's end and rows below it (to its group's last row), so a batch's pairs may take it when rows +
+// columns + 130 <= kPairReach / K. Then real values lie in [bias - reach, bias + reach], unreached ones
+// in [unreached, unreached + reach], the two stay apart by more than K, and every value and every
+// value plus one step lies in [0, 0x8000): no half overflows and no half borrows from the other.
+constexpr int32_t kPairBias = 16384;
+constexpr int32_t kPairUnreached = 1024;
+constexpr int32_t kPairReach = 7400;
+
+// The largest rows + columns a pair of the 16-bit sweep may have under a table whose largest step is
+// `step` (0 when the table's entries do not fit a byte or the step is past 512).
+__host__ __device__ inline int32_t band_pair_limit(int32_t step, bool bytes_fit) {
+    if (!bytes_fit || step <= 0 || step > 512) return 0;
+    const int32_t limit = kPairReach / step - 130;
+    return limit > 0 ? limit : 0;
+}
+
 struct BandedBatch {
     const uint32_t *tape;
     const PairShape *shapes;
@@ -57,6 +77,7 @@ struct BandedBatch {
     int64_t count;
     int32_t open, extend, best;
     uint2 rows16[4];        // the shifted table, 16 bits an entry
+    uint32_t rows8[4];      // the shifted table, a byte an entry (the 16-bit pair sweep)
     int32_t *scores;        // by pair
     uint8_t *proven;        // by pair, when given: 1 when the band proved its score
     uint32_t *leftovers;    // pairs the band did not prove
@@ -67,7 +88,8 @@ struct BandedBatch {
     int64_t first_pair;
 };
 
-// Launches the banded sweep (scores, or with `record` scores and decisions) over `batch.count` pairs.
-void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record);
+// Launches the banded sweep (scores, or with `record` scores and decisions) over `batch.count` pairs; with
+// `pairs_of_16` the 16-bit pair sweep, two pairs a lane group (every pair within band_pair_limit).
+void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16 = false);
 
 }  // namespace dinara

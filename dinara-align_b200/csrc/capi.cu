@@ -314,6 +314,19 @@ struct Timer {
     }
 };
 
+// The learned band's first thresholds, with the device time they took.
+const int64_t *timed_predictions(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
+                                 double *ms) {
+    DINARA_CUDA(cudaEventRecord(gpu->start, gpu->stream));
+    const int64_t *starts = predict_thresholds(gpu, pairs, letters, offsets);
+    DINARA_CUDA(cudaEventRecord(gpu->stop, gpu->stream));
+    DINARA_CUDA(cudaEventSynchronize(gpu->stop));
+    float elapsed = 0.f;
+    DINARA_CUDA(cudaEventElapsedTime(&elapsed, gpu->start, gpu->stop));
+    *ms = elapsed;
+    return starts;
+}
+
 }  // namespace
 
 extern "C" {
@@ -585,16 +598,18 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
         to_device(gpu, letters_device, letters + first, size_t(total), gpu->pinned_in);
         to_device(gpu, offsets_device, relative.data(), relative.size() * sizeof(int64_t), gpu->pinned_small);
         const int64_t *starts = nullptr;
+        double predict_ms = 0.0;
         if (policy == DINARA_BAND_GIVEN) {
             int64_t *device_starts = gpu->predictions.ensure<int64_t>(size_t(pairs));
             to_device(gpu, device_starts, plan->start_thresholds, size_t(pairs) * sizeof(int64_t), gpu->pinned_small);
             starts = device_starts;
         } else if (policy == DINARA_BAND_LEARNED) {
-            starts = predict_thresholds(gpu, pairs, letters_device, offsets_device);
+            starts = timed_predictions(gpu, pairs, letters_device, offsets_device, &predict_ms);
         }
         int64_t *results_device = gpu->scores.ensure<int64_t>(size_t(pairs));
         band_doubling(gpu, pairs, letters_device, offsets_device, starts, plan ? plan->default_start : 0, results_device,
                       report);
+        if (report) report->predict_ms = predict_ms;
         to_host(gpu, results, results_device, size_t(pairs) * sizeof(int64_t));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         if (report) {
@@ -734,10 +749,13 @@ int64_t dinara_gpu_resident_distances(dinara_gpu *gpu, const dinara_band_plan *p
             starts = device_starts;
         }
         Timer timer(gpu);
-        if (policy == DINARA_BAND_LEARNED) starts = predict_thresholds(gpu, r.pairs, r.letters_device, r.offsets_device);
+        double predict_ms = 0.0;
+        if (policy == DINARA_BAND_LEARNED)
+            starts = timed_predictions(gpu, r.pairs, r.letters_device, r.offsets_device, &predict_ms);
         int64_t *results_device = gpu->scores.ensure<int64_t>(size_t(r.pairs));
         band_doubling(gpu, r.pairs, r.letters_device, r.offsets_device, starts, plan ? plan->default_start : 0,
                       results_device, report);
+        if (report) report->predict_ms = predict_ms;
         if (report) report->full_cells = r.cells;
         r.last = 2;
         timer.finish(timing, r.cells);
@@ -824,6 +842,25 @@ int64_t dinara_gpu_predictor_get(dinara_gpu *gpu, float *parameters, double *mar
         }
         if (margin) *margin = gpu->predictor_margin;
         if (slack) *slack = gpu->predictor_slack;
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_predictor_margins(dinara_gpu *gpu, int64_t set, double *margins) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !margins) throw Failure(DINARA_INVALID_MODE, "no context or margins");
+        if (!set) {
+            for (int k = 0; k < 4; ++k) margins[k] = gpu->predictor_margins[k];
+            return 0;
+        }
+        for (int k = 0; k < 4; ++k)
+            if (!(margins[k] >= 0.0)) throw Failure(DINARA_INVALID_MODE, "a negative margin");
+        double widest = 0.0;
+        for (int k = 0; k < 4; ++k) {
+            gpu->predictor_margins[k] = margins[k];
+            widest = std::max(widest, margins[k]);
+        }
+        gpu->predictor_margin = widest;
         return 0;
     });
 }

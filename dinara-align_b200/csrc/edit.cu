@@ -295,11 +295,13 @@ __global__ void band_keys_kernel(const EditPair *__restrict__ pairs, const uint3
 }
 
 // After a round: a result within its threshold, or from a band as wide as the matrix, is the distance;
-// the rest double their thresholds and go round again.
+// the rest go round again with the threshold doubled, capped by the cheapest alignment any round found
+// for the pair (band.mojo:619-657: a round's result is a real alignment's cost, so a threshold at it
+// reaches the distance).
 __global__ void settle_kernel(const EditPair *__restrict__ pairs, const uint32_t *__restrict__ pending,
                               const unsigned int *__restrict__ pending_count, int64_t *__restrict__ thresholds,
-                              const int64_t *__restrict__ banded, int64_t *__restrict__ results,
-                              int64_t *__restrict__ rounds, uint32_t *__restrict__ next,
+                              int64_t *__restrict__ cheapest, const int64_t *__restrict__ banded,
+                              int64_t *__restrict__ results, int64_t *__restrict__ rounds, uint32_t *__restrict__ next,
                               unsigned int *__restrict__ next_count) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= *pending_count) return;
@@ -322,7 +324,10 @@ __global__ void settle_kernel(const EditPair *__restrict__ pairs, const uint32_t
     } else if (!covered && t >= int64_t(e.n) + e.m) {
         results[pair] = DINARA_OUT_OF_MEMORY;
     } else {
-        thresholds[pair] = 2 * t;
+        // A window short of its band proves nothing at the cap, so only a covered round caps the next.
+        const int64_t best = found < cheapest[pair] ? found : cheapest[pair];
+        cheapest[pair] = best;
+        thresholds[pair] = covered && best < 2 * t ? best : 2 * t;
         next[atomicAdd(next_count, 1u)] = pair;
     }
 }
@@ -397,9 +402,10 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 
-    int64_t *thresholds = gpu->thresholds.ensure<int64_t>(3 * size_t(pairs));
+    int64_t *thresholds = gpu->thresholds.ensure<int64_t>(4 * size_t(pairs));
     int64_t *firsts = thresholds + pairs;
     int64_t *rounds = thresholds + 2 * pairs;
+    int64_t *cheapest = thresholds + 3 * pairs;
     int64_t *banded = gpu->distances.ensure<int64_t>(size_t(pairs));
     uint32_t *pending = gpu->pending.ensure<uint32_t>(size_t(pairs));
     uint32_t *next = gpu->pending_next.ensure<uint32_t>(size_t(pairs));
@@ -408,6 +414,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     unsigned long long *swept = reinterpret_cast<unsigned long long *>(counters + 32);
     DINARA_CUDA(cudaMemsetAsync(counters, 0, 64 * sizeof(unsigned int), stream));
     DINARA_CUDA(cudaMemsetAsync(rounds, 0, size_t(pairs) * sizeof(int64_t), stream));
+    DINARA_CUDA(cudaMemsetAsync(cheapest, 0x7f, size_t(pairs) * sizeof(int64_t), stream));  // above any cost
     start_kernel<<<thread_blocks, threads, 0, stream>>>(info, pairs, first_thresholds_device,
                                                         default_start > 0 ? default_start : 256, status, thresholds,
                                                         firsts, pending, counters);
@@ -422,7 +429,12 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     int64_t count = host_counts[0];
     int64_t launches = 0;
     float kernel_ms = 0.f;
+    int64_t round = 0;
+    int64_t round_pairs[16] = {0}, round_launches[16] = {0};
+    double round_ms[16] = {0.0};
     while (count > 0) {
+        const int64_t launches_before = launches;
+        const int64_t round_count = count;
         // Order the round's pairs: by band shape, longest text first.
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, (1 + kBandShapes) * sizeof(unsigned int), stream));
         const unsigned blocks = unsigned((count + threads - 1) / threads);
@@ -485,8 +497,8 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         }
         DINARA_CUDA(cudaEventRecord(gpu->stop, stream));
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned int), stream));
-        settle_kernel<<<blocks, threads, 0, stream>>>(info, order_sorted, counters, thresholds, banded, results, rounds,
-                                                      next, counters + 1);
+        settle_kernel<<<blocks, threads, 0, stream>>>(info, order_sorted, counters, thresholds, cheapest, banded,
+                                                      results, rounds, next, counters + 1);
         gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         DINARA_CUDA(cudaMemcpyAsync(counters, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToDevice, stream));
@@ -495,6 +507,12 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         float ms = 0.f;
         DINARA_CUDA(cudaEventElapsedTime(&ms, gpu->start, gpu->stop));
         kernel_ms += ms;
+        if (round < 16) {
+            round_pairs[round] = round_count;
+            round_launches[round] = launches - launches_before;
+            round_ms[round] = ms;
+        }
+        ++round;
         count = host_counts[0];
         std::swap(pending, next);
     }
@@ -514,6 +532,11 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         report->overshoot = int64_t(host[3]);
         report->undershoot = int64_t(host[4]);
         report->kernel_ms = kernel_ms;
+        for (int k = 0; k < 16; ++k) {
+            report->round_pairs[k] = round_pairs[k];
+            report->round_launches[k] = round_launches[k];
+            report->round_ms[k] = round_ms[k];
+        }
     }
 }
 

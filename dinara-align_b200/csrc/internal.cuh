@@ -116,7 +116,7 @@ struct dinara_gpu {
     cudaStream_t stream = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
     // Side streams that let a round's launches of different shapes run at once, joined by events.
-    static constexpr int kSideStreams = 8;
+    static constexpr int kSideStreams = 18;  // one for each band window shape
     cudaStream_t side[kSideStreams] = {nullptr};
     cudaEvent_t fork = nullptr, joins[kSideStreams] = {nullptr};
     std::string error;

@@ -115,47 +115,59 @@ __global__ void generate_letters_kernel(uint64_t seed, int64_t pairs, double low
 // The sketch
 // ------------------------------------------------------------------------------------------------
 
-__device__ __forceinline__ int base_code(uint32_t byte) {
-    switch (byte) {
-        case 'A': return 0;
-        case 'C': return 1;
-        case 'G': return 2;
-        case 'T': return 3;
-        default: return -1;
-    }
+// A letter's 2-bit code (A 0, C 1, G 2, T 3), or -1 for any byte but those four: bits 1, 3, 7 and 20 of
+// the mask stand for A, C, G and T (0x41, 0x43, 0x47, 0x54 less 0x40).
+__device__ __forceinline__ int code_of(uint32_t byte) {
+    const bool dna = (byte & 0xE0u) == 0x40u && ((0x0010008Au >> (byte & 31u)) & 1u);
+    return dna ? int(((byte >> 1) & 3u) ^ ((byte >> 2) & 1u)) : -1;
 }
 
-// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints), `sign` +1 or -1: each lane
-// takes a stretch, rolling its 4-mer across letters; a k-mer holding another letter is skipped.
+// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints), `sign` +1 or -1; a 4-mer holding
+// another letter is skipped.
 __device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, int *counts) {
+    // The warp reads the sequence 512 letters at a time, lane i the 4-mers starting at the 16 letters from
+    // 16i, through six aligned words that hold those letters and the three after them (a word may reach
+    // three bytes past the sequence's end: device letter buffers keep 16 bytes of room there).
     const int lane = threadIdx.x & 31;
-    const int64_t stretch = (length + 31) / 32;
-    const int64_t begin = lane * stretch, end = min(length, begin + stretch);
-    // The k-mers starting in [begin, end) each need the 3 letters after them.
-    int valid = 0;
-    uint32_t code = 0;
-    for (int64_t i = begin - 3 < 0 ? 0 : begin - 3; i < end + 3 && i < length; ++i) {
-        const int c = base_code(sequence[i]);
-        if (c < 0) {
-            valid = 0;
-            code = 0;
-            continue;
+    const uintptr_t origin = reinterpret_cast<uintptr_t>(sequence);
+    const uintptr_t end = origin + uintptr_t(length);
+    for (int64_t chunk = 0; chunk < length; chunk += 512) {
+        const int64_t first = chunk + 16 * lane;
+        if (first >= length) continue;
+        const uintptr_t address = origin + uintptr_t(first);
+        const uintptr_t aligned = address & ~uintptr_t(3);
+        const uint32_t *words = reinterpret_cast<const uint32_t *>(aligned);
+        uint32_t w[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) w[i] = aligned + 4 * uintptr_t(i) < end ? __ldg(words + i) : 0u;
+        const uint32_t shift = uint32_t(address & 3u) * 8u;
+        uint32_t a[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) a[i] = __funnelshift_r(w[i], w[i + 1], shift);
+        uint32_t kmer = 0;
+        int run = 0;
+#pragma unroll
+        for (int j = 0; j < 19; ++j) {
+            const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
+            kmer = ((kmer << 2) | uint32_t(c & 3)) & 0xFFu;
+            run = c < 0 ? 0 : run + 1;
+            if (j >= 3 && run >= 4) atomicAdd(&counts[kmer], sign);
         }
-        code = ((code << 2) | uint32_t(c)) & 0xFFu;
-        valid = valid < 4 ? valid + 1 : 4;
-        const int64_t start = i - 3;
-        if (valid == 4 && start >= begin && start < end) atomicAdd(&counts[code], sign);
     }
 }
 
-// Writes a pair's 257 features, scaled as the network reads them: the count differences over the root of
-// the mean length, since each error moves a handful of 4-mers between bins and the differences' squares
-// then sum to about the errors a letter whatever the length; and the length ratio.
+// Writes a pair's 257 features, scaled as the network reads them: each count difference squared, times
+// 32 over the mean length, since an error moves a handful of 4-mers between bins and the squares of the
+// differences then sum to about eight times the errors whether a bin holds one move or many of either
+// sign, so their sum over the length tracks the error rate; and the length ratio.
 __device__ void features_of(const int *counts, int64_t reference, int64_t query, float *out, int stride) {
     const int lane = threadIdx.x & 31;
     const float mean = 0.5f * float(reference + query);
-    const float scale = rsqrtf(mean > 1.0f ? mean : 1.0f);
-    for (int k = lane; k < 256; k += 32) out[int64_t(k) * stride] = float(counts[k]) * scale;
+    const float scale = 32.0f / (mean > 1.0f ? mean : 1.0f);
+    for (int k = lane; k < 256; k += 32) {
+        const float difference = float(counts[k]);
+        out[int64_t(k) * stride] = difference * difference * scale;
+    }
     if (lane == 0) {
         const int64_t low = min(reference, query), high = max(reference, query);
         out[int64_t(256) * stride] = high > 0 ? float(low) / float(high) : 1.0f;
@@ -591,8 +603,9 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
                                 cudaMemcpyDeviceToHost, stream));
     DINARA_CUDA(cudaStreamSynchronize(stream));
     // Each held-out pair's ratio of distance (less the slack) to guess, by length class; a class's margin
-    // reaches the asked share of its pairs. A long pair that undershoots costs a whole extra round, a short
-    // one that overshoots only a wider band, so every class is held to the same coverage of its own pairs.
+    // reaches a share of its pairs. A pair that undershoots sweeps again, and the round it adds lasts as
+    // long as its longest pair's sweep, so the longer classes are held to a higher share: the asked
+    // coverage for pairs under 1,000 letters, a third of the misses past it under 4,096, a tenth longer.
     std::vector<double> ratios[4];
     double squared = 0.0;
     for (int64_t k = 0; k < held; ++k) {
@@ -605,12 +618,14 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
         squared += e * e;
     }
     const double coverage = std::min(std::max(options.coverage, 0.5), 0.999);
+    const double misses[4] = {1.0, 1.0, 1.0 / 3.0, 0.1};
     double widest = 1.0;
     for (int c = 0; c < 4; ++c) {
         double margin = 1.0;
         if (!ratios[c].empty()) {
             std::sort(ratios[c].begin(), ratios[c].end());
-            margin = std::max(1.0, ratios[c][size_t(double(ratios[c].size() - 1) * coverage)]);
+            const double share = 1.0 - (1.0 - coverage) * misses[c];
+            margin = std::max(1.0, ratios[c][size_t(double(ratios[c].size() - 1) * share)]);
         }
         gpu->predictor_margins[c] = margin;
         widest = std::max(widest, margin);

@@ -66,7 +66,8 @@ __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int
 // the highest), then strips of its width, then rows, so a descending sort puts each class's longest pairs
 // first and warps hold pairs of like size. Counts each class.
 __global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ list,
-                                     int64_t first, int64_t count, int record, int band, uint32_t *__restrict__ keys,
+                                     int64_t first, int64_t count, int record, int band, int32_t pair_limit,
+                                     uint32_t *__restrict__ keys,
                                      uint32_t *__restrict__ order, unsigned int *__restrict__ class_counts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
@@ -76,7 +77,7 @@ __global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const
     int cls;
     uint32_t strips = 0;
     if (band && band_eligible(shape.rows, shape.columns)) {
-        cls = kBandClass;
+        cls = int64_t(shape.rows) + shape.columns <= pair_limit ? kBandPairsClass : kBandClass;
     } else {
         cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);
         const uint32_t width = uint32_t(affine_lanes(cls) * affine_columns(cls));
@@ -102,7 +103,7 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
 }
 
 Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
-                   bool record, bool band) {
+                   bool record, bool band, int32_t pair_limit) {
     Schedule out;
     for (int c = 0; c < kClasses; ++c) out.counts[c] = 0;
     out.order = nullptr;
@@ -115,7 +116,7 @@ Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list
     DINARA_CUDA(cudaMemsetAsync(class_counts, 0, kClasses * sizeof(unsigned int), gpu->stream));
     const int threads = 256;
     schedule_keys_kernel<<<unsigned((count + threads - 1) / threads), threads, 0, gpu->stream>>>(
-        shapes, list, first, count, record ? 1 : 0, band ? 1 : 0, keys, order, class_counts);
+        shapes, list, first, count, record ? 1 : 0, band ? 1 : 0, pair_limit, keys, order, class_counts);
     DINARA_CUDA(cudaGetLastError());
     gpu->launches += 1;
     size_t scratch = 0;

@@ -12,10 +12,12 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
                 const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown);
 
 // A batch's sweep order: pairs by class (the whole-matrix shape classes 0-4, affine_shape_for with
-// `record`, and with `band` the proven band, kBandClass), classes in descending order, then strips and rows
-// descending. `order` is valid on the device until the next call.
-constexpr int kClasses = 6;
+// `record`; with `band` the proven band, kBandClass, and of those the pairs whose rows and columns sum to
+// at most `pair_limit`, kBandPairsClass, for the 16-bit pair sweep), classes in descending order, then
+// strips and rows descending. `order` is valid on the device until the next call.
+constexpr int kClasses = 7;
 constexpr int kBandClass = 5;
+constexpr int kBandPairsClass = 6;
 struct Schedule {
     const uint32_t *order;
     int64_t counts[kClasses];
@@ -23,6 +25,6 @@ struct Schedule {
 
 // The order of pairs [first, first + count), or of the `count` pairs listed in `list` (device) when given.
 Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
-                  bool record, bool band);
+                  bool record, bool band, int32_t pair_limit = 0);
 
 }  // namespace dinara

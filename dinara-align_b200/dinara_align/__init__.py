@@ -419,7 +419,7 @@ def distances_tape(tape: Tape, *, policy: int = native.BAND_PLAIN, start_thresho
                                                    native.pointer(out, ctypes.c_int64), ctypes.byref(summary))
     native.check(code, handle)
     if report:
-        return out[:pairs], {name: getattr(summary, name) for name, _ in native.CBandReport._fields_}
+        return out[:pairs], summary.as_dict()
     return out[:pairs]
 
 

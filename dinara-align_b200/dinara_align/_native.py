@@ -61,7 +61,18 @@ class CBandPlan(ctypes.Structure):
 
 class CBandReport(ctypes.Structure):
     _fields_ = [("rounds", i64), ("pair_rounds", i64), ("words_swept", i64), ("full_cells", i64),
-                ("first_round_hits", i64), ("overshoot", i64), ("undershoot", i64), ("kernel_ms", ctypes.c_double)]
+                ("first_round_hits", i64), ("overshoot", i64), ("undershoot", i64), ("kernel_ms", ctypes.c_double),
+                ("predict_ms", ctypes.c_double), ("round_pairs", i64 * 16), ("round_launches", i64 * 16),
+                ("round_ms", ctypes.c_double * 16)]
+
+    def as_dict(self) -> dict:
+        """The report as plain numbers, the per-round lists cut at the last round swept."""
+        out = {}
+        rounds = sum(1 for value in self.round_pairs if value > 0)
+        for name, _ in self._fields_:
+            value = getattr(self, name)
+            out[name] = list(value)[:rounds] if name.startswith("round_") else value
+        return out
 
 
 _lib = None

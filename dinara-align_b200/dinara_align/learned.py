@@ -13,7 +13,7 @@ from . import Placement, Tape, _placement
 from . import _native as native
 
 PARAMETERS = 20737
-VERSION = 1
+VERSION = 2
 
 
 class TrainOptions(ctypes.Structure):
@@ -40,6 +40,8 @@ def _declare(lib):
     lib.dinara_gpu_predictor_set.argtypes = [vp, f32p, ctypes.c_double, ctypes.c_double]
     lib.dinara_gpu_predictor_get.restype = i64
     lib.dinara_gpu_predictor_get.argtypes = [vp, f32p, f64p, f64p]
+    lib.dinara_gpu_predictor_margins.restype = i64
+    lib.dinara_gpu_predictor_margins.argtypes = [vp, i64, f64p]
     lib.dinara_gpu_predictor_features.restype = i64
     lib.dinara_gpu_predictor_features.argtypes = [vp, i64, vp, i64p, f32p]
     lib.dinara_gpu_predictor_gradients.restype = i64
@@ -86,10 +88,17 @@ class Predictor:
         native.check(self.lib.dinara_gpu_predictor_set(self.handle, native.pointer(flat, ctypes.c_float), margin,
                                                        slack), self.handle)
 
+    def margins(self, values=None) -> list:
+        """The margins by mean length (< 300, < 1,000, < 4,096, longer); installs `values` when given."""
+        out = (ctypes.c_double * 4)(*(values if values is not None else (0.0,) * 4))
+        native.check(self.lib.dinara_gpu_predictor_margins(self.handle, 0 if values is None else 1, out), self.handle)
+        return list(out)
+
     def save(self, path: str) -> None:
-        """A versioned blob: the parameters, the margin and slack, and the training seed."""
+        """A versioned blob: the parameters, the margins and slack, and the training seed."""
         flat, margin, slack = self.parameters()
-        meta = json.dumps({"version": VERSION, "seed": self.seed, "margin": margin, "slack": slack})
+        meta = json.dumps({"version": VERSION, "seed": self.seed, "margin": margin, "margins": self.margins(),
+                           "slack": slack, "features": "squared 4-mer count differences x 32 / mean length"})
         np.savez(path, parameters=flat, meta=np.frombuffer(meta.encode(), dtype=np.uint8))
 
     def load(self, path: str) -> None:
@@ -98,6 +107,7 @@ class Predictor:
         if meta.get("version") != VERSION:
             raise ValueError(f"predictor blob version {meta.get('version')}, expected {VERSION}")
         self.install(data["parameters"], meta["margin"], meta["slack"])
+        self.margins(meta["margins"])
         self.seed = meta.get("seed")
 
     def features(self, tape: Tape) -> np.ndarray:

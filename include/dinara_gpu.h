@@ -161,6 +161,10 @@ typedef struct {
     int64_t overshoot;       /* pairs whose first threshold was at least twice their distance */
     int64_t undershoot;      /* pairs whose first threshold was below their distance */
     double kernel_ms;        /* device time of the band kernels */
+    double predict_ms;       /* device time of the learned band's predictions (DINARA_BAND_LEARNED) */
+    int64_t round_pairs[16]; /* pairs swept in each of the first 16 rounds */
+    int64_t round_launches[16]; /* band kernel launches (window shapes) in each round */
+    double round_ms[16];     /* device time of each round's band kernels */
 } dinara_band_report;
 
 /* Distances over one tape by band doubling from the plan's first thresholds; `report` may be null. */
@@ -206,6 +210,11 @@ int64_t dinara_gpu_predictor_train(dinara_gpu *gpu, const dinara_train_options *
 /* Installs parameters (and the margin and slack) on the context, or reads them back. */
 int64_t dinara_gpu_predictor_set(dinara_gpu *gpu, const float *parameters, double margin, double slack);
 int64_t dinara_gpu_predictor_get(dinara_gpu *gpu, float *parameters, double *margin, double *slack);
+/* The predictor's margins by the pair's mean length (< 300, < 1,000, < 4,096, longer): read into
+ * `margins` (4 doubles) when `set` is 0, else installed from it. Training sets them from its held-out
+ * pairs; dinara_gpu_predictor_set sets all four to its one margin. */
+int64_t dinara_gpu_predictor_margins(dinara_gpu *gpu, int64_t set, double *margins);
+
 /* The 257 features of each pair of a tape, pair-major into `features` (pairs x 257 floats). */
 int64_t dinara_gpu_predictor_features(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
                                       float *features);

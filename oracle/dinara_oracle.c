@@ -439,15 +439,19 @@ static int64_t band_doubling_impl(const uint8_t *a, int64_t n, const uint8_t *b,
     uint64_t *negative = (uint64_t *)malloc((size_t)words * sizeof(uint64_t));
     int64_t delta = tlen - plen;
     int64_t t = start < delta ? delta : start;
-    int64_t result;
+    int64_t result, best = INT64_MAX;
     for (;;) {
         if (rounds) *rounds += 1;
         result = banded_round_impl(pattern, plen, text, tlen, t, planes, codes, count, positive, negative,
                                    words_swept);
         if (only_round || result <= t) break;
-        /* band.mojo:617: the next bound doubles the last; past the whole matrix any band is exact. */
+        /* band.mojo:619-657: the next bound doubles the last, capped by the cheapest alignment a round has
+         * found so far (a round's result is a real alignment's cost); past the whole matrix any band is
+         * exact. */
         if (t >= plen + tlen) break;
+        if (result < best) best = result;
         t = t > 0 ? 2 * t : 1;
+        if (best < t) t = best;
     }
     free(planes);
     free(positive);

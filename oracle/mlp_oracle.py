@@ -48,10 +48,12 @@ def kmer_counts(sequence: bytes) -> np.ndarray:
 
 
 def features(reference: bytes, query: bytes) -> np.ndarray:
-    """The 257 inputs: count differences over the root of the mean length, then the length ratio."""
+    """The 257 inputs: each 4-mer count difference squared, times 32 over the mean length, then the length
+    ratio."""
     out = np.zeros(INPUTS, dtype=np.float64)
     mean = 0.5 * (len(reference) + len(query))
-    out[:256] = (kmer_counts(reference) - kmer_counts(query)) / np.sqrt(max(mean, 1.0))
+    difference = (kmer_counts(reference) - kmer_counts(query)).astype(np.float64)
+    out[:256] = 32.0 * difference ** 2 / max(mean, 1.0)
     low, high = min(len(reference), len(query)), max(len(reference), len(query))
     out[256] = low / high if high > 0 else 1.0
     return out

@@ -169,15 +169,25 @@ def test_refusals(da):
     assert list(statuses) == [-3]
 
 
-@pytest.mark.parametrize("scoring_name", ["config2", "dna"])
+SCORINGS = {
+    "config2": (0, -4, -6, -2),
+    "dna": (2, -4, -4, -2),
+    # A large step from cell to cell: only short pairs fit the 16-bit pair sweep, the rest take 32 bits.
+    "steep": (10, -20, -30, -1),
+    # Entries too large for the 16-bit pair sweep at any length: every band pair takes 32 bits.
+    "wide": (100, -100, -4, -2),
+}
+
+
+@pytest.mark.parametrize("scoring_name", sorted(SCORINGS))
 def test_band_proofs_and_leftovers(da, oracle, scoring_name):
     """Global pairs the proven band serves and pairs it leaves to the whole matrix: error rates from 0 to
-    40%, length differences up to and past the band's 63 diagonals, long pairs; scores and CIGARs must
-    equal the whole-matrix oracle's either way."""
+    40%, length differences up to and past the band's 63 diagonals, long pairs, pairs each side of the
+    16-bit pair sweep's length limit; scores and CIGARs must equal the whole-matrix oracle's either way."""
     from dinara_align import workloads
 
     rng = np.random.default_rng(41)
-    scoring = da.Scoring.uniform(0, -4, -6, -2) if scoring_name == "config2" else da.Scoring.dna()
+    scoring = da.Scoring.uniform(*SCORINGS[scoring_name])
     tapes = []
     for rate in (0.0, 0.02, 0.1, 0.25, 0.4):
         tapes.append(workloads.pairs_with_errors(rng, rng.integers(20, 700, size=120), rate,

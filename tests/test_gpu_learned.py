@@ -51,7 +51,7 @@ def test_gradients_match_oracle(learned):
     assert abs(loss - expected_loss) <= 1e-5 * max(1.0, expected_loss)
 
 
-def test_learned_band_is_exact_and_gains(da, oracle, learned):
+def test_learned_band_is_exact_and_gains(da, oracle, learned, tmp_path):
     """A predictor trained on the GPU starts each pair near its distance: every distance stays exact (the
     doubling that follows is plain band doubling's), and the band sweeps fewer words than plain doubling's
     default start."""
@@ -70,3 +70,11 @@ def test_learned_band_is_exact_and_gains(da, oracle, learned):
     assert learned_report["words_swept"] < 0.8 * plain_report["words_swept"], (plain_report, learned_report)
     predicted, thresholds = predictor.predict(tape)
     assert (thresholds >= 1).all() and np.isfinite(predicted).all()
+    # The blob keeps every length class's margin: loaded back, the thresholds are the same.
+    margins = predictor.margins()
+    blob = str(tmp_path / "predictor.npz")
+    predictor.save(blob)
+    predictor.install(np.zeros(learned.PARAMETERS, dtype=np.float32), 1.0, 0.0)
+    predictor.load(blob)
+    assert predictor.margins() == margins
+    np.testing.assert_array_equal(predictor.predict(tape)[1], thresholds)

@@ -228,4 +228,8 @@ def test_mlp_oracle_kmer_features():
     counts = mlp_oracle.kmer_counts(b"AAAACNAAAA")
     assert counts[0] == 2 and counts.sum() == 3  # AAAA twice, AAAC once; k-mers over N skipped
     f = mlp_oracle.features(b"AAAAA", b"AAAA")
-    assert abs(f[0] - (2 - 1) / np.sqrt(4.5)) < 1e-12 and abs(f[256] - 0.8) < 1e-12
+    assert abs(f[0] - 32.0 * (2 - 1) ** 2 / 4.5) < 1e-12 and abs(f[256] - 0.8) < 1e-12
+    # The squares of the differences lose their sign: the pair either way round reads the same.
+    g = mlp_oracle.features(b"ACGTTGCAAC", b"ACGTAGCAAC")
+    h = mlp_oracle.features(b"ACGTAGCAAC", b"ACGTTGCAAC")
+    assert np.array_equal(g, h) and abs(g[:256].sum() - 32.0 * 8 / 10) < 1e-12
