@@ -288,6 +288,17 @@ KernelFn pick_kernel(int cls, bool local, bool record, int bits, bool smem) {
 #undef DINARA_SHAPE
 }
 
+// The 16-bit pair score sweep for a whole-matrix shape class.
+KernelFn pick_pairs_kernel(int cls, bool local) {
+    switch (cls) {
+        case 0: return local ? &affine_pairs_kernel<4, 16, true> : &affine_pairs_kernel<4, 16, false>;
+        case 1: return local ? &affine_pairs_kernel<8, 16, true> : &affine_pairs_kernel<8, 16, false>;
+        case 2: return local ? &affine_pairs_kernel<16, 16, true> : &affine_pairs_kernel<16, 16, false>;
+        case 3: return local ? &affine_pairs_kernel<16, 20, true> : &affine_pairs_kernel<16, 20, false>;
+        default: return local ? &affine_pairs_kernel<32, 16, true> : &affine_pairs_kernel<32, 16, false>;
+    }
+}
+
 int persistent_blocks(dinara_gpu *gpu, KernelFn fn) {
     int per_sm = 0;
     DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
@@ -312,6 +323,9 @@ TableArgs table_args(const AffineTable &table, bool local) {
             }
             t.rows16[r].x = uint32_t(e[0]) | (uint32_t(e[1]) << 16);
             t.rows16[r].y = uint32_t(e[2]) | (uint32_t(e[3]) << 16);
+            // The byte table of the 16-bit pair sweeps (entries past a byte never reach them).
+            t.rows8[r] = uint32_t(uint8_t(e[0])) | (uint32_t(uint8_t(e[1])) << 8) | (uint32_t(uint8_t(e[2])) << 16) |
+                         (uint32_t(uint8_t(e[3])) << 24);
         }
     }
     return t;
@@ -334,16 +348,17 @@ void upload_table32(dinara_gpu *gpu, const AffineTable &table, bool local, int32
     *out = dev;
 }
 
-// The sorted order's ranges per whole-matrix class: the band's pairs first, then classes 4 to 0.
+// The sorted order's range of each class: classes in descending order (the whole-matrix 16-bit pair
+// classes, then the band's two, then the whole-matrix classes 4 to 0).
 struct Buckets {
-    int64_t begin[kAffineShapes];
-    int64_t end[kAffineShapes];
+    int64_t begin[kClasses];
+    int64_t end[kClasses];
 };
 
 Buckets buckets_of(const Schedule &schedule) {
     Buckets b;
-    int64_t at = schedule.counts[kBandPairsClass] + schedule.counts[kBandClass];
-    for (int cls = kAffineShapes - 1; cls >= 0; --cls) {
+    int64_t at = 0;
+    for (int cls = kClasses - 1; cls >= 0; --cls) {
         b.begin[cls] = at;
         at += schedule.counts[cls];
         b.end[cls] = at;
@@ -376,27 +391,33 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
     if (smem) upload_table32(gpu, table, batch.local, &table32);
     const Buckets b = buckets_of(schedule);
     args.order = schedule.order;
-    for (int cls = kAffineShapes - 1; cls >= 0; --cls) {
-        if (b.end[cls] <= b.begin[cls]) continue;
-        KernelFn fn = pick_kernel(cls, batch.local, record, batch.bits, smem);
-        const int G = smem ? 32 : affine_lanes(cls);
-        const int groups_per_block = kBlock / G;
+    for (int bucket = kClasses - 1; bucket >= 0; --bucket) {
+        if (bucket == kBandClass || bucket == kBandPairsClass) continue;
+        if (b.end[bucket] <= b.begin[bucket]) continue;
+        const bool wide = bucket == kWideClass;
+        const bool pairs16 = !wide && bucket >= kWholePairsClass;
+        const int cls = pairs16 ? bucket - kWholePairsClass : wide ? 4 : bucket;
+        KernelFn fn = wide      ? (batch.local ? &affine_wide_kernel<true> : &affine_wide_kernel<false>)
+                      : pairs16 ? pick_pairs_kernel(cls, batch.local)
+                                : pick_kernel(cls, batch.local, record, batch.bits, smem);
+        const int G = wide ? kBlock : smem && !pairs16 ? 32 : affine_lanes(cls);
+        const int groups_per_block = (pairs16 ? 2 : 1) * kBlock / G;
         int64_t blocks = persistent_blocks(gpu, fn);
-        const int64_t needed = (b.end[cls] - b.begin[cls] + groups_per_block - 1) / groups_per_block;
+        const int64_t needed = (b.end[bucket] - b.begin[bucket] + groups_per_block - 1) / groups_per_block;
         if (blocks > needed) blocks = needed;
         if (blocks < 1) blocks = 1;
         // Carry slots, one a group, each as long as the tallest pair: only a launch whose pairs may be
         // wider than one strip reads them.
-        const int width = smem ? 512 : affine_lanes(cls) * affine_columns(cls);
+        const int width = wide ? 16 * kBlock : smem && !pairs16 ? 512 : affine_lanes(cls) * affine_columns(cls);
         args.carry = nullptr;
         args.carry_stride = 0;
         if (batch.max_columns > uint32_t(width)) {
-            const int64_t slots = blocks * groups_per_block;
+            const int64_t slots = blocks * (kBlock / G);
             args.carry_stride = int64_t(batch.max_rows) + 1;
             args.carry = gpu->carry.ensure<int2>(size_t(slots * args.carry_stride));
         }
-        args.begin = uint32_t(b.begin[cls]);
-        args.end = uint32_t(b.end[cls]);
+        args.begin = uint32_t(b.begin[bucket]);
+        args.end = uint32_t(b.end[bucket]);
         fn<<<dim3(unsigned(blocks)), kBlock, 0, gpu->stream>>>(args, targs, table32);
         DINARA_CUDA(cudaGetLastError());
         gpu->launches += 1;
@@ -417,8 +438,38 @@ int32_t pair_limit_of(const AffineTable &table) {
     return band_pair_limit(step, bytes_fit);
 }
 
+// Which whole-matrix pairs the 16-bit pair score sweep takes (a table of up to four letters on the 2-bit
+// tape): locally, scores reach at most the best entry times the columns swept and fall no lower than a
+// gap's first letter, so the swept columns are held to (30,000 less the gaps) over the best entry;
+// globally, a shifted cell moves at most the largest step a cell, so rows and swept columns are each held
+// to half of 30,000 over it, every value within 30,000 of zero. Entries must fit a byte (shifted, globally).
+PairLimits whole_limits_of(const AffineBatch &batch, const AffineTable &table) {
+    PairLimits limits;
+    if (batch.bits != 2 || !table.packed16) return limits;
+    limits.wide = 1;
+    const int32_t gaps = std::abs(table.open) + std::abs(table.extend);
+    if (gaps > 8000) return limits;
+    if (batch.local) {
+        int32_t best = 1;
+        for (int r = 0; r < table.size; ++r)
+            for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
+        limits.local = 1;
+        limits.whole = (30000 - gaps) / best;
+        return limits;
+    }
+    int32_t step = std::abs(table.open - table.extend);
+    for (int r = 0; r < table.size; ++r)
+        for (int c = 0; c < table.size; ++c) {
+            const int32_t v = table.entries[r * 32 + c] - 2 * table.extend;
+            if (v < -128 || v > 127) return limits;
+            step = std::max(step, std::abs(v));
+        }
+    limits.whole = 30000 / std::max(step, 1) - 4;
+    return limits;
+}
+
 // The band's shifted table and best entry for a banded launch: the band's pairs of the 16-bit pair sweep
-// (`pairs_of_16`), which come first in the order, or the rest after them.
+// (`pairs_of_16`) or the rest, each class's range of the order.
 BandedBatch banded_batch(const AffineBatch &batch, const AffineTable &table, const Schedule &schedule, int32_t *scores,
                          uint8_t *proven, uint32_t *leftovers, unsigned int *leftover_count, bool pairs_of_16) {
     BandedBatch band;
@@ -438,8 +489,10 @@ BandedBatch banded_batch(const AffineBatch &batch, const AffineTable &table, con
         for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
     band.tape = batch.tape;
     band.shapes = batch.shapes;
-    band.order = pairs_of_16 ? schedule.order : schedule.order + schedule.counts[kBandPairsClass];
-    band.count = schedule.counts[pairs_of_16 ? kBandPairsClass : kBandClass];
+    const Buckets buckets = buckets_of(schedule);
+    const int cls = pairs_of_16 ? kBandPairsClass : kBandClass;
+    band.order = schedule.order + buckets.begin[cls];
+    band.count = schedule.counts[cls];
     band.open = table.open;
     band.extend = table.extend;
     band.best = best;
@@ -503,8 +556,9 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
                    int64_t first, int64_t count) {
     if (count <= 0) return;
     const bool band = band_serves(batch, table);
-    const Schedule schedule_all =
-        dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, band, band ? pair_limit_of(table) : 0);
+    PairLimits limits = whole_limits_of(batch, table);
+    limits.band = band ? pair_limit_of(table) : 0;
+    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, band, limits);
     PhaseTimer timer(gpu, &gpu->kernel_ms);
     KernelArgs args;
     std::memset(&args, 0, sizeof args);
@@ -527,7 +581,8 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
         DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         if (left > 0) {
-            const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, false, false);
+            const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, false, false,
+                                                    whole_limits_of(batch, table));
             affine_launch_all(gpu, batch, table, again, false, args);
         }
     }
@@ -570,8 +625,9 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     char *slots = gpu->walk_out.ensure<char>(size_t(totals[1]) + 8);
     int64_t *ends = gpu->spans.ensure<int64_t>(size_t(count) + 1);
     int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(size_t(count) + 1);
-    const Schedule schedule_all =
-        dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band, band ? pair_limit_of(table) : 0);
+    PairLimits limits;
+    limits.band = band ? pair_limit_of(table) : 0;
+    const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band, limits);
 
     PhaseTimer timer(gpu, &gpu->record_ms);
     KernelArgs args;

@@ -54,6 +54,7 @@ struct KernelArgs {
 
 struct TableArgs {
     uint2 rows16[4];       // packed 16-bit entries, letter x at bytes 2x..2x+1
+    uint32_t rows8[4];     // byte entries, letter x at byte x (the 16-bit pair sweep)
     int32_t size;
 };
 
@@ -224,9 +225,12 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                 p.carry[slot * p.carry_stride + row] = make_int2(H[C - 1], I);
                             }
                             if (!LOCAL && row == rows && owned > 0 && first_col + owned == cols) {
+                                // The corner by masks, not by an index into H (which would put H in memory).
 #pragma unroll
-                                for (int k = 0; k < C; ++k)
-                                    if (k == owned - 1) reported = H[k];
+                                for (int k = 0; k < C; ++k) {
+                                    const int32_t hit = -int32_t(k == owned - 1);
+                                    reported = (reported & ~hit) | (H[k] & hit);
+                                }
                             }
                             if (RECORD) {
                                 buffered[u] = (uint64_t(word_hi) << 32) | word_lo;
@@ -285,6 +289,343 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                     p.scores[pair] = reported + total * extend;
                 }
             }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Scores of two pairs a lane group, pair A in every register's low 16 bits and pair B in its high 16 bits:
+// the sweep above, cell for cell, each DPX instruction on 16-bit pairs (full rate on this part, as the
+// 32-bit ones) moving a cell of each pair. The schedule gives it only pairs whose every value, and every
+// value of the cells it sweeps past their ends, stays inside 16 bits: a local score is at most the best
+// entry times the columns swept and never below a gap's opening; a global cell held shifted moves at
+// most the largest shifted entry or opening a step. Cells past a pair's last row read a row of zero
+// entries and cells past its last column a padding of 0 or -1, so neither beats the pair's real cells
+// (a local best) nor feeds them (a global corner).
+// ------------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t halves(int32_t low, int32_t high) {
+    return (uint32_t(low) & 0xFFFFu) | (uint32_t(high) << 16);
+}
+__device__ __forceinline__ int32_t low_of(uint32_t v) { return int32_t(int16_t(uint16_t(v & 0xFFFFu))); }
+__device__ __forceinline__ int32_t high_of(uint32_t v) { return int32_t(int16_t(uint16_t(v >> 16))); }
+
+// A column's selector for both pairs: bytes 0-1 pick pair A's entry (sign-extended) from its row's
+// register, bytes 2-3 pair B's from the other; kPadHalf reads 0 or -1 (a sign of a byte, replicated).
+constexpr uint32_t kPadHalf = 0x99u;
+__device__ __forceinline__ uint32_t pair_selector(uint32_t a, uint32_t b) { return a | (b << 8); }
+__device__ __forceinline__ uint32_t half_selector_a(uint32_t y) { return 17u * y + 128u; }
+__device__ __forceinline__ uint32_t half_selector_b(uint32_t y) { return 17u * y + 196u; }
+
+template <int G, int C, bool LOCAL>
+__global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__) {
+    constexpr int W = G * C;
+    constexpr int GPW = 32 / G;
+    __shared__ uint32_t rows8[4];
+    if (threadIdx.x < 4) rows8[threadIdx.x] = t.rows8[threadIdx.x];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int member = lane % G;
+    const int group = lane / G;
+    const int warp = int((int64_t(blockIdx.x) * kBlock + threadIdx.x) >> 5);
+    const int warps = int((int64_t(gridDim.x) * kBlock) >> 5);
+    const int32_t open = p.open, extend = p.extend;
+    const int32_t opening = open - extend;
+    const int32_t first_gap = open + extend;
+    const int64_t slot = int64_t(warp) * GPW + group;
+    const uint32_t open2 = halves(open, open), extend2 = halves(extend, extend), opening2 = halves(opening, opening);
+    const uint32_t floor2 = halves(-32768, -32768);
+    const int32_t top = LOCAL ? 0 : opening;
+    const uint32_t top2 = halves(top, top), top_gap2 = halves(top + first_gap, top + first_gap);
+
+    for (uint32_t base = p.begin + uint32_t(warp) * 2 * GPW; base < p.end; base += uint32_t(warps) * 2 * GPW) {
+        const uint32_t item = base + 2 * group;
+        bool live[2];
+        uint32_t pair[2] = {0, 0};
+        PairShape sh[2] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        int rows[2], cols[2], strips[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            live[h] = item + h < p.end;
+            if (live[h]) {
+                pair[h] = p.order[item + h];
+                sh[h] = p.shapes[pair[h]];
+            }
+            rows[h] = int(sh[h].rows);
+            cols[h] = int(sh[h].columns);
+            strips[h] = live[h] && rows[h] > 0 && cols[h] > 0 ? (cols[h] + W - 1) / W : 0;
+        }
+        const int warp_strips = warp_max(max(strips[0], strips[1]));
+        uint32_t best2 = 0;
+        int32_t reported[2] = {0, 0};
+
+        for (int s = 0; s < warp_strips; ++s) {
+            bool strip_live[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) strip_live[h] = s < strips[h];
+            const int first_col = s * W + member * C;
+            uint32_t sel[C];
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                const int col = first_col + k;
+                const uint32_t a = strip_live[0] && col < cols[0]
+                                       ? half_selector_a(letter_at<2>(p.tape, sh[0].second_word, uint32_t(col)))
+                                       : kPadHalf;
+                const uint32_t b = strip_live[1] && col < cols[1]
+                                       ? half_selector_b(letter_at<2>(p.tape, sh[1].second_word, uint32_t(col)))
+                                       : kPadHalf;
+                sel[k] = pair_selector(a, b);
+            }
+            uint32_t H[C], D[C];
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                H[k] = top2;
+                D[k] = top_gap2;
+            }
+            uint32_t edgeH = top2, edgeI = top_gap2;
+            const int32_t corner = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
+            uint32_t above_left = halves(corner, corner);
+            int group_rows = 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) group_rows = max(group_rows, strip_live[h] ? rows[h] : 0);
+            const int steps = group_rows > 0 ? group_rows + G : 0;
+            const int warp_steps = warp_max(steps);
+
+            for (int step = 1; step <= warp_steps; ++step) {
+                const int row = step - member;
+                uint32_t leftH = __shfl_up_sync(kFull, edgeH, 1, G);
+                uint32_t leftI = __shfl_up_sync(kFull, edgeI, 1, G);
+                if (member == 0) {
+                    if (s == 0) {
+                        leftH = top2;
+                        leftI = top_gap2;
+                    } else {
+                        const int r = min(max(row, 0), group_rows);
+                        const int2 c = p.carry[slot * p.carry_stride + r];
+                        leftH = uint32_t(c.x);
+                        leftI = uint32_t(c.y);
+                    }
+                }
+                uint32_t diag = above_left;
+                above_left = leftH;
+                if (row >= 1 && row <= group_rows) {
+                    uint32_t tr[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        tr[h] = strip_live[h] && row <= rows[h]
+                                    ? rows8[letter_at<2>(p.tape, sh[h].first_word, uint32_t(row - 1))]
+                                    : 0u;
+                    uint32_t I = 0, Xprev = 0;
+#pragma unroll
+                    for (int k = 0; k < C; ++k) {
+                        const uint32_t sub = uint32_t(prmt(tr[0], tr[1], sel[k]));
+                        const uint32_t Hup = H[k], Dup = D[k];
+                        uint32_t Dn, X, Hn;
+                        if (LOCAL) {
+                            Dn = __viaddmax_s16x2(Hup, open2, __viaddmax_s16x2(Dup, extend2, floor2));
+                        } else {
+                            Dn = __viaddmax_s16x2(Hup, opening2, Dup);
+                        }
+                        X = __viaddmax_s16x2(diag, sub, Dn);
+                        if (k == 0) {
+                            I = LOCAL ? __viaddmax_s16x2(leftH, open2, __viaddmax_s16x2(leftI, extend2, floor2))
+                                      : __viaddmax_s16x2(leftH, opening2, leftI);
+                        } else {
+                            I = LOCAL ? __viaddmax_s16x2(I, extend2, Xprev) : __viaddmax_s16x2(Xprev, opening2, I);
+                        }
+                        if (LOCAL) {
+                            Hn = __vimax_s16x2_relu(X, I);
+                            best2 = __vimax_s16x2_relu(best2, Hn);
+                            // The next cell's insertion reads max(X, 0) + open.
+                            Xprev = __viaddmax_s16x2(X, open2, open2);
+                        } else {
+                            Hn = __vimax3_s16x2(X, I, X);
+                            Xprev = X;
+                        }
+                        diag = Hup;
+                        H[k] = Hn;
+                        D[k] = Dn;
+                    }
+                    edgeH = H[C - 1];
+                    edgeI = I;
+                    if (member == G - 1 && s + 1 < warp_strips)
+                        p.carry[slot * p.carry_stride + row] = make_int2(int32_t(H[C - 1]), int32_t(I));
+                    if (!LOCAL) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int owned = min(max(cols[h] - first_col, 0), C);
+                            if (strip_live[h] && row == rows[h] && owned > 0 && first_col + owned == cols[h]) {
+                                // The corner by masks, not by an index into H (which would put H in memory).
+                                uint32_t corner = 0;
+#pragma unroll
+                                for (int k = 0; k < C; ++k) {
+                                    const uint32_t hit = 0u - uint32_t(k == owned - 1);
+                                    corner |= H[k] & hit;
+                                }
+                                reported[h] = h == 0 ? low_of(corner) : high_of(corner);
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+
+        // Results: a local score is the group's best, a global one the corner (one lane holds it) shifted back.
+        if (LOCAL) {
+#pragma unroll
+            for (int span = 1; span < G; span <<= 1) best2 = __vimax_s16x2_relu(best2, __shfl_xor_sync(kFull, best2, span, G));
+            if (member == 0) {
+                if (live[0]) p.scores[pair[0]] = low_of(best2);
+                if (live[1]) p.scores[pair[1]] = high_of(best2);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int32_t value = reported[h];
+#pragma unroll
+                for (int span = 1; span < G; span <<= 1) value += __shfl_xor_sync(kFull, value, span, G);
+                if (live[h] && member == 0) p.scores[pair[h]] = value + (rows[h] + cols[h]) * extend;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Scores of one long pair a block: the sweep above with the whole block of 256 lanes as one group, a
+// strip 4,096 columns wide, so a pair of tens of thousands of letters runs on an SM's eight warps
+// instead of one. Lane m runs one row behind lane m-1 as before; across a warp boundary the left
+// neighbour's edge comes through shared memory, written by the previous warp's last lane in the step
+// before and read after the block's barrier that ends it (two buffers by step parity). Every step ends
+// with that barrier, so no warp waits on another in any other way.
+// ------------------------------------------------------------------------------------------------
+
+template <bool LOCAL>
+__global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__) {
+    constexpr int C = 16;
+    constexpr int W = kBlock * C;
+    constexpr int kWarps = kBlock / 32;
+    __shared__ uint2 rows16[4];
+    __shared__ int2 handoff[2][kWarps];
+    __shared__ int32_t block_best[kWarps];
+    if (threadIdx.x < 4) rows16[threadIdx.x] = t.rows16[threadIdx.x];
+    __syncthreads();
+
+    const int member = threadIdx.x;
+    const int lane = member & 31;
+    const int warp = member >> 5;
+    const int32_t open = p.open, extend = p.extend;
+    const int32_t opening = open - extend;
+    const int32_t first_gap = open + extend;
+    const int64_t slot = blockIdx.x;
+
+    for (uint32_t item = p.begin + blockIdx.x; item < p.end; item += gridDim.x) {
+        const uint32_t pair = p.order[item];
+        const PairShape sh = p.shapes[pair];
+        const int rows = int(sh.rows), cols = int(sh.columns);
+        const int strips = (cols + W - 1) / W;
+        int32_t best = 0;
+
+        for (int s = 0; s < strips; ++s) {
+            const int first_col = s * W + member * C;
+            const int owned = min(max(cols - first_col, 0), C);
+            uint32_t sel[C];
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                const int col = first_col + k;
+                sel[k] = col < cols ? selector_of(letter_at<2>(p.tape, sh.second_word, uint32_t(col))) : kPadSelector;
+            }
+            const int32_t top = LOCAL ? 0 : opening;
+            int32_t H[C], D[C];
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                H[k] = top;
+                D[k] = top + first_gap;
+            }
+            int32_t edgeH = top, edgeI = top + first_gap;
+            int32_t above_left = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
+            const int steps = rows + kBlock;
+
+            for (int step = 1; step <= steps; ++step) {
+                const int row = step - member;
+                int32_t leftH = __shfl_up_sync(kFull, edgeH, 1);
+                int32_t leftI = __shfl_up_sync(kFull, edgeI, 1);
+                if (lane == 0) {
+                    if (member == 0) {
+                        if (s == 0) {
+                            leftH = LOCAL ? 0 : opening;
+                            leftI = leftH + first_gap;
+                        } else {
+                            const int r = min(max(row, 0), rows);
+                            const int2 c = p.carry[slot * p.carry_stride + r];
+                            leftH = c.x;
+                            leftI = c.y;
+                        }
+                    } else {
+                        const int2 c = handoff[(step - 1) & 1][warp - 1];
+                        leftH = c.x;
+                        leftI = c.y;
+                    }
+                }
+                int32_t diag = above_left;
+                above_left = leftH;
+                if (row >= 1 && row <= rows) {
+                    const uint32_t rl = letter_at<2>(p.tape, sh.first_word, uint32_t(row - 1));
+                    const uint2 tr = rows16[rl];
+                    int32_t I = 0, Xprev = 0;
+#pragma unroll
+                    for (int k = 0; k < C; ++k) {
+                        const int32_t sub = prmt(tr.x, tr.y, sel[k]);
+                        const int32_t Hup = H[k], Dup = D[k];
+                        int32_t Dn, X, Hn;
+                        if (LOCAL) {
+                            Dn = __viaddmax_s32(Hup, open, Dup + extend);
+                        } else {
+                            Dn = __viaddmax_s32(Hup, opening, Dup);
+                        }
+                        X = __viaddmax_s32(diag, sub, Dn);
+                        if (k == 0) {
+                            I = LOCAL ? max(leftH + open, leftI + extend) : __viaddmax_s32(leftH, opening, leftI);
+                        } else {
+                            I = LOCAL ? __viaddmax_s32(I, extend, Xprev) : __viaddmax_s32(Xprev, opening, I);
+                        }
+                        Hn = LOCAL ? __vimax_s32_relu(X, I) : max(X, I);
+                        if (LOCAL) best = max(best, Hn);
+                        Xprev = LOCAL ? __viaddmax_s32(X, open, open) : X;
+                        diag = Hup;
+                        H[k] = Hn;
+                        D[k] = Dn;
+                    }
+                    edgeH = H[C - 1];
+                    edgeI = I;
+                    if (member == kBlock - 1 && s + 1 < strips) p.carry[slot * p.carry_stride + row] = make_int2(edgeH, I);
+                    if (!LOCAL && row == rows && owned > 0 && first_col + owned == cols) {
+                        // The corner by masks, not by an index into H (which would put H in memory).
+                        int32_t corner = 0;
+#pragma unroll
+                        for (int k = 0; k < C; ++k) {
+                            const int32_t hit = -int32_t(k == owned - 1);
+                            corner = (corner & ~hit) | (H[k] & hit);
+                        }
+                        p.scores[pair] = corner + (rows + cols) * extend;
+                    }
+                }
+                if (lane == 31) handoff[step & 1][warp] = make_int2(edgeH, edgeI);
+                __syncthreads();
+            }
+        }
+        if (LOCAL) {
+            const int32_t mine = warp_max(best);
+            if (lane == 0) block_best[warp] = mine;
+            __syncthreads();
+            if (member == 0) {
+                int32_t all = 0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) all = max(all, block_best[w]);
+                p.scores[pair] = all;
+            }
+            __syncthreads();
         }
     }
 }

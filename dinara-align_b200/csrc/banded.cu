@@ -235,6 +235,10 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
     constexpr int G = kBandLanes, C = kBandColumns;
     constexpr int GPW = 32 / G;      // lane groups a warp
     constexpr int PPW = 2 * GPW;     // pairs a warp
+    // Rows a selector window serves: fewer when recording, whose longer body would outgrow the
+    // instruction cache unrolled over sixteen rows.
+    constexpr int U = RECORD ? 8 : 16;
+    constexpr int WIN = C + U;
     __shared__ uint32_t rows8[4];
     if (threadIdx.x < 4) rows8[threadIdx.x] = b.rows8[threadIdx.x];
     __syncthreads();
@@ -294,12 +298,12 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
         int32_t reported[2] = {0, 0};
         uint2 buffered[2][2];  // [pair][row of two]: the rows' 64-bit words, low and high 32 bits
 
-        for (int r0 = 1; r0 <= warp_rows; r0 += 16) {
-            // Selectors of 32 consecutive columns from r0 + low + first_place, both pairs in one: bytes 0-1
+        for (int r0 = 1; r0 <= warp_rows; r0 += U) {
+            // Selectors of WIN consecutive columns from r0 + low + first_place, both pairs in one: bytes 0-1
             // pick pair A's entry (sign-extended to 16 bits) from its row, bytes 2-3 pair B's.
-            uint32_t window[32];
+            uint32_t window[WIN];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
+            for (int j = 0; j < WIN; ++j) {
                 uint32_t y[2];
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                 window[j] = (17u * y[0] + 128u) | ((17u * y[1] + 196u) << 8);
             }
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int row = r0 + u;
                 if (row <= warp_rows) {
                     const uint32_t nextH = __shfl_down_sync(kFull, H[0], 1, G);

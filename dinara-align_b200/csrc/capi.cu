@@ -23,6 +23,8 @@ thread_local std::string new_error;
 
 template <class F>
 int64_t guard(dinara_gpu *gpu, F &&body) {
+    // Allocations during the call are ordered on the context's stream.
+    AllocationScope scope(gpu ? gpu->stream : nullptr);
     try {
         return body();
     } catch (const Failure &failure) {
@@ -342,6 +344,12 @@ dinara_gpu *dinara_gpu_new(int64_t device) {
         gpu->multiprocessors = properties.multiProcessorCount;
         std::snprintf(gpu->name, sizeof gpu->name, "%s", properties.name);
         DINARA_CUDA(cudaStreamCreateWithFlags(&gpu->stream, cudaStreamNonBlocking));
+        // The device's pool keeps what contexts free for their next growth instead of handing it back at
+        // every synchronisation (this process's pool only; nothing outlives it).
+        cudaMemPool_t pool = nullptr;
+        DINARA_CUDA(cudaDeviceGetDefaultMemPool(&pool, int(device)));
+        uint64_t keep = UINT64_MAX;
+        DINARA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         DINARA_CUDA(cudaEventCreate(&gpu->start));
         DINARA_CUDA(cudaEventCreate(&gpu->stop));
         DINARA_CUDA(cudaEventCreateWithFlags(&gpu->fork, cudaEventDisableTiming));
@@ -360,18 +368,11 @@ dinara_gpu *dinara_gpu_new(int64_t device) {
 void dinara_gpu_free(dinara_gpu *gpu) {
     if (!gpu) return;
     cudaSetDevice(gpu->device);
+    AllocationScope scope(gpu->stream);
     if (gpu->stream) cudaStreamSynchronize(gpu->stream);
     if (gpu->resident) gpu->resident_free(gpu->resident);
-    dinara::DeviceBuffer *buffers[] = {&gpu->letters,        &gpu->offsets,       &gpu->code_table,   &gpu->tape,
-                                       &gpu->shapes,         &gpu->flags,         &gpu->keys,         &gpu->keys_sorted,
-                                       &gpu->order,          &gpu->order_sorted,  &gpu->sort_scratch, &gpu->ranges,
-                                       &gpu->scores,         &gpu->carry,         &gpu->decisions,    &gpu->decision_offsets,
-                                       &gpu->walk_out,       &gpu->cigar_slots,   &gpu->cigar_lengths, &gpu->cigar_offsets,
-                                       &gpu->cigar_bytes,    &gpu->spans,         &gpu->planes,       &gpu->plane_offsets,
-                                       &gpu->thresholds,     &gpu->distances,     &gpu->pending,      &gpu->pending_next,
-                                       &gpu->counters,       &gpu->table32,       &gpu->features,      &gpu->weights,      &gpu->gradients,
-                                       &gpu->optimizer,      &gpu->predictions,   &gpu->targets,      &gpu->activations};
-    for (auto *buffer : buffers) buffer->release();
+    gpu->for_each_buffer([](dinara::DeviceBuffer &buffer) { buffer.release(); });
+    if (gpu->stream) cudaStreamSynchronize(gpu->stream);
     gpu->pinned_in.release();
     gpu->pinned_out.release();
     gpu->pinned_small.release();

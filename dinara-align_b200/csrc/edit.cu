@@ -242,7 +242,8 @@ __global__ void prepare_kernel(const uint8_t *__restrict__ letters, const int64_
         results[warp] = -1000;  // not yet known
 }
 
-// A warp a DNA pair: its pattern's four match planes, a word per 64 letters.
+// A warp a DNA pair: its pattern's four match planes, a word per 64 letters. The warp reads a word's 64
+// letters two to a lane (coalesced) and takes each plane's 64 bits as two ballots.
 __global__ void planes_kernel(const uint8_t *__restrict__ letters, const EditPair *__restrict__ pairs, int64_t count,
                               const int64_t *__restrict__ plane_offsets, uint64_t *__restrict__ planes) {
     const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -252,12 +253,17 @@ __global__ void planes_kernel(const uint8_t *__restrict__ letters, const EditPai
     if (!e.dna || e.n == 0) return;
     uint64_t *out = planes + plane_offsets[warp];
     const uint8_t *pattern = letters + e.pattern;
-    for (int w = lane; w < e.words; w += 32) {
-        uint64_t bits[4] = {0, 0, 0, 0};
-        const int first = w * 64;
-        const int count_in = min(64, e.n - first);
-        for (int j = 0; j < count_in; ++j) bits[dna_code(pattern[first + j])] |= 1ull << j;
-        for (int x = 0; x < 4; ++x) out[4 * int64_t(w) + x] = bits[x];
+    for (int w = 0; w < e.words; ++w) {
+        const int first = 64 * w + lane, second = first + 32;
+        // Letters past the pattern match no plane.
+        const uint32_t low_code = first < e.n ? dna_code(__ldg(pattern + first)) : 4u;
+        const uint32_t high_code = second < e.n ? dna_code(__ldg(pattern + second)) : 4u;
+#pragma unroll
+        for (uint32_t x = 0; x < 4; ++x) {
+            const uint32_t low = __ballot_sync(kFull, low_code == x);
+            const uint32_t high = __ballot_sync(kFull, high_code == x);
+            if (lane == int(x)) out[4 * int64_t(w) + x] = (uint64_t(high) << 32) | low;
+        }
     }
 }
 
@@ -282,12 +288,12 @@ __global__ void start_kernel(const EditPair *__restrict__ pairs, int64_t count, 
 // Keys for the pending pairs: band shape in the top bits, then the text length, longest first.
 __global__ void band_keys_kernel(const EditPair *__restrict__ pairs, const uint32_t *__restrict__ pending,
                                  const unsigned int *__restrict__ pending_count, const int64_t *__restrict__ thresholds,
-                                 uint32_t *__restrict__ keys, unsigned int *__restrict__ shape_counts) {
+                                 bool latency, uint32_t *__restrict__ keys, unsigned int *__restrict__ shape_counts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= *pending_count) return;
     const uint32_t pair = pending[k];
     const EditPair e = pairs[pair];
-    const int shape = band_shape_for(e.n, e.m, thresholds[pair]);
+    const int shape = band_shape_for(e.n, e.m, thresholds[pair], latency);
     uint32_t length = uint32_t(e.m) >> 2;
     if (length > 0xFFFFFFu) length = 0xFFFFFFu;
     keys[k] = (uint32_t(shape) << 24) | length;
@@ -301,8 +307,8 @@ __global__ void band_keys_kernel(const EditPair *__restrict__ pairs, const uint3
 __global__ void settle_kernel(const EditPair *__restrict__ pairs, const uint32_t *__restrict__ pending,
                               const unsigned int *__restrict__ pending_count, int64_t *__restrict__ thresholds,
                               int64_t *__restrict__ cheapest, const int64_t *__restrict__ banded,
-                              int64_t *__restrict__ results, int64_t *__restrict__ rounds, uint32_t *__restrict__ next,
-                              unsigned int *__restrict__ next_count) {
+                              int64_t *__restrict__ results, int64_t *__restrict__ rounds, bool latency,
+                              uint32_t *__restrict__ next, unsigned int *__restrict__ next_count) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= *pending_count) return;
     const uint32_t pair = pending[k];
@@ -310,7 +316,7 @@ __global__ void settle_kernel(const EditPair *__restrict__ pairs, const uint32_t
     const int64_t t = thresholds[pair];
     const int64_t found = banded[pair];
     rounds[pair] += 1;
-    const int shape = band_shape_for(e.n, e.m, t);
+    const int shape = band_shape_for(e.n, e.m, t, latency);
     const int64_t window = int64_t(band_lanes(shape)) * band_words_per_lane(shape);
     const bool whole = window >= e.words;  // the window holds every word: the whole matrix
     // The proof needs the window to cover the band; the widest window (512 words) falls short only for
@@ -353,7 +359,12 @@ BandFn pick_band(int shape) {
         case 14: return &band_kernel<32, 6>;
         case 15: return &band_kernel<32, 8>;
         case 16: return &band_kernel<32, 12>;
-        default: return &band_kernel<32, 16>;
+        case 17: return &band_kernel<32, 16>;
+        case 18: return &band_kernel<2, 1>;
+        case 19: return &band_kernel<4, 1>;
+        case 20: return &band_kernel<8, 1>;
+        case 21: return &band_kernel<16, 1>;
+        default: return &band_kernel<32, 1>;
     }
 }
 
@@ -438,7 +449,11 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         // Order the round's pairs: by band shape, longest text first.
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, (1 + kBandShapes) * sizeof(unsigned int), stream));
         const unsigned blocks = unsigned((count + threads - 1) / threads);
-        band_keys_kernel<<<blocks, threads, 0, stream>>>(info, pending, counters, thresholds, keys, counters + 2);
+        // A round of few pairs takes the one-word-a-lane windows: lanes to spare, and the sweep's time is
+        // its longest pair's chain of steps.
+        const bool latency = count <= int64_t(gpu->multiprocessors) * 32;
+        band_keys_kernel<<<blocks, threads, 0, stream>>>(info, pending, counters, thresholds, latency, keys,
+                                                         counters + 2);
         gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         size_t sort_bytes = 0;
@@ -498,7 +513,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         DINARA_CUDA(cudaEventRecord(gpu->stop, stream));
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned int), stream));
         settle_kernel<<<blocks, threads, 0, stream>>>(info, order_sorted, counters, thresholds, cheapest, banded,
-                                                      results, rounds, next, counters + 1);
+                                                      results, rounds, latency, next, counters + 1);
         gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         DINARA_CUDA(cudaMemcpyAsync(counters, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToDevice, stream));

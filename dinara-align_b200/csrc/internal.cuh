@@ -30,6 +30,19 @@ inline void check_cuda(cudaError_t status, const char *what, const char *file, i
 
 #define DINARA_CUDA(call) ::dinara::check_cuda((call), #call, __FILE__, __LINE__)
 
+// The stream the calling thread's context orders its allocations on (set for the length of each entry
+// point). Device buffers grow and shrink by stream-ordered allocation from the device's pool: a plain
+// cudaMalloc or cudaFree would wait for every kernel on the device, so one context growing a buffer would
+// stall the work every other context (a serving slot, say) has in flight.
+inline thread_local cudaStream_t allocation_stream = nullptr;
+
+// Sets the allocation stream for a scope and puts the previous one back after it.
+struct AllocationScope {
+    cudaStream_t previous;
+    explicit AllocationScope(cudaStream_t stream) : previous(allocation_stream) { allocation_stream = stream; }
+    ~AllocationScope() { allocation_stream = previous; }
+};
+
 // A device allocation that grows on demand and is reused by later calls.
 struct DeviceBuffer {
     void *ptr = nullptr;
@@ -39,12 +52,12 @@ struct DeviceBuffer {
         size_t wanted = count * sizeof(T);
         if (wanted == 0) wanted = 256;
         if (wanted > bytes) {
-            if (ptr) cudaFree(ptr);
+            if (ptr) cudaFreeAsync(ptr, allocation_stream);
             ptr = nullptr;
             bytes = 0;
             size_t grown = wanted + wanted / 4;
             grown = (grown + 255) & ~size_t(255);
-            DINARA_CUDA(cudaMalloc(&ptr, grown));
+            DINARA_CUDA(cudaMallocAsync(&ptr, grown, allocation_stream));
             bytes = grown;
         }
         return static_cast<T *>(ptr);
@@ -54,7 +67,7 @@ struct DeviceBuffer {
         return static_cast<T *>(ptr);
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) cudaFreeAsync(ptr, allocation_stream);
         ptr = nullptr;
         bytes = 0;
     }
@@ -116,7 +129,7 @@ struct dinara_gpu {
     cudaStream_t stream = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
     // Side streams that let a round's launches of different shapes run at once, joined by events.
-    static constexpr int kSideStreams = 18;  // one for each band window shape
+    static constexpr int kSideStreams = 23;  // one for each band window shape
     cudaStream_t side[kSideStreams] = {nullptr};
     cudaEvent_t fork = nullptr, joins[kSideStreams] = {nullptr};
     std::string error;
@@ -131,7 +144,7 @@ struct dinara_gpu {
     // Unit-cost band state.
     dinara::DeviceBuffer planes, plane_offsets, thresholds, distances, pending, pending_next, counters, table32;
     // Learned band predictor.
-    dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations;
+    dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations, sketches;
     bool predictor_ready = false;
     double predictor_margin = 1.25;    // the largest of the classes' margins (reported)
     double predictor_margins[4] = {1.25, 1.25, 1.25, 1.25};  // by mean length: < 300, < 1000, < 4096, more
@@ -145,4 +158,17 @@ struct dinara_gpu {
     // The resident batch (capi.cu), if one is loaded.
     void *resident = nullptr;
     void (*resident_free)(void *) = nullptr;
+
+    // Every device buffer the context holds.
+    template <class F>
+    void for_each_buffer(F &&visit) {
+        dinara::DeviceBuffer *all[] = {
+            &letters,   &offsets,      &code_table, &tape,          &shapes,        &flags,         &keys,
+            &keys_sorted, &order,      &order_sorted, &sort_scratch, &ranges,       &class_counts,  &layouts,
+            &leftovers, &decisions_extra, &scores,  &carry,         &decisions,     &decision_offsets, &walk_out,
+            &cigar_slots, &cigar_lengths, &cigar_offsets, &cigar_bytes, &spans,      &planes,        &plane_offsets,
+            &thresholds, &distances,   &pending,    &pending_next,  &counters,      &table32,       &features,
+            &weights,   &gradients,    &optimizer,  &predictions,   &targets,       &activations,   &sketches};
+        for (dinara::DeviceBuffer *buffer : all) visit(*buffer);
+    }
 };

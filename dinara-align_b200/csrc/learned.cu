@@ -174,8 +174,10 @@ __device__ void features_of(const int *counts, int64_t reference, int64_t query,
     }
 }
 
-// A warp a pair: the features into a feature-major matrix (feature f of pair p at f * pairs + p).
-__global__ void features_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs, float *features) {
+// A warp a pair: the features into a matrix, feature f of pair p at f * pairs + p (feature-major, as
+// training reads them) or at p * kIn + f (pair-major, as prediction does).
+__global__ void features_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs, float *features,
+                                bool pair_major) {
     __shared__ int counts[8][256];
     const int warp_in_block = threadIdx.x >> 5;
     const int64_t pair = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp_in_block;
@@ -189,8 +191,9 @@ __global__ void features_kernel(const uint8_t *letters, const int64_t *offsets, 
         count_kmers(letters + q0, q1 - q0, -1, mine);
     }
     __syncwarp();
-    if (pair < pairs) features_of(mine, offsets[2 * pair + 1] - offsets[2 * pair],
-                                  offsets[2 * pair + 2] - offsets[2 * pair + 1], features + pair, int(pairs));
+    if (pair < pairs)
+        features_of(mine, offsets[2 * pair + 1] - offsets[2 * pair], offsets[2 * pair + 2] - offsets[2 * pair + 1],
+                    pair_major ? features + pair * kIn : features + pair, pair_major ? 1 : int(pairs));
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -350,7 +353,7 @@ struct Margins {
 
 __device__ __host__ inline int length_class(double mean) { return mean < 300 ? 0 : mean < 1000 ? 1 : mean < 4096 ? 2 : 3; }
 
-__global__ void __launch_bounds__(256) predict_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs,
+__global__ void __launch_bounds__(256) predict_kernel(const float *features, const int64_t *offsets, int64_t pairs,
                                                       const float *params, Margins margins, float slack,
                                                       int64_t *thresholds, float *predicted) {
     extern __shared__ float shared[];
@@ -361,20 +364,13 @@ __global__ void __launch_bounds__(256) predict_kernel(const uint8_t *letters, co
     float *w3 = b2 + kH;
     float *b3 = w3 + kH;
     float *inputs = shared + kParamsRoom;  // 8 warps x 260 (kIn and padding)
-    int *counts = reinterpret_cast<int *>(inputs + 8 * 260);  // 8 warps x 256
     for (int i = threadIdx.x; i < kPredictorParameters; i += blockDim.x) shared[i] = params[i];
     const int warp_in_block = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int *mine = counts + warp_in_block * 256;
     float *x = inputs + warp_in_block * 260;
     __syncthreads();
     for (int64_t pair = int64_t(blockIdx.x) * 8 + warp_in_block; pair < pairs; pair += int64_t(gridDim.x) * 8) {
-        for (int k = lane; k < 256; k += 32) mine[k] = 0;
-        __syncwarp();
         const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
-        count_kmers(letters + r0, q0 - r0, 1, mine);
-        count_kmers(letters + q0, q1 - q0, -1, mine);
-        __syncwarp();
-        features_of(mine, q0 - r0, q1 - q0, x, 1);
+        for (int i = lane; i < kIn; i += 32) x[i] = __ldg(features + pair * kIn + i);
         __syncwarp();
         // Hidden layers: lane j computes units j and j + 32.
         float h[2];
@@ -413,7 +409,7 @@ __global__ void __launch_bounds__(256) predict_kernel(const uint8_t *letters, co
     }
 }
 
-size_t predict_shared_bytes() { return size_t(kParamsRoom + 8 * 260) * sizeof(float) + 8 * 256 * sizeof(int); }
+size_t predict_shared_bytes() { return size_t(kParamsRoom + 8 * 260) * sizeof(float); }
 
 // Parameter offsets in the flat vector: w1 [kIn][kH], b1, w2 [kH][kH], b2, w3, b3.
 constexpr int kW1 = 0, kB1 = kW1 + kIn * kH, kW2 = kB1 + kH, kB2 = kW2 + kH * kH, kW3 = kB2 + kH, kB3 = kW3 + kH;
@@ -456,7 +452,7 @@ size_t work_floats(int batch) { return size_t(batch) * (4 * kH + 2) + 64; }
 void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
                         float *features) {
     const int threads = 256;
-    features_kernel<<<unsigned((pairs + 7) / 8), threads, 0, gpu->stream>>>(letters, offsets, pairs, features);
+    features_kernel<<<unsigned((pairs + 7) / 8), threads, 0, gpu->stream>>>(letters, offsets, pairs, features, false);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 }
@@ -485,8 +481,14 @@ const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t 
     blocks = std::min<int64_t>(blocks, (pairs + 7) / 8);
     Margins margins;
     for (int k = 0; k < 4; ++k) margins.by_length[k] = float(gpu->predictor_margins[k]);
+    // The sketches first, a warp a pair at full occupancy (reading the letters is the slow part), then the
+    // network from them with its weights in shared memory.
+    float *sketches = gpu->sketches.ensure<float>(size_t(pairs) * kIn);
+    features_kernel<<<unsigned((pairs + 7) / 8), 256, 0, gpu->stream>>>(letters, offsets, pairs, sketches, true);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
     predict_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), 256, shared, gpu->stream>>>(
-        letters, offsets, pairs, gpu->weights.as<float>(), margins, float(gpu->predictor_slack), thresholds, predicted);
+        sketches, offsets, pairs, gpu->weights.as<float>(), margins, float(gpu->predictor_slack), thresholds, predicted);
     DINARA_CUDA(cudaGetLastError());
     gpu->launches += 1;
     return thresholds;

@@ -62,34 +62,55 @@ __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int
     }
 }
 
-// Scheduling keys: the pair's class in the top bits (the whole-matrix shape class, or the proven band,
-// the highest), then strips of its width, then rows, so a descending sort puts each class's longest pairs
-// first and warps hold pairs of like size. Counts each class.
-__global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ list,
-                                     int64_t first, int64_t count, int record, int band, int32_t pair_limit,
-                                     uint32_t *__restrict__ keys,
-                                     uint32_t *__restrict__ order, unsigned int *__restrict__ class_counts) {
-    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= count) return;
+// One pair's scheduling key and class (the kernel below).
+__device__ void classify_pair(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ list, int64_t first,
+                              int64_t k, int record, int band, PairLimits limits, uint32_t *__restrict__ keys,
+                              uint32_t *__restrict__ order, unsigned int *block_counts) {
     const uint32_t pair = list ? list[k] : uint32_t(first + k);
     const PairShape shape = shapes[pair];
     const bool empty = shape.rows == 0 || shape.columns == 0;
     int cls;
     uint32_t strips = 0;
     if (band && band_eligible(shape.rows, shape.columns)) {
-        cls = int64_t(shape.rows) + shape.columns <= pair_limit ? kBandPairsClass : kBandClass;
+        cls = int64_t(shape.rows) + shape.columns <= limits.band ? kBandPairsClass : kBandClass;
     } else {
         cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);
-        const uint32_t width = uint32_t(affine_lanes(cls) * affine_columns(cls));
+        if (!record && limits.wide && shape.rows >= kWideRows && shape.columns >= kWideColumns) cls = kWideClass;
+        const uint32_t width = cls == kWideClass ? 4096u : uint32_t(affine_lanes(cls) * affine_columns(cls));
         strips = empty ? 0 : (shape.columns + width - 1) / width;
+        const int64_t swept = int64_t(strips) * width;
+        const bool pairs16 = cls != kWideClass && !record && !empty && limits.whole > 0 &&
+                             (limits.local ? swept <= limits.whole
+                                           : 2 * swept <= limits.whole && 2 * int64_t(shape.rows) <= limits.whole);
+        if (pairs16) cls += kWholePairsClass;
         if (strips > 255) strips = 255;
     }
     uint32_t rows = shape.rows >> 2;
     if (rows > 0xFFFFFu) rows = 0xFFFFFu;
     keys[k] = (uint32_t(cls) << 28) | (strips << 20) | rows;
     order[k] = pair;
-    atomicAdd(&class_counts[cls], 1u);
+    atomicAdd(&block_counts[cls], 1u);
 }
+
+// Scheduling keys: the pair's class in the top bits (the whole-matrix shape class, or the proven band,
+// the highest), then strips of its width, then rows, so a descending sort puts each class's longest pairs
+// first and warps hold pairs of like size. Counts each class.
+__global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ list,
+                                     int64_t first, int64_t count, int record, int band, PairLimits limits,
+                                     uint32_t *__restrict__ keys,
+                                     uint32_t *__restrict__ order, unsigned int *__restrict__ class_counts) {
+    // Each block counts its classes in shared memory first: a million pairs' counts on a dozen global
+    // counters would otherwise queue on the same addresses.
+    __shared__ unsigned int block_counts[kClasses];
+    if (threadIdx.x < kClasses) block_counts[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < count) classify_pair(shapes, list, first, k, record, band, limits, keys, order, block_counts);
+    __syncthreads();
+    if (threadIdx.x < kClasses && block_counts[threadIdx.x] > 0)
+        atomicAdd(&class_counts[threadIdx.x], block_counts[threadIdx.x]);
+}
+
 
 void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
                 const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown) {
@@ -103,7 +124,7 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
 }
 
 Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
-                   bool record, bool band, int32_t pair_limit) {
+                   bool record, bool band, PairLimits limits) {
     Schedule out;
     for (int c = 0; c < kClasses; ++c) out.counts[c] = 0;
     out.order = nullptr;
@@ -116,7 +137,7 @@ Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list
     DINARA_CUDA(cudaMemsetAsync(class_counts, 0, kClasses * sizeof(unsigned int), gpu->stream));
     const int threads = 256;
     schedule_keys_kernel<<<unsigned((count + threads - 1) / threads), threads, 0, gpu->stream>>>(
-        shapes, list, first, count, record ? 1 : 0, band ? 1 : 0, pair_limit, keys, order, class_counts);
+        shapes, list, first, count, record ? 1 : 0, band ? 1 : 0, limits, keys, order, class_counts);
     DINARA_CUDA(cudaGetLastError());
     gpu->launches += 1;
     size_t scratch = 0;

@@ -11,20 +11,37 @@ namespace dinara {
 void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
                 const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown);
 
-// A batch's sweep order: pairs by class (the whole-matrix shape classes 0-4, affine_shape_for with
-// `record`; with `band` the proven band, kBandClass, and of those the pairs whose rows and columns sum to
-// at most `pair_limit`, kBandPairsClass, for the 16-bit pair sweep), classes in descending order, then
-// strips and rows descending. `order` is valid on the device until the next call.
-constexpr int kClasses = 7;
+// A batch's sweep order: pairs by class, classes in descending order, then strips and rows descending.
+// Classes: the whole-matrix shape classes 0-4 (affine_shape_for with `record`); with `band` the proven
+// band, kBandClass, and of those the pairs whose rows and columns sum to at most `limits.band`,
+// kBandPairsClass, for the 16-bit pair band sweep; the whole-matrix pairs the 16-bit pair score sweep
+// takes, kWholePairsClass plus the shape class; and long pairs one block sweeps, kWideClass. `order` is
+// valid on the device until the next call.
+constexpr int kClasses = 13;
 constexpr int kBandClass = 5;
 constexpr int kBandPairsClass = 6;
+constexpr int kWholePairsClass = 7;
+constexpr int kWideClass = 12;
+// A pair a whole block sweeps (kWideClass), scoring without a CIGAR: at least this tall and this wide.
+constexpr uint32_t kWideRows = 4096, kWideColumns = 2048;
 struct Schedule {
     const uint32_t *order;
     int64_t counts[kClasses];
 };
 
+// Which pairs the 16-bit pair sweeps take: band pairs whose rows and columns sum to at most `band`; and,
+// scoring without a CIGAR, non-empty whole-matrix pairs whose swept columns are at most `whole` (local)
+// or whose rows and swept columns are each at most half of it (global). Zero takes none. With `wide`,
+// scoring without a CIGAR, whole-matrix pairs of at least kWideRows x kWideColumns go to kWideClass.
+struct PairLimits {
+    int32_t band = 0;
+    int32_t whole = 0;
+    int32_t local = 0;
+    int32_t wide = 0;
+};
+
 // The order of pairs [first, first + count), or of the `count` pairs listed in `list` (device) when given.
 Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list, int64_t first, int64_t count,
-                  bool record, bool band, int32_t pair_limit = 0);
+                  bool record, bool band, PairLimits limits = PairLimits());
 
 }  // namespace dinara

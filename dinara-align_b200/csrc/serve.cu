@@ -46,28 +46,17 @@ struct Request {
 };
 
 // Device bytes a context holds in its buffers.
-int64_t resident_bytes(const dinara_gpu *g) {
-    const dinara::DeviceBuffer *buffers[] = {
-        &g->letters,   &g->offsets,       &g->code_table,   &g->tape,         &g->shapes,        &g->flags,
-        &g->keys,      &g->keys_sorted,   &g->order,        &g->order_sorted, &g->sort_scratch,  &g->ranges,
-        &g->class_counts, &g->layouts,    &g->leftovers,    &g->decisions_extra, &g->scores,     &g->carry,
-        &g->decisions, &g->decision_offsets, &g->walk_out,  &g->cigar_slots,  &g->cigar_lengths, &g->cigar_offsets,
-        &g->cigar_bytes, &g->spans,       &g->table32,      &g->counters};
+int64_t resident_bytes(dinara_gpu *g) {
     int64_t total = 0;
-    for (const auto *b : buffers) total += int64_t(b->bytes);
+    g->for_each_buffer([&](const dinara::DeviceBuffer &b) { total += int64_t(b.bytes); });
     return total;
 }
 
+// Gives a context's device buffers back to the device's pool, ordered after its own work.
 void release_buffers(dinara_gpu *g) {
-    dinara::DeviceBuffer *buffers[] = {
-        &g->letters,   &g->offsets,       &g->code_table,   &g->tape,         &g->shapes,        &g->flags,
-        &g->keys,      &g->keys_sorted,   &g->order,        &g->order_sorted, &g->sort_scratch,  &g->ranges,
-        &g->class_counts, &g->layouts,    &g->leftovers,    &g->decisions_extra, &g->scores,     &g->carry,
-        &g->decisions, &g->decision_offsets, &g->walk_out,  &g->cigar_slots,  &g->cigar_lengths, &g->cigar_offsets,
-        &g->cigar_bytes, &g->spans,       &g->table32,      &g->counters};
     cudaSetDevice(g->device);
-    cudaStreamSynchronize(g->stream);
-    for (auto *b : buffers) b->release();
+    dinara::AllocationScope scope(g->stream);
+    g->for_each_buffer([](dinara::DeviceBuffer &b) { b.release(); });
 }
 
 // What a request's scores may hold on the device: its letters and their packed copy, per-pair shapes,

@@ -108,6 +108,50 @@ def test_shapes_and_strips(da, oracle, local):
     assert [a.score for a in found] == list(expected_scores)
 
 
+@pytest.mark.parametrize("local", [False, True])
+def test_sixteen_bit_limits(da, oracle, local):
+    """Whole-matrix scores where only some pairs fit the 16-bit pair sweep: large entries bring its limit
+    down to a few hundred columns (locally) or rows and columns (globally), so pairs each side of it, and
+    pairs of different shapes sharing a lane group, are scored in one batch."""
+    rng = np.random.default_rng(77)
+    scoring = da.Scoring.uniform(120, -120, -10, -5) if local else da.Scoring.uniform(60, -60, -20, -3)
+    mode = da.Mode.local() if local else da.Mode.GLOBAL
+    refs, queries = [], []
+    for _ in range(400):
+        rows, columns = int(rng.integers(1, 700)), int(rng.integers(1, 700))
+        a = rng.choice(list("ACGT"), size=max(rows, columns))
+        b = a[:columns].copy()
+        flips = rng.random(columns) < 0.05
+        b[flips] = rng.choice(list("ACGT"), size=int(flips.sum()))
+        refs.append("".join(a[:rows]))
+        queries.append("".join(b))
+    tape = da.Tape.of(refs, queries)
+    expected = _oracle_batch(oracle, da, tape, scoring, local, False)
+    np.testing.assert_array_equal(da.scores_tape(tape, scoring, mode), expected)
+
+
+@pytest.mark.parametrize("local", [False, True])
+def test_long_pairs_on_a_whole_block(da, oracle, local):
+    """Pairs of at least 4,096 x 2,048 letters, scored on a whole block (strips of 4,096 columns): single
+    and multiple strips, columns at and just past a strip's edge, next to shorter pairs."""
+    rng = np.random.default_rng(91)
+    scoring = da.Scoring.uniform(0, -4, -6, -2) if not local else da.Scoring.dna()
+    mode = da.Mode.local() if local else da.Mode.GLOBAL
+    shapes = [(4096, 2048), (4095, 3000), (5000, 4096), (5000, 4097), (9000, 8500), (4100, 12000), (6000, 2047),
+              (300, 250), (4500, 4480)]
+    refs, queries = [], []
+    for rows, columns in shapes:
+        a = rng.choice(list("ACGT"), size=max(rows, columns))
+        b = a[:columns].copy()
+        flips = rng.random(columns) < 0.08
+        b[flips] = rng.choice(list("ACGT"), size=int(flips.sum()))
+        refs.append("".join(a[:rows]))
+        queries.append("".join(b))
+    tape = da.Tape.of(refs, queries)
+    expected = _oracle_batch(oracle, da, tape, scoring, local, False)
+    np.testing.assert_array_equal(da.scores_tape(tape, scoring, mode), expected)
+
+
 def test_local_spans_placed_as_reference(da, oracle):
     """Local spans by as_alignment's rule (scoring.mojo:724-744): the aligned letters' last place."""
     refs = ["GGGGACGTACGTGGGG", "ACGTTTTTACGT" * 3, "TTTTACGTACGTTTTT"]
