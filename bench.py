@@ -128,7 +128,10 @@ def reference_arm(args) -> None:
 
     threads = os.cpu_count() or 1
     line = cpu_measure(oracle, args.workload, threads, args.steps, args.warmup)
-    line.update({"impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup})
+    line.update({"impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                 "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                            "timed_on": "the host's cores, a bounded sample of the workload (cpu_baseline.sample)"},
+                 "data": "synthetic", "scaling": "weak", "vs_baseline": None})
     line["e2e"] = {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line))
 
@@ -212,11 +215,12 @@ def learned_band_section(da, native, lib, handle, steps: int) -> dict:
 def serving_section(da) -> dict:
     """Open-loop serving: Poisson arrivals at 2,000 requests/s, each 1-4,096 pairs (log-uniform), lengths
     log-uniform 100 bp-50 kbp, 1-10% errors, global gap-affine (4,6,2) scores, a 40 GB device budget; a bounded
-    run of 40 requests, far past what the device sustains, so latency is mostly queueing."""
+    run of 100 requests, offered far past what the device sustains, so latency is mostly queueing and
+    requests queued together share device calls."""
     from dinara_align import serving, workloads
 
     rng = np.random.default_rng(55)
-    requests = [workloads.serving_request(rng) for _ in range(40)]
+    requests = [workloads.serving_request(rng) for _ in range(100)]
     scoring = da.Scoring.uniform(0, -4, -6, -2)
     with serving.Server(slots=4, device_bytes=40 << 30) as server:
         out = serving.open_loop(server, requests, 2000.0, scoring)
@@ -385,7 +389,9 @@ def main() -> None:
         line = {
             "metric": "pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32" if not unit else "u64", "data": "synthetic",
+            "vs_baseline": None, "data": "synthetic",
+            # Scores: 16-bit halves where a pair's values provably fit (exact), 32 bits otherwise.
+            "dtype": "u64" if unit else "int16x2+int32",
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload], "pairs_per_gpu": pairs,
                        "full_matrix_cells_per_gpu": cells, "l2": "inputs larger than L2 (packed tape and decisions)",
                        "parallelism": f"pairs sharded, {world} independent ranks"},
@@ -399,10 +405,29 @@ def main() -> None:
             peak = 2 * peaks["viaddmax"]
             achieved = swept * ops_per_cell / (kernel_ms / 1e3)
             line["roofline"] = {"bound": "int32", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gops/s",
-                                "frac": achieved / peak, "traffic": None, "ops_per_cell": ops_per_cell,
+                                "frac": achieved / peak, "ops_per_cell": ops_per_cell,
                                 "swept_cells_per_step": swept, "kernel_ms_per_step": kernel_ms,
                                 "kernel": "the recording sweep (band, then whole matrices for the rest) and the walk",
                                 "peak_source": "measured in this run: DPX viaddmax chains on every SM, 2 ops each"}
+        if unit and band_report and "viaddmax" in peaks and band_report.get("kernel_ms"):
+            # A Myers/Hyyro word step is about 20 u64 operations (bit_parallel.mojo:10-11), 40 in int32 terms,
+            # over the words the band kernels swept, against the same int32 peak as the scorers.
+            peak = 2 * peaks["viaddmax"]
+            achieved = band_report["words_swept"] * 40 / (band_report["kernel_ms"] / 1e3)
+            line["roofline"] = {"bound": "int32", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gops/s",
+                                "frac": achieved / peak, "traffic": None, "ops_per_word_step": 40,
+                                "words_swept_per_step": band_report["words_swept"],
+                                "kernel_ms_per_step": band_report["kernel_ms"],
+                                "kernel": "the band kernels of every round (band_kernel, all window shapes)",
+                                "peak_source": "measured in this run: DPX viaddmax chains on every SM, 2 ops each"}
+        if "roofline" in line and args.workload == "affine":
+            # DRAM bytes of the recording band sweep (dram__bytes_read.sum + dram__bytes_write.sum), from an
+            # ncu capture of 200,000 pairs of this distribution (8,993 bytes a pair: the recorded decisions
+            # and the sectors filled around their stores), scaled to this batch.
+            line["roofline"]["traffic"] = 8993.0 * pairs
+            line["roofline"]["traffic_unit"] = "bytes per launch of the recording band sweep"
+        elif "roofline" in line:
+            line["roofline"]["traffic"] = None
         if scorer and "viaddmax" in peaks:
             achieved = scorer["swept_cells"] * ops_per_cell / (scorer["kernel_ms"] / 1e3)
             scorer.update({"pairs_per_s": world * pairs / (scorer["ms_per_step"] / 1e3),

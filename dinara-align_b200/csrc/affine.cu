@@ -101,14 +101,15 @@ __global__ void walk_kernel(WalkArgs a) {
         const uint64_t *decisions = layout == 2 ? a.decisions_extra : a.decisions;
         const int G = record_lanes(uint32_t(cols), a.uniform);
         const int W = G * 16;
-        const int rows_pad = layout == 1 ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
-        const int low = layout == 1 ? band_low_for(rows, cols) : 0;
+        const bool banded = layout == 1 || layout == 3;
+        const int rows_pad = banded ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
+        const int low = banded ? band_low_for(rows, cols) : 0;
         const int64_t base = a.decision_offsets[k];
         int state = 0;  // 0 aligning, 1 deleting, 2 inserting
         while (row > 0 && column > 0) {
             int64_t at;
             int slot_in;
-            if (layout == 1) {
+            if (banded) {
                 // The band's layout: place o = column - row - low, a lane of 16 places a block of rows.
                 const int place = column - row - low;
                 // The proof keeps every optimal path inside the band; a place outside it would read
@@ -125,7 +126,16 @@ __global__ void walk_kernel(WalkArgs a) {
                 at = base + int64_t(s * G + member) * rows_pad + (row - 1 + (member & 3));
             }
             const uint64_t word = decisions[at];
-            const uint32_t nibble = uint32_t(word >> (4 * slot_in)) & 15u;
+            uint32_t nibble;
+            if (layout == 3) {
+                // The 16-bit pair band's planes: bit `slot_in` of deleting, inserting, deletion extending and
+                // insertion extending, 16 bits each; inserting wins over deleting as decide() orders them.
+                const uint32_t del = uint32_t(word >> slot_in) & 1u, ins = uint32_t(word >> (16 + slot_in)) & 1u;
+                const uint32_t dext = uint32_t(word >> (32 + slot_in)) & 1u, iext = uint32_t(word >> (48 + slot_in)) & 1u;
+                nibble = (ins ? 2u : del) | (dext << 2) | (iext << 3);
+            } else {
+                nibble = uint32_t(word >> (4 * slot_in)) & 15u;
+            }
             if (a.local && state == 0 && (nibble & 3u) == 3u) break;
             const int moving = state == 0 ? int(nibble & 3u) : state;
             if (moving == 1) {
@@ -178,6 +188,7 @@ __global__ void gather_cigars_kernel(const char *__restrict__ slots, const int64
 }
 
 __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count, bool uniform,
+                                  int32_t band_pair_limit,
                                   bool band, int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes,
                                   uint8_t *__restrict__ layouts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -186,7 +197,8 @@ __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t 
     int64_t words = 0;
     uint8_t layout = 0;
     if (band && band_eligible(sh.rows, sh.columns)) {
-        layout = 1;
+        // The 16-bit pair band (its pairs' rows and columns within the limit) records planes (layout 3).
+        layout = int64_t(sh.rows) + sh.columns <= band_pair_limit ? 3 : 1;
         words = int64_t(kBandLanes) * ((int64_t(sh.rows) + 3) & ~int64_t(3));
     } else if (sh.rows > 0 && sh.columns > 0) {
         const int G = record_lanes(sh.columns, uniform);
@@ -602,7 +614,9 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     uint8_t *layouts = gpu->layouts.ensure<uint8_t>(size_t(count) + 1);
     const int threads = 256;
     const unsigned blocks = unsigned((count + threads - 1) / threads);
-    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, band, words,
+    const int32_t band_pair_limit = band ? pair_limit_of(table) : 0;
+    slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, band_pair_limit,
+                                                           band, words,
                                                            slot_bytes, layouts);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());

@@ -221,13 +221,14 @@ __device__ __forceinline__ int32_t high_half(uint32_t v) { return int32_t(int16_
 // The halves' maximum: the DPX maximum floored at zero, which every value here already is at or above.
 __device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) { return __vimax_s16x2_relu(a, b); }
 
-// Sets bit `at` (and bit 16 + at) of `acc` where a half of `v` has bit 15 clear. `v` = b - a + 0x8000 per
-// half (halves in [0, 0x8000), so nothing crosses between them) has bit 15 set exactly where b >= a: a
-// clear bit records a > b.
-template <int AT>
-__device__ __forceinline__ uint32_t place_clear(uint32_t acc, uint32_t v) {
-    constexpr uint32_t mask = (1u << AT) | (1u << (16 + AT));
-    return acc | (~(v >> (15 - AT)) & mask);
+// Adds to a plane `acc` (pair A's 16 places in the low half, pair B's in the high) place k's flags: set
+// where a half of `v` has bit 15 clear. `v` = b - a + 0x8000 in each half (halves in [0, 0x8000), so
+// nothing crosses between them) has bit 15 set exactly where b >= a, so a clear bit records a > b. The
+// flags move from bits 15 and 31 down to k and 16 + k by the high word of a product, added in the same
+// instruction (the FMA pipe's, leaving the ALU to the cells).
+__device__ __forceinline__ uint32_t gather_flag(uint32_t acc, uint32_t v, int k) {
+    const uint32_t flags = ~v & 0x80008000u;
+    return k == 15 ? acc + flags : __umulhi(flags, 1u << (17 + k)) + acc;
 }
 
 template <bool RECORD>
@@ -329,7 +330,8 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                     const uint32_t trA = rows8[x_letter[0]], trB = rows8[x_letter[1]];
                     uint32_t X[C];
                     uint32_t S = unreached2;  // running max of X + opening along this lane's places
-                    uint32_t acc[4] = {0, 0, 0, 0};
+                    // Decision planes, each a bit a place for both pairs (see gather_flag).
+                    uint32_t deleting = 0, inserting = 0, deletion_runs = 0, insertion_runs = 0;
                     // Pass 1: the deletion layer, the best of the diagonal and deletion moves, and (scores)
                     // each place's best insertion from this lane's earlier places.
 #pragma unroll
@@ -343,14 +345,8 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                             X[k] = max2(xd, dn);
                             // gotoh.mojo:173-186 decide: the source leaves the diagonal only where the
                             // deletion beats it; a deletion run extends only where extending beats opening.
-                            const uint32_t del = xd - dn + at_least;         // bit 15 clear: dn > xd
-                            const uint32_t ext = Hup - Dup + at_least_open;  // clear: Dup > Hup + opening
-                            switch (k & 3) {
-                                case 0: acc[k >> 2] = place_clear<2>(place_clear<0>(acc[k >> 2], del), ext); break;
-                                case 1: acc[k >> 2] = place_clear<6>(place_clear<4>(acc[k >> 2], del), ext); break;
-                                case 2: acc[k >> 2] = place_clear<10>(place_clear<8>(acc[k >> 2], del), ext); break;
-                                default: acc[k >> 2] = place_clear<14>(place_clear<12>(acc[k >> 2], del), ext); break;
-                            }
+                            deleting = gather_flag(deleting, xd - dn + at_least, k);               // dn > xd
+                            deletion_runs = gather_flag(deletion_runs, Hup - Dup + at_least_open, k);  // Dup > Hup + opening
                             S = __viaddmax_s16x2(X[k], opening2, S);
                         } else {
                             const uint32_t x = __viaddmax_s16x2(H[k], sub, dn);
@@ -381,25 +377,9 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                             const uint32_t I = S2;
                             S2 = __viaddmax_s16x2(X[k], opening2, S2);
                             H[k] = max2(X[k], I);
-                            const uint32_t ins = X[k] - I + at_least;  // bit 15 clear: I > X
-                            // The inserting bit at 4k + 1, and the deleting bit below it cleared where set.
-                            uint32_t y = 0;
-                            switch (k & 3) {
-                                case 0: y = place_clear<1>(0u, ins); break;
-                                case 1: y = place_clear<5>(0u, ins); break;
-                                case 2: y = place_clear<9>(0u, ins); break;
-                                default: y = place_clear<13>(0u, ins); break;
-                            }
-                            acc[k >> 2] = (acc[k >> 2] & ~(y >> 1)) | y;
-                            if (k > 0) {
-                                const uint32_t grow = prevH - prevI + at_least_open;  // clear: I > H + opening
-                                switch (k & 3) {
-                                    case 0: acc[k >> 2] = place_clear<3>(acc[k >> 2], grow); break;
-                                    case 1: acc[k >> 2] = place_clear<7>(acc[k >> 2], grow); break;
-                                    case 2: acc[k >> 2] = place_clear<11>(acc[k >> 2], grow); break;
-                                    default: acc[k >> 2] = place_clear<15>(acc[k >> 2], grow); break;
-                                }
-                            }
+                            inserting = gather_flag(inserting, X[k] - I + at_least, k);  // I > X
+                            // The left cell's insertion beats its score plus an opening: the run extends.
+                            if (k > 0) insertion_runs = gather_flag(insertion_runs, prevH - prevI + at_least_open, k);
                             prevH = H[k];
                             prevI = I;
                         }
@@ -410,13 +390,14 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                             leftH = unreached2;
                             leftI = unreached2;
                         }
-                        acc[0] = place_clear<3>(acc[0], leftH - leftI + at_least_open);
-                        // Each pair's 64-bit word of the row: places 0-7 from acc[0..1], 8-15 from acc[2..3].
+                        insertion_runs = gather_flag(insertion_runs, leftH - leftI + at_least_open, 0);
+                        // Each pair's 64-bit word of the row: its deleting, inserting, deletion-run and
+                        // insertion-run planes, 16 bits each (the walk's layout 3).
                         const int slot = u & 1;
-                        buffered[0][slot] = make_uint2(uint32_t(prmt(acc[0], acc[1], 0x5410u)),
-                                                       uint32_t(prmt(acc[2], acc[3], 0x5410u)));
-                        buffered[1][slot] = make_uint2(uint32_t(prmt(acc[0], acc[1], 0x7632u)),
-                                                       uint32_t(prmt(acc[2], acc[3], 0x7632u)));
+                        buffered[0][slot] = make_uint2(uint32_t(prmt(deleting, inserting, 0x5410u)),
+                                                       uint32_t(prmt(deletion_runs, insertion_runs, 0x5410u)));
+                        buffered[1][slot] = make_uint2(uint32_t(prmt(deleting, inserting, 0x7632u)),
+                                                       uint32_t(prmt(deletion_runs, insertion_runs, 0x7632u)));
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             if (live[h] && row <= rows[h] && (slot == 1 || row == rows[h])) {

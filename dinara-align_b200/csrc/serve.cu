@@ -1,5 +1,7 @@
 // A serving loop over the batched scorer: requests (each a batch of pairs under a Scoring) arrive at any
-// time, wait in a queue, and are admitted first in first out as a worker slot and device memory free up.
+// time, wait in a queue, and are admitted first in first out as a worker slot and device memory free up;
+// a slot that frees up takes the head of the queue with every request queued behind it that shares its
+// Scoring and mode, as one device call (continuous batching).
 // Each slot is a context of its own on the device (its stream and the device buffers it keeps between
 // requests), so admitted requests run at once and their kernels overlap on the GPU; a request's result
 // is the same whether it runs alone or beside others, as no slot shares a buffer with another.
@@ -74,6 +76,15 @@ int64_t estimate_bytes(const Request &r, int multiprocessors) {
     return bytes;
 }
 
+// Whether two requests can share one device call: the same Scoring and the same mode.
+bool compatible(const Request &a, const Request &b) {
+    return a.alphabet == b.alphabet && a.table == b.table && a.opening == b.opening && a.extension == b.extension &&
+           std::memcmp(&a.mode, &b.mode, sizeof a.mode) == 0;
+}
+
+// Pairs one merged device call may hold.
+constexpr int64_t kMergePairs = int64_t(1) << 20;
+
 }  // namespace
 
 struct dinara_server {
@@ -92,7 +103,7 @@ struct dinara_server {
     int64_t next_ticket = 1;
     bool stopping = false;
     Clock::time_point origin = Clock::now();
-    int64_t admitted = 0, completed = 0, refused = 0, pairs_done = 0;
+    int64_t admitted = 0, completed = 0, refused = 0, pairs_done = 0, calls = 0;
 
     // Bytes every slot holds, the slot `k` counted at least `grown` (its request's estimate).
     int64_t projected(size_t k, int64_t grown) {
@@ -104,6 +115,41 @@ struct dinara_server {
     void release(size_t j) {
         release_buffers(slots[j]);
         held[j] = 0;
+    }
+
+    // Scores a batch of compatible requests in one device call on a slot, each request's results into it.
+    static int64_t run_batch(dinara_gpu *slot, const std::vector<Request *> &batch, int64_t pairs) {
+        Request &first = *batch.front();
+        dinara_scoring scoring{first.alphabet.data(), int64_t(first.alphabet.size()), first.table.data(),
+                               first.opening, first.extension};
+        for (Request *q : batch) {
+            q->scores.assign(size_t(std::max<int64_t>(q->pairs, 1)), 0);
+            q->statuses.assign(size_t(std::max<int64_t>(q->pairs, 1)), 0);
+        }
+        if (batch.size() == 1)
+            return dinara_gpu_scores_tape(slot, first.pairs, first.letters.data(), first.offsets.data(), &scoring,
+                                          &first.mode, first.scores.data(), first.statuses.data());
+        std::vector<char> letters;
+        std::vector<int64_t> offsets{0};
+        offsets.reserve(size_t(2 * pairs + 1));
+        for (const Request *q : batch) {
+            const int64_t base = offsets.back();
+            const int64_t length = q->offsets.empty() ? 0 : q->offsets.back();
+            letters.insert(letters.end(), q->letters.begin(), q->letters.begin() + length);
+            for (int64_t j = 1; j <= 2 * q->pairs; ++j) offsets.push_back(base + q->offsets[size_t(j)]);
+        }
+        letters.push_back(0);
+        std::vector<int32_t> scores(size_t(std::max<int64_t>(pairs, 1)));
+        std::vector<int64_t> statuses(size_t(std::max<int64_t>(pairs, 1)));
+        const int64_t code = dinara_gpu_scores_tape(slot, pairs, letters.data(), offsets.data(), &scoring, &first.mode,
+                                                    scores.data(), statuses.data());
+        int64_t at = 0;
+        for (Request *q : batch) {
+            std::copy(scores.begin() + at, scores.begin() + at + q->pairs, q->scores.begin());
+            std::copy(statuses.begin() + at, statuses.begin() + at + q->pairs, q->statuses.begin());
+            at += q->pairs;
+        }
+        return code;
     }
 
     void worker(size_t k) {
@@ -140,26 +186,38 @@ struct dinara_server {
                 }
             }
             queue.pop_front();
+            // Continuous batching: the requests queued behind this one that share its Scoring and mode
+            // join it in one device call, as far as the pair cap and the memory budget allow.
+            std::vector<Request *> batch{r};
+            int64_t batch_pairs = r->pairs, batch_estimate = r->estimate;
+            while (!queue.empty() && compatible(*queue.front(), *r) &&
+                   batch_pairs + queue.front()->pairs <= kMergePairs &&
+                   projected(k, batch_estimate + queue.front()->estimate) <= budget) {
+                batch.push_back(queue.front());
+                batch_pairs += queue.front()->pairs;
+                batch_estimate += queue.front()->estimate;
+                queue.pop_front();
+            }
             busy[k] = true;
-            held[k] = std::max(held[k], r->estimate);
-            r->admitted = seconds_since(origin);
-            ++admitted;
+            held[k] = std::max(held[k], batch_estimate);
+            const double now = seconds_since(origin);
+            for (Request *q : batch) q->admitted = now;
+            admitted += int64_t(batch.size());
+            ++calls;
             hold.unlock();
-            dinara_scoring scoring{r->alphabet.data(), int64_t(r->alphabet.size()), r->table.data(), r->opening,
-                                   r->extension};
-            r->scores.assign(size_t(std::max<int64_t>(r->pairs, 1)), 0);
-            r->statuses.assign(size_t(std::max<int64_t>(r->pairs, 1)), 0);
-            const int64_t code = dinara_gpu_scores_tape(slots[k], r->pairs, r->letters.data(), r->offsets.data(),
-                                                        &scoring, &r->mode, r->scores.data(), r->statuses.data());
+            const int64_t code = run_batch(slots[k], batch, batch_pairs);
             const int64_t now_held = resident_bytes(slots[k]);
             hold.lock();
             held[k] = now_held;
-            r->code = code;
-            r->done = true;
-            r->finished = seconds_since(origin);
+            const double end = seconds_since(origin);
+            for (Request *q : batch) {
+                q->code = code;
+                q->done = true;
+                q->finished = end;
+                pairs_done += q->pairs;
+            }
             busy[k] = false;
-            ++completed;
-            pairs_done += r->pairs;
+            completed += int64_t(batch.size());
             finished.notify_all();
             work.notify_all();
         }
@@ -280,6 +338,7 @@ int64_t dinara_server_stats(dinara_server *server, dinara_server_stats_t *stats)
     stats->running = running;
     stats->budget_bytes = server->budget;
     stats->clock = seconds_since(server->origin);
+    stats->calls = server->calls;
     return 0;
 }
 

@@ -19,6 +19,7 @@ ValueError, as the reference's GPU placement does (api.mojo:1240-1246, scoring.m
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass, replace
 from typing import Optional, Sequence, Union
 
@@ -368,13 +369,21 @@ def alignments_tape(tape: Tape, scoring: Scoring, mode: Mode = Mode.GLOBAL, *, e
                                                     native.pointer(offsets, ctypes.c_int64), ctypes.byref(buffer),
                                                     native.pointer(codes, ctypes.c_int64))
     native.check(code, handle)
-    try:
-        total = int(offsets[pairs]) if pairs else 0
-        data = ctypes.string_at(buffer.value, total) if total else b""
-    finally:
-        if buffer.value:
-            native.lib().dinara_free(buffer.value)
-    return out[:pairs], spans[:pairs], offsets, data, codes[:pairs]
+    total = int(offsets[pairs]) if pairs else 0
+    return out[:pairs], spans[:pairs], offsets, _owned_bytes(buffer.value, total), codes[:pairs]
+
+
+def _owned_bytes(address: Optional[int], size: int) -> np.ndarray:
+    """The library's CIGAR buffer as a uint8 array without a copy, freed (dinara_free) once the array and
+    every view of it are gone."""
+    if not address:
+        return np.zeros(0, dtype=np.uint8)
+    if size == 0:
+        native.lib().dinara_free(address)
+        return np.zeros(0, dtype=np.uint8)
+    array = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(address))
+    weakref.finalize(array, native.lib().dinara_free, address)
+    return array
 
 
 def alignments(references: Sequence[Text], queries: Sequence[Text], costs: Union[Costs, Scoring] = Costs(),
@@ -394,7 +403,7 @@ def alignments(references: Sequence[Text], queries: Sequence[Text], costs: Union
     _raise_first(codes, "Scoring's alphabet")
     out = []
     for pair in range(tape.pairs):
-        cigar = data[offsets[pair]:offsets[pair + 1]].decode("ascii")
+        cigar = data[offsets[pair]:offsets[pair + 1]].tobytes().decode("ascii")
         value = int(found[pair])
         span = spans[pair]
         out.append(Alignment(-value, value, cigar, int(span[0]), int(span[1]), int(span[2]), int(span[3])))

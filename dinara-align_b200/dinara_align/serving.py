@@ -24,7 +24,7 @@ class RequestTiming(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_int64) for name in ("queued", "running", "admitted", "completed", "refused",
                                                     "pairs_done", "resident_bytes", "budget_bytes")] + [
-        ("clock", ctypes.c_double)]
+        ("clock", ctypes.c_double), ("calls", ctypes.c_int64)]
 
 
 def _declare(lib):

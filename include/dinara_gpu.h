@@ -281,7 +281,8 @@ typedef struct {
 typedef struct {
     int64_t queued, running, admitted, completed, refused, pairs_done;
     int64_t resident_bytes, budget_bytes;
-    double clock; /* seconds since the server started */
+    double clock;  /* seconds since the server started */
+    int64_t calls; /* device calls made: admitted requests merged into fewer when they share a Scoring */
 } dinara_server_stats_t;
 
 dinara_server *dinara_server_new(dinara_gpu *gpu, const dinara_server_options *options);

@@ -83,7 +83,7 @@ def test_synthetic_scores_and_cigars(da, oracle, local):
     scores, spans, offsets, data, codes = da.alignments_tape(tape, scoring, mode)
     np.testing.assert_array_equal(scores, expected_scores)
     assert not codes.any()
-    cigars = [data[offsets[p]:offsets[p + 1]].decode() for p in range(tape.pairs)]
+    cigars = [data[offsets[p]:offsets[p + 1]].tobytes().decode() for p in range(tape.pairs)]
     assert cigars == expected_cigars
 
 
