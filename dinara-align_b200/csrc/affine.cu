@@ -335,9 +335,13 @@ TableArgs table_args(const AffineTable &table, bool local) {
             }
             t.rows16[r].x = uint32_t(e[0]) | (uint32_t(e[1]) << 16);
             t.rows16[r].y = uint32_t(e[2]) | (uint32_t(e[3]) << 16);
-            // The byte table of the 16-bit pair sweeps (entries past a byte never reach them).
-            t.rows8[r] = uint32_t(uint8_t(e[0])) | (uint32_t(uint8_t(e[1])) << 8) | (uint32_t(uint8_t(e[2])) << 16) |
-                         (uint32_t(uint8_t(e[3])) << 24);
+            // The byte table of the 16-bit pair sweeps, local entries less extend as that sweep holds local
+            // cells (entries past a byte never reach them: the schedule keeps such tables off it).
+            t.rows8[r] = 0;
+            for (int c = 0; c < 4; ++c) {
+                const int32_t v = int32_t(int16_t(e[c])) - (local && r < table.size && c < table.size ? table.extend : 0);
+                t.rows8[r] |= uint32_t(uint8_t(int8_t(v))) << (8 * c);
+            }
         }
     }
     return t;
@@ -451,8 +455,9 @@ int32_t pair_limit_of(const AffineTable &table) {
 }
 
 // Which whole-matrix pairs the 16-bit pair score sweep takes (a table of up to four letters on the 2-bit
-// tape): locally, scores reach at most the best entry times the columns swept and fall no lower than a
-// gap's first letter, so the swept columns are held to (30,000 less the gaps) over the best entry;
+// tape): locally, a cell held less row x extend reaches at most the best entry times the columns swept
+// plus the rows times -extend and falls no lower than a gap's first letter, so that sum is held to half of
+// 30,000 less the gaps;
 // globally, a shifted cell moves at most the largest step a cell, so rows and swept columns are each held
 // to half of 30,000 over it, every value within 30,000 of zero. Entries must fit a byte (shifted, globally).
 PairLimits whole_limits_of(const AffineBatch &batch, const AffineTable &table) {
@@ -464,9 +469,17 @@ PairLimits whole_limits_of(const AffineBatch &batch, const AffineTable &table) {
     if (batch.local) {
         int32_t best = 1;
         for (int r = 0; r < table.size; ++r)
-            for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
+            for (int c = 0; c < table.size; ++c) {
+                best = std::max(best, table.entries[r * 32 + c]);
+                const int32_t shifted = table.entries[r * 32 + c] - table.extend;
+                if (shifted < -128 || shifted > 127) return limits;
+            }
         limits.local = 1;
-        limits.whole = (30000 - gaps) / best;
+        // Half of it a pair: a lane group sweeps its two pairs to the larger one's rows and strips, so the
+        // cells past a pair's end reach at most the sum of the two pairs' terms.
+        limits.whole = (30000 - gaps) / 2;
+        limits.best = best;
+        limits.row_step = -table.extend;
         return limits;
     }
     int32_t step = std::abs(table.open - table.extend);

@@ -297,9 +297,9 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
 // Scores of two pairs a lane group, pair A in every register's low 16 bits and pair B in its high 16 bits:
 // the sweep above, cell for cell, each DPX instruction on 16-bit pairs (full rate on this part, as the
 // 32-bit ones) moving a cell of each pair. The schedule gives it only pairs whose every value, and every
-// value of the cells it sweeps past their ends, stays inside 16 bits: a local score is at most the best
-// entry times the columns swept and never below a gap's opening; a global cell held shifted moves at
-// most the largest shifted entry or opening a step. Cells past a pair's last row read a row of zero
+// value of the cells it sweeps past their ends, stays inside 16 bits: a local cell, held less row x
+// extend, is at most the best entry times the columns swept plus the rows times -extend and never below
+// a gap's opening; a global cell held shifted moves at most the largest shifted entry or opening a step. Cells past a pair's last row read a row of zero
 // entries and cells past its last column a padding of 0 or -1, so neither beats the pair's real cells
 // (a local best) nor feeds them (a global corner).
 // ------------------------------------------------------------------------------------------------
@@ -338,6 +338,9 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
     const uint32_t floor2 = halves(-32768, -32768);
     const int32_t top = LOCAL ? 0 : opening;
     const uint32_t top2 = halves(top, top), top_gap2 = halves(top + first_gap, top + first_gap);
+    // Local cells are held less row x extend (the table less extend too): a deletion run then climbs by
+    // a constant, the zero floor becomes row-dependent, and the best is shifted back a row at a time.
+    const uint32_t open_less_extend2 = halves(open - extend, open - extend);
 
     for (uint32_t base = p.begin + uint32_t(warp) * 2 * GPW; base < p.end; base += uint32_t(warps) * 2 * GPW) {
         const uint32_t item = base + 2 * group;
@@ -394,12 +397,15 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
 
             for (int step = 1; step <= warp_steps; ++step) {
                 const int row = step - member;
+                // Local: this row's lift (row x -extend, at least 0), the floor of its held cells.
+                const int32_t lift = LOCAL ? -max(row, 0) * extend : 0;
+                const uint32_t floor_h2 = halves(lift, lift), floor_i2 = halves(open + lift, open + lift);
                 uint32_t leftH = __shfl_up_sync(kFull, edgeH, 1, G);
                 uint32_t leftI = __shfl_up_sync(kFull, edgeI, 1, G);
                 if (member == 0) {
                     if (s == 0) {
-                        leftH = top2;
-                        leftI = top_gap2;
+                        leftH = LOCAL ? floor_h2 : top2;
+                        leftI = LOCAL ? halves(lift + first_gap, lift + first_gap) : top_gap2;
                     } else {
                         const int r = min(max(row, 0), group_rows);
                         const int2 c = p.carry[slot * p.carry_stride + r];
@@ -422,11 +428,7 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
                         const uint32_t sub = uint32_t(prmt(tr[0], tr[1], sel[k]));
                         const uint32_t Hup = H[k], Dup = D[k];
                         uint32_t Dn, X, Hn;
-                        if (LOCAL) {
-                            Dn = __viaddmax_s16x2(Hup, open2, __viaddmax_s16x2(Dup, extend2, floor2));
-                        } else {
-                            Dn = __viaddmax_s16x2(Hup, opening2, Dup);
-                        }
+                        Dn = __viaddmax_s16x2(Hup, LOCAL ? open_less_extend2 : opening2, Dup);
                         X = __viaddmax_s16x2(diag, sub, Dn);
                         if (k == 0) {
                             I = LOCAL ? __viaddmax_s16x2(leftH, open2, __viaddmax_s16x2(leftI, extend2, floor2))
@@ -435,10 +437,9 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
                             I = LOCAL ? __viaddmax_s16x2(I, extend2, Xprev) : __viaddmax_s16x2(Xprev, opening2, I);
                         }
                         if (LOCAL) {
-                            Hn = __vimax_s16x2_relu(X, I);
-                            best2 = __vimax_s16x2_relu(best2, Hn);
-                            // The next cell's insertion reads max(X, 0) + open.
-                            Xprev = __viaddmax_s16x2(X, open2, open2);
+                            Hn = __vimax3_s16x2(X, I, floor_h2);
+                            // The next cell's insertion reads the floored X plus an opening.
+                            Xprev = __viaddmax_s16x2(X, open2, floor_i2);
                         } else {
                             Hn = __vimax3_s16x2(X, I, X);
                             Xprev = X;
@@ -449,6 +450,14 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
                     }
                     edgeH = H[C - 1];
                     edgeI = I;
+                    if (LOCAL) {
+                        // The row's best, shifted back by its lift, into the running best.
+                        uint32_t row_best = H[0];
+#pragma unroll
+                        for (int k = 1; k + 1 < C; k += 2) row_best = __vimax3_s16x2(row_best, H[k], H[k + 1]);
+                        if (C % 2 == 0) row_best = __vimax3_s16x2(row_best, H[C - 1], H[C - 1]);
+                        best2 = __viaddmax_s16x2(row_best, halves(-lift, -lift), best2);
+                    }
                     if (member == G - 1 && s + 1 < warp_strips)
                         p.carry[slot * p.carry_stride + row] = make_int2(int32_t(H[C - 1]), int32_t(I));
                     if (!LOCAL) {

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
     constexpr int PPW = 2 * GPW;     // pairs a warp
     // Rows a selector window serves: fewer when recording, whose longer body would outgrow the
     // instruction cache unrolled over sixteen rows.
-    constexpr int U = RECORD ? 8 : 16;
+    constexpr int U = RECORD ? 4 : 16;
     constexpr int WIN = C + U;
     __shared__ uint32_t rows8[4];
     if (threadIdx.x < 4) rows8[threadIdx.x] = b.rows8[threadIdx.x];

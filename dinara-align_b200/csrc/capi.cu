@@ -463,7 +463,7 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
         // Every chunk's CIGAR bytes go straight into the caller's buffer, grown a chunk at a time.
         char *bytes = nullptr;
         size_t size = 0;
-        std::vector<int64_t> walk_spans(size_t(4 * pairs));
+        std::vector<int64_t> walk_spans(local ? size_t(4 * pairs) : 0);
         std::vector<int64_t> ends(size_t(pairs + 1));
         ends[0] = 0;
         int64_t first = 0;
@@ -492,7 +492,8 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
             std::vector<int64_t> chunk_offsets(size_t(count + 1));
             to_host(gpu, bytes + at, gpu->cigar_bytes.as<char>(), size_t(total));
             to_host(gpu, chunk_offsets.data(), gpu->cigar_offsets.as<int64_t>(), size_t(count + 1) * sizeof(int64_t));
-            to_host(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
+            // A global walk spans the whole pair, known on the host; only a local one's spans come back.
+            if (local) to_host(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
             DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
             for (int64_t k = 0; k < count; ++k) ends[size_t(first + k + 1)] = int64_t(at) + chunk_offsets[size_t(k + 1)];
             first += count;
@@ -503,7 +504,6 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         statuses_of(checked, local, pairs, offsets, unknown.data(), statuses);
         for (int64_t p = 0; p < pairs; ++p) {
-            const int64_t *w = walk_spans.data() + 4 * p;
             const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
             const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
             int64_t *span = spans + 4 * p;
@@ -513,6 +513,7 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
                 span[2] = 0;
                 span[3] = columns;
             } else {
+                const int64_t *w = walk_spans.data() + 4 * p;
                 const char *reference = letters + offsets[2 * p];
                 const char *query = letters + offsets[2 * p + 1];
                 const int64_t r0 = last_place(reference, rows, w[0], w[1]);

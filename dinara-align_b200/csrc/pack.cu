@@ -17,6 +17,9 @@ __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int
                                   int64_t pairs, const uint8_t *__restrict__ codes, int bits,
                                   uint32_t *__restrict__ tape, PairShape *__restrict__ shapes,
                                   uint8_t *__restrict__ unknown) {
+    __shared__ uint8_t code_of[256];
+    code_of[threadIdx.x & 255] = codes[threadIdx.x & 255];
+    __syncthreads();
     const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= pairs) return;
@@ -32,26 +35,43 @@ __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int
         const uint64_t word0 = packed_word_start(start, k, bits);
         starts[side] = uint32_t(word0);
         lengths[side] = uint32_t(length);
-        const int64_t chunks = (length + per_chunk - 1) / per_chunk;
-        for (int64_t c = lane; c < chunks; c += 32) {
-            uint32_t out[4];
+        // Lane i packs output words i, i + 32, ... (consecutive lanes, consecutive words: coalesced both
+        // ways), each from its letters read through aligned 32-bit words; the sequence's last chunk is
+        // zero-filled past its end. No load starts at or past the sequence's end.
+        const uintptr_t end = reinterpret_cast<uintptr_t>(letters + start + length);
+        const int64_t words = (length + per_chunk - 1) / per_chunk * 4;
+        for (int64_t w = lane; w < words; w += 32) {
+            const int64_t first = w * per_word;
+            uint32_t word = 0;
+            if (first < length) {
+                const uintptr_t address = reinterpret_cast<uintptr_t>(letters + start + first);
+                const uintptr_t aligned = address & ~uintptr_t(3);
+                const uint32_t shift = uint32_t(address & 3u) * 8u;
+                uint32_t raw[5];
 #pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                uint32_t word = 0;
-                for (int i = 0; i < per_word; ++i) {
-                    const int64_t index = c * per_chunk + w * per_word + i;
-                    if (index < length) {
-                        uint32_t code = codes[letters[start + index]];
-                        if (code == 255u) {
-                            bad = true;
-                            code = 0;
+                for (int r = 0; r < 5; ++r)
+                    raw[r] = (r <= per_word / 4) && aligned + 4 * uintptr_t(r) < end
+                                 ? __ldg(reinterpret_cast<const uint32_t *>(aligned) + r)
+                                 : 0u;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (q * 4 >= per_word) break;
+                    const uint32_t four = __funnelshift_r(raw[q], raw[q + 1], shift);
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int j = 4 * q + b;
+                        if (first + j < length) {
+                            uint32_t code = code_of[(four >> (8 * b)) & 0xFFu];
+                            if (code == 255u) {
+                                bad = true;
+                                code = 0;
+                            }
+                            word |= (code & mask) << (bits * j);
                         }
-                        word |= (code & mask) << (bits * i);
                     }
                 }
-                out[w] = word;
             }
-            *reinterpret_cast<uint4 *>(tape + word0 + 4 * c) = make_uint4(out[0], out[1], out[2], out[3]);
+            tape[word0 + uint64_t(w)] = word;
         }
     }
     bad = __any_sync(0xffffffffu, bad);
@@ -80,7 +100,7 @@ __device__ void classify_pair(const PairShape *__restrict__ shapes, const uint32
         strips = empty ? 0 : (shape.columns + width - 1) / width;
         const int64_t swept = int64_t(strips) * width;
         const bool pairs16 = cls != kWideClass && !record && !empty && limits.whole > 0 &&
-                             (limits.local ? swept <= limits.whole
+                             (limits.local ? swept * limits.best + int64_t(shape.rows) * limits.row_step <= limits.whole
                                            : 2 * swept <= limits.whole && 2 * int64_t(shape.rows) <= limits.whole);
         if (pairs16) cls += kWholePairsClass;
         if (strips > 255) strips = 255;

@@ -30,14 +30,17 @@ struct Schedule {
 };
 
 // Which pairs the 16-bit pair sweeps take: band pairs whose rows and columns sum to at most `band`; and,
-// scoring without a CIGAR, non-empty whole-matrix pairs whose swept columns are at most `whole` (local)
-// or whose rows and swept columns are each at most half of it (global). Zero takes none. With `wide`,
+// scoring without a CIGAR, non-empty whole-matrix pairs with best x swept columns + rows x row_step at
+// most `whole` (local) or whose rows and swept columns are each at most half of it (global). Zero takes none. With `wide`,
 // scoring without a CIGAR, whole-matrix pairs of at least kWideRows x kWideColumns go to kWideClass.
 struct PairLimits {
     int32_t band = 0;
     int32_t whole = 0;
     int32_t local = 0;
     int32_t wide = 0;
+    // Local: a pair fits when best x swept columns + rows x row_step is at most `whole`.
+    int32_t best = 1;
+    int32_t row_step = 0;
 };
 
 // The order of pairs [first, first + count), or of the `count` pairs listed in `list` (device) when given.
