@@ -330,8 +330,8 @@ def scores_tape(tape: Tape, scoring: Scoring, mode: Mode = Mode.GLOBAL, *, place
     struct, _table, _alphabet = scoring._struct()
     mode_struct = mode._struct()
     pairs = tape.pairs
-    out = np.zeros(max(pairs, 1), dtype=np.int32)
-    codes = np.zeros(max(pairs, 1), dtype=np.int64)
+    out = np.empty(max(pairs, 1), dtype=np.int32)
+    codes = np.empty(max(pairs, 1), dtype=np.int64)
     code = native.lib().dinara_gpu_scores_tape(handle, pairs, tape.letters.ctypes.data,
                                                 native.pointer(tape.offsets, ctypes.c_int64), ctypes.byref(struct),
                                                 ctypes.byref(mode_struct), native.pointer(out, ctypes.c_int32),
@@ -356,10 +356,10 @@ def alignments_tape(tape: Tape, scoring: Scoring, mode: Mode = Mode.GLOBAL, *, e
     struct, _table, _alphabet = scoring._struct()
     mode_struct = mode._struct()
     pairs = tape.pairs
-    out = np.zeros(max(pairs, 1), dtype=np.int32)
-    spans = np.zeros((max(pairs, 1), 4), dtype=np.int64)
-    offsets = np.zeros(pairs + 1, dtype=np.int64)
-    codes = np.zeros(max(pairs, 1), dtype=np.int64)
+    out = np.empty(max(pairs, 1), dtype=np.int32)
+    spans = np.empty((max(pairs, 1), 4), dtype=np.int64)
+    offsets = np.empty(pairs + 1, dtype=np.int64)
+    codes = np.empty(max(pairs, 1), dtype=np.int64)
     buffer = ctypes.c_void_p()
     code = native.lib().dinara_gpu_alignments_tape(handle, pairs, tape.letters.ctypes.data,
                                                     native.pointer(tape.offsets, ctypes.c_int64),
@@ -416,7 +416,7 @@ def distances_tape(tape: Tape, *, policy: int = native.BAND_PLAIN, start_thresho
     entries are the pair's own code), with the band report when asked."""
     handle = native.context(_placement(placement))
     pairs = tape.pairs
-    out = np.zeros(max(pairs, 1), dtype=np.int64)
+    out = np.empty(max(pairs, 1), dtype=np.int64)
     plan = native.CBandPlan(policy, None, default_start)
     starts = None
     if start_thresholds is not None:
