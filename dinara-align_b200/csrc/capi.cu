@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "affine.cuh"
@@ -151,6 +152,57 @@ void to_device(dinara_gpu *gpu, void *device, const void *host, size_t bytes, di
 void to_host(dinara_gpu *gpu, void *host, const void *device, size_t bytes) {
     if (bytes == 0) return;
     DINARA_CUDA(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, gpu->stream));
+}
+
+// A host copy shared by four threads.
+void parallel_copy(uint8_t *to, const uint8_t *from, size_t bytes) {
+    constexpr int kThreads = 4;
+    if (bytes < (size_t(1) << 20)) {
+        std::memcpy(to, from, bytes);
+        return;
+    }
+    const size_t part = (bytes + kThreads - 1) / kThreads;
+    std::thread helpers[kThreads - 1];
+    for (int t = 1; t < kThreads; ++t) {
+        const size_t begin = std::min(bytes, size_t(t) * part), end = std::min(bytes, begin + part);
+        helpers[t - 1] = std::thread([=] { std::memcpy(to + begin, from + begin, end - begin); });
+    }
+    std::memcpy(to, from, std::min(bytes, part));
+    for (auto &helper : helpers) helper.join();
+}
+
+// Copies `bytes` of device memory to host memory and waits for them. Large copies into pageable memory
+// (which the driver moves at a few GB/s) go through the context's page-locked staging a slice at a time,
+// each slice's transfer overlapping the host copy of the one before it.
+void to_host_now(dinara_gpu *gpu, void *host, const void *device, size_t bytes) {
+    if (bytes == 0) return;
+    const size_t slice = size_t(32) << 20;
+    if (bytes < (size_t(4) << 20) || is_pinned(host)) {
+        DINARA_CUDA(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, gpu->stream));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        return;
+    }
+    uint8_t *stage = gpu->pinned_out.ensure<uint8_t>(std::min(bytes, 2 * slice));
+    const uint8_t *from = static_cast<const uint8_t *>(device);
+    uint8_t *to = static_cast<uint8_t *>(host);
+    size_t at = 0;
+    int half = 0;
+    size_t previous_at = 0, previous_n = 0;
+    while (at < bytes) {
+        const size_t n = std::min(slice, bytes - at);
+        uint8_t *buffer = stage + (bytes > slice ? size_t(half) * slice : 0);
+        DINARA_CUDA(cudaMemcpyAsync(buffer, from + at, n, cudaMemcpyDeviceToHost, gpu->stream));
+        // The slice before this one, whose transfer the stream finished first, is copied meanwhile.
+        if (previous_n > 0) {
+            parallel_copy(to + previous_at, stage + (bytes > slice ? size_t(half ^ 1) * slice : 0), previous_n);
+        }
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        previous_at = at;
+        previous_n = n;
+        at += n;
+        half ^= 1;
+    }
+    parallel_copy(to + previous_at, stage + (bytes > slice ? size_t(half ^ 1) * slice : 0), previous_n);
 }
 
 // The batch's letters and offsets on the device, packed, with every pair's shape.
@@ -413,9 +465,8 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
         int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
         affine_scores(gpu, batch, checked.table, scores_device, 0, pairs);
         std::vector<uint8_t> unknown(static_cast<size_t>(pairs));
-        to_host(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
-        to_host(gpu, unknown.data(), packed.unknown, size_t(pairs));
-        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        to_host_now(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
+        to_host_now(gpu, unknown.data(), packed.unknown, size_t(pairs));
         statuses_of(checked, local, pairs, offsets, unknown.data(), statuses);
         return 0;
     });
@@ -490,39 +541,53 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
             bytes = grown;
             size = at + size_t(total);
             std::vector<int64_t> chunk_offsets(size_t(count + 1));
-            to_host(gpu, bytes + at, gpu->cigar_bytes.as<char>(), size_t(total));
-            to_host(gpu, chunk_offsets.data(), gpu->cigar_offsets.as<int64_t>(), size_t(count + 1) * sizeof(int64_t));
+            to_host_now(gpu, bytes + at, gpu->cigar_bytes.as<char>(), size_t(total));
+            to_host_now(gpu, chunk_offsets.data(), gpu->cigar_offsets.as<int64_t>(),
+                        size_t(count + 1) * sizeof(int64_t));
             // A global walk spans the whole pair, known on the host; only a local one's spans come back.
-            if (local) to_host(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
-            DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+            if (local)
+                to_host_now(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
             for (int64_t k = 0; k < count; ++k) ends[size_t(first + k + 1)] = int64_t(at) + chunk_offsets[size_t(k + 1)];
             first += count;
         }
         std::vector<uint8_t> unknown(static_cast<size_t>(pairs));
-        to_host(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
-        to_host(gpu, unknown.data(), packed.unknown, size_t(pairs));
-        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        to_host_now(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
+        to_host_now(gpu, unknown.data(), packed.unknown, size_t(pairs));
         statuses_of(checked, local, pairs, offsets, unknown.data(), statuses);
-        for (int64_t p = 0; p < pairs; ++p) {
-            const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-            const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-            int64_t *span = spans + 4 * p;
-            if (!local) {
-                span[0] = 0;
-                span[1] = rows;
-                span[2] = 0;
-                span[3] = columns;
-            } else {
-                const int64_t *w = walk_spans.data() + 4 * p;
-                const char *reference = letters + offsets[2 * p];
-                const char *query = letters + offsets[2 * p + 1];
-                const int64_t r0 = last_place(reference, rows, w[0], w[1]);
-                const int64_t c0 = last_place(query, columns, w[2], w[3]);
-                span[0] = r0;
-                span[1] = r0 + (w[1] - w[0]);
-                span[2] = c0;
-                span[3] = c0 + (w[3] - w[2]);
+        // Each pair's spans, a share of the pairs a thread.
+        auto place_spans = [&](int64_t begin, int64_t end) {
+            for (int64_t p = begin; p < end; ++p) {
+                const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
+                const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
+                int64_t *span = spans + 4 * p;
+                if (!local) {
+                    span[0] = 0;
+                    span[1] = rows;
+                    span[2] = 0;
+                    span[3] = columns;
+                } else {
+                    const int64_t *w = walk_spans.data() + 4 * p;
+                    const char *reference = letters + offsets[2 * p];
+                    const char *query = letters + offsets[2 * p + 1];
+                    const int64_t r0 = last_place(reference, rows, w[0], w[1]);
+                    const int64_t c0 = last_place(query, columns, w[2], w[3]);
+                    span[0] = r0;
+                    span[1] = r0 + (w[1] - w[0]);
+                    span[2] = c0;
+                    span[3] = c0 + (w[3] - w[2]);
+                }
             }
+        };
+        constexpr int kSpanThreads = 4;
+        if (pairs < 65536) {
+            place_spans(0, pairs);
+        } else {
+            std::thread helpers[kSpanThreads - 1];
+            const int64_t part = (pairs + kSpanThreads - 1) / kSpanThreads;
+            for (int t = 1; t < kSpanThreads; ++t)
+                helpers[t - 1] = std::thread(place_spans, std::min(pairs, t * part), std::min(pairs, (t + 1) * part));
+            place_spans(0, std::min(pairs, part));
+            for (auto &helper : helpers) helper.join();
         }
         if (cigar_offsets) std::memcpy(cigar_offsets, ends.data(), size_t(pairs + 1) * sizeof(int64_t));
         if (!bytes) bytes = static_cast<char *>(std::malloc(1));
@@ -612,8 +677,7 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
         band_doubling(gpu, pairs, letters_device, offsets_device, starts, plan ? plan->default_start : 0, results_device,
                       report);
         if (report) report->predict_ms = predict_ms;
-        to_host(gpu, results, results_device, size_t(pairs) * sizeof(int64_t));
-        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        to_host_now(gpu, results, results_device, size_t(pairs) * sizeof(int64_t));
         if (report) {
             int64_t cells = 0;
             for (int64_t p = 0; p < pairs; ++p)
