@@ -231,14 +231,42 @@ __device__ __forceinline__ uint32_t gather_flag(uint32_t acc, uint32_t v, int k)
     return k == 15 ? acc + flags : __umulhi(flags, 1u << (17 + k)) + acc;
 }
 
+// The 2-bit codes of the 32 letters of a pair's sequence (`length` letters from packed word `first_word`)
+// from letter index `start` on, letter j of the run at bits 2(j % 16) of out[j / 16]; letters before the
+// sequence or past its end read as code 0. Three aligned words, shifted into place and masked: no word
+// outside the sequence's own is read.
+__device__ __forceinline__ void run_of_letters(const uint32_t *__restrict__ tape, uint32_t first_word, int length,
+                                               int start, uint32_t out[2]) {
+    out[0] = out[1] = 0;
+    if (length <= 0) return;
+    const int word = start >> 4;  // arithmetic shift: the floor for starts before the sequence
+    const int last = (length - 1) >> 4;
+    uint32_t words[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) words[i] = __ldg(tape + first_word + min(max(word + i, 0), last));
+    const uint32_t shift = uint32_t(start & 15) * 2u;
+    out[0] = __funnelshift_r(words[0], words[1], shift);
+    out[1] = __funnelshift_r(words[1], words[2], shift);
+    // Keep letters j with 0 <= start + j < length (any word clamped above holds none of them).
+    const int first = max(-start, 0), final = min(length - 1 - start, 31);
+    if (final < first) {
+        out[0] = out[1] = 0;
+        return;
+    }
+    const uint64_t upto = final == 31 ? ~0ull : ((1ull << (2 * (final + 1))) - 1ull);
+    const uint64_t keep = upto & ~((1ull << (2 * first)) - 1ull);
+    out[0] &= uint32_t(keep);
+    out[1] &= uint32_t(keep >> 32);
+}
+
 template <bool RECORD>
 __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) {
     constexpr int G = kBandLanes, C = kBandColumns;
     constexpr int GPW = 32 / G;      // lane groups a warp
     constexpr int PPW = 2 * GPW;     // pairs a warp
-    // Rows a selector window serves: fewer when recording, whose longer body would outgrow the
-    // instruction cache unrolled over sixteen rows.
-    constexpr int U = RECORD ? 4 : 16;
+    // Rows a selector window serves: few enough that the unrolled body stays in the instruction cache
+    // (fewer when recording, whose body is longer); a refill costs a few instructions a column.
+    constexpr int U = RECORD ? 4 : 8;
     constexpr int WIN = C + U;
     __shared__ uint32_t rows8[4];
     if (threadIdx.x < 4) rows8[threadIdx.x] = b.rows8[threadIdx.x];
@@ -302,18 +330,17 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
         for (int r0 = 1; r0 <= warp_rows; r0 += U) {
             // Selectors of WIN consecutive columns from r0 + low + first_place, both pairs in one: bytes 0-1
             // pick pair A's entry (sign-extended to 16 bits) from its row, bytes 2-3 pair B's.
+            uint32_t codes[2][2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                run_of_letters(b.tape, sh[h].second_word, live[h] ? cols[h] : 0, r0 + low[h] + first_place - 1,
+                               codes[h]);
             uint32_t window[WIN];
 #pragma unroll
             for (int j = 0; j < WIN; ++j) {
-                uint32_t y[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int column = r0 + low[h] + first_place + j;
-                    y[h] = (live[h] && column >= 1 && column <= cols[h])
-                               ? letter_at<2>(b.tape, sh[h].second_word, uint32_t(column - 1))
-                               : 0u;
-                }
-                window[j] = (17u * y[0] + 128u) | ((17u * y[1] + 196u) << 8);
+                const uint32_t a = (codes[0][j >> 4] >> (2 * (j & 15))) & 3u;
+                const uint32_t c = (codes[1][j >> 4] >> (2 * (j & 15))) & 3u;
+                window[j] = (17u * a + 128u) | ((17u * c + 196u) << 8);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
