@@ -42,8 +42,8 @@ WORKLOADS = {
 def parse() -> argparse.Namespace:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=5)
-    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--steps", type=int, default=40)
+    parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--workload", choices=sorted(WORKLOADS), default="affine")
     parser.add_argument("--pairs", type=int, default=0, help="override the workload's pair count")
@@ -66,33 +66,37 @@ def make_workload(name: str, pairs: int, seed: int):
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock, max clock and throttle reasons while the timed region runs."""
+    """nvidia-smi samples of SM clock, max clock and throttle reasons, each with its time, from start() to
+    stop(); summary() keeps those taken inside a window (the timed region). The sampler starts well before
+    the timed region, since nvidia-smi takes a while to give its first sample."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.process = None
         self.file = None
 
-    def __enter__(self):
+    def start(self):
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.process = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.process = None
         return self
 
-    def __exit__(self, *exc):
+    def stop(self):
         if self.process:
             self.process.terminate()
             self.process.wait(timeout=10)
+            self.process = None
 
-    def summary(self) -> dict:
+    def summary(self, begin: float, end: float) -> dict:
+        """The samples taken between `begin` and `end` (time.time() seconds)."""
         if not self.file:
             return {}
         self.file.seek(0)
@@ -100,17 +104,23 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.file.read().splitlines():
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 8:
+            if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[0]))
-                maxima.append(float(parts[1]))
-            except ValueError:
+                at = time.mktime(time.strptime(parts[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                at += float("0." + parts[0].split(".")[1]) if "." in parts[0] else 0.0
+                clock, maximum = float(parts[1]), float(parts[2])
+            except (ValueError, IndexError):
                 continue
-            for name, flag in zip(names, parts[4:8]):
+            if not begin <= at <= end:
+                continue
+            sm.append(clock)
+            maxima.append(maximum)
+            for name, flag in zip(names, parts[5:9]):
                 if flag.lower() == "active":
                     reasons.add(name)
         os.unlink(self.file.name)
+        self.file = None
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(maxima), "reasons": sorted(reasons),
@@ -259,6 +269,8 @@ def main() -> None:
     import torch
 
     torch.cuda.set_device(local_rank)
+    # Clock samples from now on; the line keeps those inside the timed region.
+    clocks = Clocks(local_rank).start()
     dist = None
     if world > 1:
         import datetime
@@ -318,10 +330,12 @@ def main() -> None:
         dist.barrier()
     torch.cuda.synchronize()
     timings = []
-    with Clocks(local_rank) as clocks:
-        for _ in range(args.steps):
-            timings.append(step())
+    region_begin = time.time()
+    for _ in range(args.steps):
+        timings.append(step())
     torch.cuda.synchronize()
+    region_end = time.time()
+    clocks.stop()
     device_ms = sum(t.total_ms for t in timings)
     kernel_ms = sum(t.record_ms + t.kernel_ms for t in timings) / len(timings)
     launches = sum(t.launches for t in timings)
@@ -397,7 +411,7 @@ def main() -> None:
                        "parallelism": f"pairs sharded, {world} independent ranks"},
             "gcups": world * cells / (ms_per_step / 1e3) / 1e9,
             "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "clocks": clocks.summary(region_begin, region_end),
             "e2e": e2e,
         }
         swept = sum(t.cells for t in timings) / len(timings)
