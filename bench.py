@@ -436,9 +436,9 @@ def main() -> None:
                                 "peak_source": "measured in this run: DPX viaddmax chains on every SM, 2 ops each"}
         if "roofline" in line and args.workload == "affine":
             # DRAM bytes of the recording band sweep (dram__bytes_read.sum + dram__bytes_write.sum), from an
-            # ncu capture of 200,000 pairs of this distribution (8,052 bytes a pair: the recorded decisions
+            # ncu capture of 200,000 pairs of this distribution (8,217 bytes a pair: the recorded decisions
             # and the sectors filled around their stores), scaled to this batch.
-            line["roofline"]["traffic"] = 8052.0 * pairs
+            line["roofline"]["traffic"] = 8217.0 * pairs
             line["roofline"]["traffic_unit"] = "bytes per launch of the recording band sweep"
         elif "roofline" in line:
             line["roofline"]["traffic"] = None
