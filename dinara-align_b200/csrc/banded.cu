@@ -12,7 +12,7 @@
 //
 // The query's letters move one place along the band each row: a lane keeps the selectors of 32
 // consecutive letters and reads them at a place that advances with the row, the rows unrolled sixteen at
-// a time so every place is a constant, and refills the 32 every sixteen rows.
+// a time so every place is a constant, and refills the 32 every sixteen rows from three packed words.
 //
 // The band's score is accepted when every path leaving the band provably scores below it
 // (band_proves); then every optimal path lies inside it, so the band's cells on those paths hold the
@@ -27,6 +27,34 @@ namespace {
 using namespace sweep;
 
 constexpr int32_t kUnreached = -(1 << 28);  // below every score a sweep can hold (ScoreReach bounds them)
+
+// The 2-bit codes of the 32 letters of a pair's sequence (`length` letters from packed word `first_word`)
+// from letter index `start` on, letter j of the run at bits 2(j % 16) of out[j / 16]; letters before the
+// sequence or past its end read as code 0. Three aligned words, shifted into place and masked: no word
+// outside the sequence's own is read.
+__device__ __forceinline__ void run_of_letters(const uint32_t *__restrict__ tape, uint32_t first_word, int length,
+                                               int start, uint32_t out[2]) {
+    out[0] = out[1] = 0;
+    if (length <= 0) return;
+    const int word = start >> 4;  // arithmetic shift: the floor for starts before the sequence
+    const int last = (length - 1) >> 4;
+    uint32_t words[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) words[i] = __ldg(tape + first_word + min(max(word + i, 0), last));
+    const uint32_t shift = uint32_t(start & 15) * 2u;
+    out[0] = __funnelshift_r(words[0], words[1], shift);
+    out[1] = __funnelshift_r(words[1], words[2], shift);
+    // Keep letters j with 0 <= start + j < length (any word clamped above holds none of them).
+    const int first = max(-start, 0), final = min(length - 1 - start, 31);
+    if (final < first) {
+        out[0] = out[1] = 0;
+        return;
+    }
+    const uint64_t upto = final == 31 ? ~0ull : ((1ull << (2 * (final + 1))) - 1ull);
+    const uint64_t keep = upto & ~((1ull << (2 * first)) - 1ull);
+    out[0] &= uint32_t(keep);
+    out[1] &= uint32_t(keep >> 32);
+}
 
 template <bool RECORD>
 __global__ void __launch_bounds__(kBlock) banded_kernel(BandedBatch b) {
@@ -75,15 +103,13 @@ __global__ void __launch_bounds__(kBlock) banded_kernel(BandedBatch b) {
         uint64_t buffered[4] = {0, 0, 0, 0};
 
         for (int r0 = 1; r0 <= warp_rows; r0 += 16) {
-            // Selectors of the 32 letters from column r0 + low + first_place on (letter index one less).
+            // Selectors of the 32 letters from column r0 + low + first_place on (letter index one less);
+            // columns outside the pair read letter 0, which no real cell's value depends on.
+            uint32_t codes[2];
+            run_of_letters(b.tape, sh.second_word, live ? cols : 0, r0 + low + first_place - 1, codes);
             uint32_t window[32];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int column = r0 + low + first_place + j;  // the column whose letter place j holds
-                window[j] = (live && column >= 1 && column <= cols)
-                                ? selector_of(letter_at<2>(b.tape, sh.second_word, uint32_t(column - 1)))
-                                : 0x9999u;
-            }
+            for (int j = 0; j < 32; ++j) window[j] = selector_of((codes[j >> 4] >> (2 * (j & 15))) & 3u);
 #pragma unroll
             for (int u = 0; u < 16; ++u) {
                 const int row = r0 + u;
@@ -229,34 +255,6 @@ __device__ __forceinline__ uint32_t max2(uint32_t a, uint32_t b) { return __vima
 __device__ __forceinline__ uint32_t gather_flag(uint32_t acc, uint32_t v, int k) {
     const uint32_t flags = ~v & 0x80008000u;
     return k == 15 ? acc + flags : __umulhi(flags, 1u << (17 + k)) + acc;
-}
-
-// The 2-bit codes of the 32 letters of a pair's sequence (`length` letters from packed word `first_word`)
-// from letter index `start` on, letter j of the run at bits 2(j % 16) of out[j / 16]; letters before the
-// sequence or past its end read as code 0. Three aligned words, shifted into place and masked: no word
-// outside the sequence's own is read.
-__device__ __forceinline__ void run_of_letters(const uint32_t *__restrict__ tape, uint32_t first_word, int length,
-                                               int start, uint32_t out[2]) {
-    out[0] = out[1] = 0;
-    if (length <= 0) return;
-    const int word = start >> 4;  // arithmetic shift: the floor for starts before the sequence
-    const int last = (length - 1) >> 4;
-    uint32_t words[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) words[i] = __ldg(tape + first_word + min(max(word + i, 0), last));
-    const uint32_t shift = uint32_t(start & 15) * 2u;
-    out[0] = __funnelshift_r(words[0], words[1], shift);
-    out[1] = __funnelshift_r(words[1], words[2], shift);
-    // Keep letters j with 0 <= start + j < length (any word clamped above holds none of them).
-    const int first = max(-start, 0), final = min(length - 1 - start, 31);
-    if (final < first) {
-        out[0] = out[1] = 0;
-        return;
-    }
-    const uint64_t upto = final == 31 ? ~0ull : ((1ull << (2 * (final + 1))) - 1ull);
-    const uint64_t keep = upto & ~((1ull << (2 * first)) - 1ull);
-    out[0] &= uint32_t(keep);
-    out[1] &= uint32_t(keep >> 32);
 }
 
 template <bool RECORD>
