@@ -1,6 +1,7 @@
 // The C ABI (include/dinara_gpu.h): checks what the reference checks, moves the caller's letters to the
 // device, packs and schedules them there, runs the kernels and brings the results back.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -214,11 +215,32 @@ struct Packed {
     uint32_t max_rows = 0, max_columns = 0;
 };
 
+// Runs work(begin, end) over [0, count) on four threads when the count is large, else on this one; each
+// share is contiguous and the shares do not overlap.
+template <class F>
+void split_work(int64_t count, F &&work) {
+    constexpr int kThreads = 4;
+    if (count < 65536) {
+        work(int64_t(0), count);
+        return;
+    }
+    const int64_t part = (count + kThreads - 1) / kThreads;
+    std::thread helpers[kThreads - 1];
+    for (int t = 1; t < kThreads; ++t)
+        helpers[t - 1] = std::thread([&, t] { work(std::min(count, t * part), std::min(count, (t + 1) * part)); });
+    work(int64_t(0), std::min(count, part));
+    for (auto &helper : helpers) helper.join();
+}
+
 void check_offsets(int64_t pairs, const int64_t *offsets) {
     if (pairs < 0) throw Failure(DINARA_INVALID_LENGTH, "a negative pair count");
     if (pairs > 0 && !offsets) throw Failure(DINARA_INVALID_LENGTH, "no offsets");
-    for (int64_t k = 0; k < 2 * pairs; ++k)
-        if (offsets[k + 1] < offsets[k]) throw Failure(DINARA_INVALID_LENGTH, "a sequence's length below zero");
+    std::atomic<bool> falling{false};
+    split_work(2 * pairs, [&](int64_t begin, int64_t end) {
+        for (int64_t k = begin; k < end; ++k)
+            if (offsets[k + 1] < offsets[k]) falling = true;
+    });
+    if (falling) throw Failure(DINARA_INVALID_LENGTH, "a sequence's length below zero");
     if (pairs > 0 && offsets[0] < 0) throw Failure(DINARA_INVALID_LENGTH, "an offset below zero");
 }
 
@@ -268,17 +290,20 @@ int64_t record_words(int64_t rows, int64_t columns, bool uniform, bool band) {
 // Per-pair statuses: scores that could pass 2^28 (-3), then a letter outside the alphabet (-1).
 void statuses_of(const CheckedScoring &checked, bool local, int64_t pairs, const int64_t *offsets,
                  const uint8_t *unknown_host, int64_t *statuses) {
-    for (int64_t p = 0; p < pairs; ++p) {
-        const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-        const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-        const int64_t letters = local ? std::min(rows, columns) : rows + columns;
-        int64_t status = 0;
-        if (checked.reach_opening + 2 * (letters + 2) * checked.reach_step >= (int64_t(1) << 28))
-            status = DINARA_INVALID_COSTS;
-        else if (unknown_host[p])
-            status = DINARA_UNSUPPORTED_SYMBOLS;
-        if (statuses) statuses[p] = status;
-    }
+    if (!statuses) return;
+    split_work(pairs, [&](int64_t begin, int64_t end) {
+        for (int64_t p = begin; p < end; ++p) {
+            const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
+            const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
+            const int64_t letters = local ? std::min(rows, columns) : rows + columns;
+            int64_t status = 0;
+            if (checked.reach_opening + 2 * (letters + 2) * checked.reach_step >= (int64_t(1) << 28))
+                status = DINARA_INVALID_COSTS;
+            else if (unknown_host[p])
+                status = DINARA_UNSUPPORTED_SYMBOLS;
+            statuses[p] = status;
+        }
+    });
 }
 
 // A tape of the caller's pointer arrays, letters end to end (the reference's PairTape layout).
@@ -578,17 +603,7 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
                 }
             }
         };
-        constexpr int kSpanThreads = 4;
-        if (pairs < 65536) {
-            place_spans(0, pairs);
-        } else {
-            std::thread helpers[kSpanThreads - 1];
-            const int64_t part = (pairs + kSpanThreads - 1) / kSpanThreads;
-            for (int t = 1; t < kSpanThreads; ++t)
-                helpers[t - 1] = std::thread(place_spans, std::min(pairs, t * part), std::min(pairs, (t + 1) * part));
-            place_spans(0, std::min(pairs, part));
-            for (auto &helper : helpers) helper.join();
-        }
+        split_work(pairs, place_spans);
         if (cigar_offsets) std::memcpy(cigar_offsets, ends.data(), size_t(pairs + 1) * sizeof(int64_t));
         if (!bytes) bytes = static_cast<char *>(std::malloc(1));
         if (!bytes) throw std::bad_alloc();
