@@ -232,13 +232,26 @@ def serving_section(da) -> dict:
     rng = np.random.default_rng(55)
     requests = [workloads.serving_request(rng) for _ in range(100)]
     scoring = da.Scoring.uniform(0, -4, -6, -2)
+
+    def cells_of(batch):
+        return int(sum(((t.offsets[1::2] - t.offsets[0:-1:2]) * (t.offsets[2::2] - t.offsets[1::2])).sum()
+                       for t in batch))
+
     with serving.Server(slots=4, device_bytes=40 << 30) as server:
         out = serving.open_loop(server, requests, 2000.0, scoring)
         out["stats"] = server.stats()
-    out["cells"] = int(sum(((t.offsets[1::2] - t.offsets[0:-1:2]) * (t.offsets[2::2] - t.offsets[1::2])).sum()
-                           for t in requests))
+    out["cells"] = cells_of(requests)
     out["gcups"] = out["cells"] / out["seconds"] / 1e9
     out["offered_pairs_per_s"] = 2000.0 * float(np.mean([t.pairs for t in requests]))
+    # The same distribution offered at 5 requests/s, about a quarter of what the device sustains on these
+    # requests: latency with little standing queue (40 requests, about 8 s).
+    sustained = [workloads.serving_request(rng) for _ in range(40)]
+    with serving.Server(slots=4, device_bytes=40 << 30) as server:
+        steady = serving.open_loop(server, sustained, 5.0, scoring, seed=6)
+        steady["stats"] = server.stats()
+    steady["cells"] = cells_of(sustained)
+    steady["gcups"] = steady["cells"] / steady["seconds"] / 1e9
+    out["sustained_5_per_s"] = steady
     return out
 
 
