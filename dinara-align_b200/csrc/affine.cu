@@ -358,10 +358,16 @@ void upload_table32(dinara_gpu *gpu, const AffineTable &table, bool local, int32
             else if (!local) v -= 2 * table.extend;
             host[r * 33 + c] = v;
         }
-    int32_t *dev = gpu->table32.ensure<int32_t>(host.size());
-    DINARA_CUDA(cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice, gpu->stream));
-    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
-    *out = dev;
+    // The device copy is kept while the table stays the same: a batch's units each sweep with it, and a
+    // copy queued behind the batch's letters would wait for all of them.
+    if (gpu->table32_host != host || !gpu->table32.ptr) {
+        int32_t *dev = gpu->table32.ensure<int32_t>(host.size());
+        DINARA_CUDA(
+            cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(int32_t), cudaMemcpyHostToDevice, gpu->stream));
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        gpu->table32_host = host;
+    }
+    *out = gpu->table32.as<int32_t>();
 }
 
 // The sorted order's range of each class: classes in descending order (the whole-matrix 16-bit pair
@@ -538,8 +544,7 @@ void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     unsigned long long host = 0;
-    DINARA_CUDA(cudaMemcpyAsync(&host, out, sizeof host, cudaMemcpyDeviceToHost, gpu->stream));
-    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    read_back(gpu, &host, out, sizeof host);
     gpu->swept_cells += int64_t(host);
 }
 
@@ -603,8 +608,7 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
     affine_launch_all(gpu, batch, table, schedule_all, false, args);
     unsigned int left = 0;
     if (band_pairs(schedule_all) > 0) {
-        DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
-        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        read_back(gpu, &left, leftover_count, sizeof left);
         if (left > 0) {
             const Schedule again = dinara::schedule(gpu, batch.shapes, leftovers, 0, left, false, false,
                                                     whole_limits_of(batch, table));
@@ -645,9 +649,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, words, word_offsets, int(count + 1), gpu->stream));
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch2, slot_bytes, slot_offsets, int(count + 1), gpu->stream));
     int64_t totals[2];
-    DINARA_CUDA(cudaMemcpyAsync(&totals[0], word_offsets + count, sizeof(int64_t), cudaMemcpyDeviceToHost, gpu->stream));
-    DINARA_CUDA(cudaMemcpyAsync(&totals[1], slot_offsets + count, sizeof(int64_t), cudaMemcpyDeviceToHost, gpu->stream));
-    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    read_back(gpu, &totals[0], word_offsets + count, sizeof(int64_t));
+    read_back(gpu, &totals[1], slot_offsets + count, sizeof(int64_t));
     uint64_t *decisions = gpu->decisions.ensure<uint64_t>(size_t(totals[0]) + 8);
     char *slots = gpu->walk_out.ensure<char>(size_t(totals[1]) + 8);
     int64_t *ends = gpu->spans.ensure<int64_t>(size_t(count) + 1);
@@ -681,8 +684,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     affine_launch_all(gpu, batch, table, schedule_all, true, args);
     unsigned int left = 0;
     if (band_pairs(schedule_all) > 0) {
-        DINARA_CUDA(cudaMemcpyAsync(&left, leftover_count, sizeof left, cudaMemcpyDeviceToHost, gpu->stream));
-        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        read_back(gpu, &left, leftover_count, sizeof left);
         if (left > 0) {
             // The band's leftovers, swept whole: their decisions in the extra buffer.
             int64_t *left_words = gpu->thresholds.ensure<int64_t>(2 * (size_t(left) + 1) + 2);
@@ -698,9 +700,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
             space = gpu->sort_scratch.ensure<uint8_t>(bytes + 256);
             DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, bytes, left_words, left_offsets, int(left + 1), gpu->stream));
             int64_t extra_total = 0;
-            DINARA_CUDA(cudaMemcpyAsync(&extra_total, left_offsets + left, sizeof(int64_t), cudaMemcpyDeviceToHost,
-                                        gpu->stream));
-            DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+            read_back(gpu, &extra_total, left_offsets + left, sizeof(int64_t));
             extra = gpu->decisions_extra.ensure<uint64_t>(size_t(extra_total) + 8);
             leftover_places_kernel<<<left_blocks, threads, 0, gpu->stream>>>(leftovers, left, first_pair, left_offsets,
                                                                              word_offsets, layouts);
@@ -749,8 +749,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     space = gpu->sort_scratch.ensure<uint8_t>(scratch3 + 256);
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch3, lengths, offsets, int(count + 1), gpu->stream));
     int64_t total = 0;
-    DINARA_CUDA(cudaMemcpyAsync(&total, offsets + count, sizeof(int64_t), cudaMemcpyDeviceToHost, gpu->stream));
-    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    read_back(gpu, &total, offsets + count, sizeof(int64_t));
     char *out = gpu->cigar_bytes.ensure<char>(size_t(total) + 8);
     const unsigned gather_blocks = unsigned((count * 32 + threads - 1) / threads);
     gather_cigars_kernel<<<gather_blocks, threads, 0, gpu->stream>>>(slots, slot_offsets, lengths, offsets, out, count);

@@ -3,12 +3,19 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <exception>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <new>
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <sys/mman.h>
 
 #include "affine.cuh"
 #include "banded.cuh"
@@ -244,6 +251,24 @@ void check_offsets(int64_t pairs, const int64_t *offsets) {
     if (pairs > 0 && offsets[0] < 0) throw Failure(DINARA_INVALID_LENGTH, "an offset below zero");
 }
 
+// The batch's longest reference and longest query.
+void shape_maxima(int64_t pairs, const int64_t *offsets, uint32_t *max_rows, uint32_t *max_columns) {
+    std::atomic<uint32_t> rows{0}, columns{0};
+    split_work(pairs, [&](int64_t begin, int64_t end) {
+        uint32_t r = 0, c = 0;
+        for (int64_t p = begin; p < end; ++p) {
+            r = std::max<uint32_t>(r, uint32_t(offsets[2 * p + 1] - offsets[2 * p]));
+            c = std::max<uint32_t>(c, uint32_t(offsets[2 * p + 2] - offsets[2 * p + 1]));
+        }
+        for (uint32_t seen = rows.load(); seen < r && !rows.compare_exchange_weak(seen, r);) {
+        }
+        for (uint32_t seen = columns.load(); seen < c && !columns.compare_exchange_weak(seen, c);) {
+        }
+    });
+    *max_rows = rows.load();
+    *max_columns = columns.load();
+}
+
 Packed pack_batch(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets, const uint8_t codes[256],
                   int bits) {
     Packed out;
@@ -258,10 +283,7 @@ Packed pack_batch(dinara_gpu *gpu, int64_t pairs, const char *letters, const int
         for (int64_t k = 0; k <= 2 * pairs; ++k) relative[size_t(k)] = offsets[k] - first;
         device_offsets_host = relative.data();
     }
-    for (int64_t p = 0; p < pairs; ++p) {
-        out.max_rows = std::max<uint32_t>(out.max_rows, uint32_t(offsets[2 * p + 1] - offsets[2 * p]));
-        out.max_columns = std::max<uint32_t>(out.max_columns, uint32_t(offsets[2 * p + 2] - offsets[2 * p + 1]));
-    }
+    shape_maxima(pairs, offsets, &out.max_rows, &out.max_columns);
     uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
     int64_t *offsets_device = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
     uint8_t *codes_device = gpu->code_table.ensure<uint8_t>(256);
@@ -272,7 +294,7 @@ Packed pack_batch(dinara_gpu *gpu, int64_t pairs, const char *letters, const int
     out.tape = gpu->tape.ensure<uint32_t>(size_t(words));
     out.shapes = gpu->shapes.ensure<PairShape>(size_t(pairs));
     out.unknown = gpu->flags.ensure<uint8_t>(size_t(pairs));
-    pack_pairs(gpu, letters_device, offsets_device, pairs, codes_device, bits, out.tape, out.shapes, out.unknown);
+    pack_pairs(gpu, letters_device, offsets_device, 0, pairs, codes_device, bits, out.tape, out.shapes, out.unknown);
     return out;
 }
 
@@ -287,19 +309,20 @@ int64_t record_words(int64_t rows, int64_t columns, bool uniform, bool band) {
     return (columns + lanes * 16 - 1) / (lanes * 16) * lanes * (((rows + 2) | 3) + 1);
 }
 
-// Per-pair statuses: scores that could pass 2^28 (-3), then a letter outside the alphabet (-1).
-void statuses_of(const CheckedScoring &checked, bool local, int64_t pairs, const int64_t *offsets,
+// Per-pair statuses of pairs [first, first + count): scores that could pass 2^28 (-3), then a letter
+// outside the alphabet (-1); `unknown_host` holds the range's flags.
+void statuses_of(const CheckedScoring &checked, bool local, int64_t first, int64_t count, const int64_t *offsets,
                  const uint8_t *unknown_host, int64_t *statuses) {
     if (!statuses) return;
-    split_work(pairs, [&](int64_t begin, int64_t end) {
-        for (int64_t p = begin; p < end; ++p) {
+    split_work(count, [&](int64_t begin, int64_t end) {
+        for (int64_t p = first + begin; p < first + end; ++p) {
             const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
             const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
             const int64_t letters = local ? std::min(rows, columns) : rows + columns;
             int64_t status = 0;
             if (checked.reach_opening + 2 * (letters + 2) * checked.reach_step >= (int64_t(1) << 28))
                 status = DINARA_INVALID_COSTS;
-            else if (unknown_host[p])
+            else if (unknown_host[p - first])
                 status = DINARA_UNSUPPORTED_SYMBOLS;
             statuses[p] = status;
         }
@@ -341,6 +364,444 @@ int64_t last_place(const char *text, int64_t length, int64_t start, int64_t end)
     return start;
 }
 
+// A large batch runs as units of pairs, each packed, swept and walked while later units' letters are
+// still crossing the bus and earlier units' results are being moved into the caller's buffers.
+
+// Letters go to the device in pieces of this size.
+constexpr size_t kUploadPiece = size_t(32) << 20;
+// A batch runs in at most this many units, each of at least kUnitPairs pairs: fewer and the first
+// upload and the last unit's moves stand out; more and the units' fixed costs (schedules, host waits,
+// the tails of the sweeps) do.
+constexpr int64_t kMaxUnits = 8;
+constexpr int64_t kUnitPairs = 32768;
+// Units run on this many lanes (the context, then its partner).
+constexpr size_t kLanes = 2;
+
+// The caller's letters copied to the device a piece at a time on the context's upload stream. From
+// page-locked memory every piece is queued at once; from pageable memory a helper thread stages each
+// piece through page-locked memory (a four-thread copy) and queues it.
+class LetterUpload {
+  public:
+    LetterUpload(dinara_gpu *gpu, uint8_t *device, const uint8_t *host, size_t bytes)
+        : gpu_(gpu), device_(device), host_(host), bytes_(bytes) {
+        events_.assign((bytes + kUploadPiece - 1) / kUploadPiece, nullptr);
+        DINARA_CUDA(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming));
+        for (cudaEvent_t &event : events_) DINARA_CUDA(cudaEventCreateWithFlags(&event, cudaEventDisableTiming));
+        // The copies come after what the context's stream did before: the buffer's allocation and
+        // earlier calls' reads of it.
+        DINARA_CUDA(cudaEventRecord(ready_, gpu->stream));
+        DINARA_CUDA(cudaStreamWaitEvent(gpu->upload, ready_, 0));
+        if (events_.empty()) return;
+        if (is_pinned(host)) {
+            for (size_t piece = 0; piece < events_.size(); ++piece) queue(piece, host + piece * kUploadPiece);
+            queued_ = events_.size();
+            return;
+        }
+        stage_ = gpu->pinned_in.ensure<uint8_t>(std::min(bytes, 2 * kUploadPiece));
+        helper_ = std::thread([this] { stage_all(); });
+    }
+
+    ~LetterUpload() {
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            stop_ = true;
+        }
+        if (helper_.joinable()) helper_.join();
+        // Later work on the context's stream (the buffer's next growth, the next call's copies) comes
+        // after every queued copy.
+        if (queued_ > 0) cudaStreamWaitEvent(gpu_->stream, events_[queued_ - 1], 0);
+        for (cudaEvent_t event : events_)
+            if (event) cudaEventDestroy(event);
+        if (ready_) cudaEventDestroy(ready_);
+    }
+
+    // Makes `stream` wait until letters [0, end) are on the device.
+    void wait_for(size_t end, cudaStream_t stream) {
+        if (end == 0 || events_.empty()) return;
+        const size_t piece = std::min(events_.size(), (end + kUploadPiece - 1) / kUploadPiece) - 1;
+        {
+            std::unique_lock<std::mutex> lock(mutex_);
+            ready_cv_.wait(lock, [&] { return queued_ > piece || failure_; });
+            if (failure_) std::rethrow_exception(failure_);
+        }
+        DINARA_CUDA(cudaStreamWaitEvent(stream, events_[piece], 0));
+    }
+
+  private:
+    void queue(size_t piece, const uint8_t *from) {
+        const size_t at = piece * kUploadPiece, n = std::min(kUploadPiece, bytes_ - at);
+        DINARA_CUDA(cudaMemcpyAsync(device_ + at, from, n, cudaMemcpyHostToDevice, gpu_->upload));
+        DINARA_CUDA(cudaEventRecord(events_[piece], gpu_->upload));
+    }
+
+    void stage_all() {
+        try {
+            DINARA_CUDA(cudaSetDevice(gpu_->device));
+            for (size_t piece = 0; piece < events_.size(); ++piece) {
+                {
+                    std::lock_guard<std::mutex> lock(mutex_);
+                    if (stop_) return;
+                }
+                uint8_t *buffer = stage_ + (piece & 1) * kUploadPiece;
+                // This half's previous copy has left it.
+                if (piece >= 2) DINARA_CUDA(cudaEventSynchronize(events_[piece - 2]));
+                const size_t at = piece * kUploadPiece;
+                parallel_copy(buffer, host_ + at, std::min(kUploadPiece, bytes_ - at));
+                queue(piece, buffer);
+                {
+                    std::lock_guard<std::mutex> lock(mutex_);
+                    queued_ = piece + 1;
+                }
+                ready_cv_.notify_all();
+            }
+        } catch (...) {
+            std::lock_guard<std::mutex> lock(mutex_);
+            failure_ = std::current_exception();
+            ready_cv_.notify_all();
+        }
+    }
+
+    dinara_gpu *gpu_;
+    uint8_t *device_;
+    const uint8_t *host_;
+    size_t bytes_;
+    uint8_t *stage_ = nullptr;
+    cudaEvent_t ready_ = nullptr;
+    std::vector<cudaEvent_t> events_;
+    std::mutex mutex_;
+    std::condition_variable ready_cv_;
+    size_t queued_ = 0;
+    bool stop_ = false;
+    std::exception_ptr failure_;
+    std::thread helper_;
+};
+
+// A batch cut into contiguous units by letters (at most kMaxUnits, each of at least kUnitPairs pairs; one
+// unit when `split` is false), none of whose recorded decisions pass `budget_words` when `budgeted` (a
+// pair's decision words from `words_of`). The first and last units take half the letters of the others:
+// the first one's letters arrive sooner, and the last one's results leave sooner. When the whole batch's
+// decisions fit the budget, as they mostly do, the cuts are binary searches over the offsets.
+template <class W>
+std::vector<std::pair<int64_t, int64_t>> plan_units(int64_t pairs, const int64_t *offsets, bool split, W &&words_of,
+                                                    bool budgeted, int64_t budget_words) {
+    const int64_t letters = offsets[2 * pairs] - offsets[0];
+    const int64_t units = split ? std::min(kMaxUnits, std::max<int64_t>(1, pairs / kUnitPairs)) : 1;
+    // Unit u ends where the share of letters of units 0..u does: halves at both ends.
+    auto share_end = [&](int64_t u) {
+        if (u >= units) return letters;
+        const double whole = double(units - 1), before = 0.5 + double(u - 1);
+        return int64_t(double(letters) * before / whole);
+    };
+    std::vector<std::pair<int64_t, int64_t>> out;
+    std::atomic<int64_t> all_words{0};
+    if (budgeted)
+        split_work(pairs, [&](int64_t begin, int64_t end) {
+            int64_t sum = 0;
+            for (int64_t p = begin; p < end; ++p) sum += words_of(p);
+            all_words += sum;
+        });
+    if (!budgeted || all_words.load() <= budget_words) {
+        int64_t first = 0;
+        for (int64_t u = 1; u <= units && first < pairs; ++u) {
+            // The unit ends at the first pair starting at or past its share of the letters.
+            int64_t low = first + 1, high = pairs;
+            const int64_t goal = offsets[0] + share_end(u);
+            while (low < high) {
+                const int64_t middle = low + (high - low) / 2;
+                if (offsets[2 * middle] >= goal)
+                    high = middle;
+                else
+                    low = middle + 1;
+            }
+            const int64_t end = u == units ? pairs : low;
+            out.emplace_back(first, end - first);
+            first = end;
+        }
+        return out;
+    }
+    const int64_t target = (letters + units - 1) / units;
+    int64_t first = 0;
+    while (first < pairs) {
+        int64_t count = 0, w = 0;
+        const int64_t start = offsets[2 * first];
+        while (first + count < pairs) {
+            const int64_t p = first + count;
+            const int64_t wp = words_of(p);
+            if (count > 0 && (offsets[2 * p] - start >= target || w + wp > budget_words)) break;
+            w += wp;
+            ++count;
+        }
+        out.emplace_back(first, count);
+        first += count;
+    }
+    return out;
+}
+
+// Where a unit's results sit in its page-locked stage: CIGAR bytes, their offsets (count + 1), scores,
+// unknown-letter flags and, for local alignments, the walk's spans (4 a pair).
+struct StageLayout {
+    size_t cigars = 0, cigar_offsets = 0, scores = 0, unknown = 0, spans = 0, bytes = 0;
+    StageLayout(int64_t count, int64_t total, bool with_spans) {
+        auto up = [](size_t n) { return (n + 255) & ~size_t(255); };
+        cigar_offsets = up(size_t(total));
+        scores = cigar_offsets + up(size_t(count + 1) * sizeof(int64_t));
+        unknown = scores + up(size_t(count) * sizeof(int32_t));
+        spans = unknown + up(size_t(count));
+        bytes = spans + (with_spans ? size_t(4 * count) * sizeof(int64_t) : 0);
+    }
+};
+
+// A unit whose copies into a stage are queued.
+struct StagedUnit {
+    int64_t first = 0, count = 0, total = 0;
+    const uint8_t *stage = nullptr;
+    StageLayout layout{0, 0, false};
+};
+
+// Units' results moved from their stages into the caller's buffers in the units' order: by a helper
+// thread when the batch has more than one unit, so that work runs alongside later units' sweeps, else
+// on the caller's thread. Unit k writes stage k mod kStages, which it may do once unit k - kStages is
+// done. Units may be pushed out of order (from two lanes). The events that follow each unit's copies
+// are made and destroyed on the caller's thread: a destroy on the helper would wait on the driver
+// while the lanes call into it.
+class UnitFinisher {
+  public:
+    using Work = std::function<void(const StagedUnit &)>;
+    UnitFinisher(dinara_gpu *gpu, size_t units, Work work)
+        : gpu_(gpu), work_(std::move(work)), pending_(units), arrived_(units, false), done_(units, nullptr) {
+        for (cudaEvent_t &event : done_) DINARA_CUDA(cudaEventCreateWithFlags(&event, cudaEventDisableTiming));
+        if (units > 1) helper_ = std::thread([this] { run(); });
+    }
+
+    ~UnitFinisher() {
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            abandon_ = true;
+        }
+        cv_.notify_all();
+        if (helper_.joinable()) helper_.join();
+        for (cudaEvent_t event : done_)
+            if (event) cudaEventDestroy(event);
+    }
+
+    // The stage unit `index` is to write, once it is free.
+    uint8_t *stage_for(int64_t index, size_t bytes) {
+        {
+            std::unique_lock<std::mutex> lock(mutex_);
+            cv_.wait(lock, [&] { return finished_ + dinara_gpu::kStages > index || failure_; });
+            if (failure_) std::rethrow_exception(failure_);
+        }
+        return gpu_->stages[index % dinara_gpu::kStages].ensure<uint8_t>(bytes);
+    }
+
+    // Takes unit `index`, whose copies are queued on `stream`.
+    void push(int64_t index, const StagedUnit &unit, cudaStream_t stream) {
+        DINARA_CUDA(cudaEventRecord(done_[size_t(index)], stream));
+        if (!helper_.joinable()) {
+            finish_one(size_t(index), unit);
+            ++finished_;
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            pending_[size_t(index)] = unit;
+            arrived_[size_t(index)] = true;
+        }
+        cv_.notify_all();
+    }
+
+    // Stops the units' moves after a lane's failure; waiters rethrow it.
+    void fail(std::exception_ptr failure) {
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            if (!failure_) failure_ = failure;
+        }
+        cv_.notify_all();
+    }
+
+    // Waits until every unit is in the caller's buffers; rethrows a failure.
+    void finish() {
+        if (helper_.joinable()) helper_.join();
+        if (failure_) std::rethrow_exception(failure_);
+    }
+
+  private:
+    void finish_one(size_t index, const StagedUnit &unit) {
+        DINARA_CUDA(cudaEventSynchronize(done_[index]));
+        work_(unit);
+    }
+
+    void run() {
+        try {
+            DINARA_CUDA(cudaSetDevice(gpu_->device));
+            for (size_t next = 0; next < pending_.size(); ++next) {
+                StagedUnit unit;
+                {
+                    std::unique_lock<std::mutex> lock(mutex_);
+                    cv_.wait(lock, [&] { return arrived_[next] || failure_ || abandon_; });
+                    if (failure_ || abandon_) return;
+                    unit = pending_[next];
+                }
+                finish_one(next, unit);
+                {
+                    std::lock_guard<std::mutex> lock(mutex_);
+                    ++finished_;
+                }
+                cv_.notify_all();
+            }
+        } catch (...) {
+            fail(std::current_exception());
+        }
+    }
+
+    dinara_gpu *gpu_;
+    Work work_;
+    std::mutex mutex_;
+    std::condition_variable cv_;
+    std::vector<StagedUnit> pending_;
+    std::vector<bool> arrived_;
+    std::vector<cudaEvent_t> done_;
+    int64_t finished_ = 0;
+    bool abandon_ = false;
+    std::exception_ptr failure_;
+    std::thread helper_;
+};
+
+// Room for a batch's CIGARs taken at once, so that they never move as units arrive: `bound` bytes, which
+// an allocation this large takes as address space, mapped (with large pages where the system allows)
+// as the copies first touch it. Left empty, to grow a unit at a time, when the address space is refused.
+void reserve_cigars(std::unique_ptr<char, void (*)(void *)> &bytes, size_t &room, size_t bound) {
+    char *reserved = static_cast<char *>(std::malloc(bound));
+    if (!reserved) return;
+    bytes.reset(reserved);
+    room = bound;
+    const uintptr_t huge = uintptr_t(2) << 20;
+    const uintptr_t begin = (reinterpret_cast<uintptr_t>(reserved) + huge - 1) & ~(huge - 1);
+    const uintptr_t end = (reinterpret_cast<uintptr_t>(reserved) + bound) & ~(huge - 1);
+    if (end > begin) madvise(reinterpret_cast<void *>(begin), size_t(end - begin), MADV_HUGEPAGE);
+}
+
+// A batch whose letters are on their way to the device a piece at a time, with its packed form's buffers:
+// pack_unit packs a unit of pairs once its letters are there.
+struct StreamedBatch {
+    Packed packed;
+    int64_t base = 0;  // the batch's first letter in the caller's tape
+    int bits = 0;
+    const uint8_t *letters_device = nullptr;
+    const int64_t *offsets_device = nullptr;
+    const uint8_t *codes_device = nullptr;
+    int32_t *scores = nullptr;  // every pair's score on the device
+    std::unique_ptr<LetterUpload> upload;
+    // Follows the buffers' allocations and the offsets' and codes' copies on the batch's context's stream.
+    cudaEvent_t inputs_ready = nullptr;
+
+    StreamedBatch() = default;
+    StreamedBatch(const StreamedBatch &) = delete;
+    StreamedBatch &operator=(const StreamedBatch &) = delete;
+    ~StreamedBatch() {
+        upload.reset();
+        if (inputs_ready) cudaEventDestroy(inputs_ready);
+    }
+
+    // Packs a unit on `ctx`'s stream (the batch's context or its partner) once its letters are there.
+    void pack_unit(dinara_gpu *ctx, const int64_t *offsets, int64_t first, int64_t count) {
+        upload->wait_for(size_t(offsets[2 * (first + count)] - base), ctx->stream);
+        pack_pairs(ctx, letters_device, offsets_device, first, count, codes_device, bits, packed.tape, packed.shapes,
+                   packed.unknown);
+    }
+};
+
+void start_batch(StreamedBatch &out, dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                 const uint8_t codes[256], int bits) {
+    out.packed.pairs = pairs;
+    out.base = offsets[0];
+    out.bits = bits;
+    const int64_t total = offsets[2 * pairs] - out.base;
+    // The code table is copied only when it changes: it comes from pageable memory, a copy the host
+    // waits for, behind whatever is queued before it.
+    const bool new_codes = !gpu->code_table.ptr || std::memcmp(gpu->codes_host, codes, 256) != 0;
+    uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
+    int64_t *offsets_device = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
+    uint8_t *codes_device = gpu->code_table.ensure<uint8_t>(256);
+    if (new_codes) {
+        DINARA_CUDA(cudaMemcpyAsync(codes_device, codes, 256, cudaMemcpyHostToDevice, gpu->stream));
+        std::memcpy(gpu->codes_host, codes, 256);
+    }
+    out.packed.tape = gpu->tape.ensure<uint32_t>(size_t(packed_words_total(total, 2 * pairs, bits)));
+    out.packed.shapes = gpu->shapes.ensure<PairShape>(size_t(pairs));
+    out.packed.unknown = gpu->flags.ensure<uint8_t>(size_t(pairs));
+    out.scores = gpu->scores.ensure<int32_t>(size_t(pairs));
+    out.letters_device = letters_device;
+    out.offsets_device = offsets_device;
+    out.codes_device = codes_device;
+    // The offsets (from the batch's first letter) on the context's stream, then the letters on the upload
+    // stream: copies in one direction share the copy engines in the order they are queued, so the small
+    // ones go first.
+    std::vector<int64_t> relative;
+    const int64_t *device_offsets_host = offsets;
+    if (out.base != 0) {
+        relative.resize(size_t(2 * pairs + 1));
+        split_work(2 * pairs + 1, [&](int64_t begin, int64_t end) {
+            for (int64_t k = begin; k < end; ++k) relative[size_t(k)] = offsets[k] - out.base;
+        });
+        device_offsets_host = relative.data();
+    }
+    to_device(gpu, offsets_device, device_offsets_host, size_t(2 * pairs + 1) * sizeof(int64_t), gpu->pinned_small);
+    DINARA_CUDA(cudaEventCreateWithFlags(&out.inputs_ready, cudaEventDisableTiming));
+    DINARA_CUDA(cudaEventRecord(out.inputs_ready, gpu->stream));
+    out.upload = std::make_unique<LetterUpload>(gpu, letters_device,
+                                                reinterpret_cast<const uint8_t *>(letters) + out.base, size_t(total));
+    shape_maxima(pairs, offsets, &out.packed.max_rows, &out.packed.max_columns);
+}
+
+// The context's partner, set up at its first use and freed with the context.
+dinara_gpu *partner_of(dinara_gpu *gpu) {
+    if (!gpu->partner) {
+        gpu->partner = dinara_gpu_new(gpu->device);
+        if (!gpu->partner) throw Failure(DINARA_DEVICE_FAILURE, "a second stream for a batch's units: " + new_error);
+    }
+    return gpu->partner;
+}
+
+// Runs body(ctx, k) for every unit k of a batch. With `lanes` 2 (and more than one unit), units alternate
+// between the context and its partner (a second stream with scratch buffers of its own), each driven by
+// its own thread, so that one unit's last pairs, copies and host waits overlap the next unit's sweeps.
+template <class F>
+void run_units(dinara_gpu *gpu, const StreamedBatch &streamed, size_t units, size_t lanes, UnitFinisher &finisher,
+               F &&body) {
+    if (units < 2) lanes = 1;
+    dinara_gpu *contexts[2] = {gpu, lanes > 1 ? partner_of(gpu) : nullptr};
+    std::exception_ptr failures[2];
+    auto lane = [&](size_t l) {
+        try {
+            dinara_gpu *ctx = contexts[l];
+            AllocationScope scope(ctx->stream);
+            DINARA_CUDA(cudaSetDevice(gpu->device));
+            if (ctx != gpu) DINARA_CUDA(cudaStreamWaitEvent(ctx->stream, streamed.inputs_ready, 0));
+            for (size_t k = l; k < units; k += lanes) body(ctx, k);
+        } catch (...) {
+            failures[l] = std::current_exception();
+            finisher.fail(failures[l]);
+        }
+    };
+    std::thread helper;
+    if (lanes > 1) helper = std::thread(lane, size_t(1));
+    lane(0);
+    if (helper.joinable()) helper.join();
+    if (lanes > 1) {
+        // Later work on the context's stream comes after everything the partner queued.
+        cudaEvent_t joined = nullptr;
+        if (cudaEventCreateWithFlags(&joined, cudaEventDisableTiming) == cudaSuccess) {
+            if (cudaEventRecord(joined, contexts[1]->stream) == cudaSuccess) cudaStreamWaitEvent(gpu->stream, joined, 0);
+            cudaEventDestroy(joined);
+        } else {
+            cudaStreamSynchronize(contexts[1]->stream);
+        }
+    }
+    for (std::exception_ptr &failure : failures)
+        if (failure) std::rethrow_exception(failure);
+}
+
 // The resident batch: packed letters kept on the device between calls.
 struct Resident {
     int64_t pairs = 0;
@@ -352,6 +813,8 @@ struct Resident {
     const int64_t *offsets_device = nullptr;
     int64_t cells = 0;
     int last = 0;  // 1 scores, 2 distances
+    // The cuts of a recording pass (global, then local), planned at the first one.
+    std::vector<std::pair<int64_t, int64_t>> plans[2];
 };
 
 void free_resident(void *pointer) { delete static_cast<Resident *>(pointer); }
@@ -421,6 +884,8 @@ dinara_gpu *dinara_gpu_new(int64_t device) {
         gpu->multiprocessors = properties.multiProcessorCount;
         std::snprintf(gpu->name, sizeof gpu->name, "%s", properties.name);
         DINARA_CUDA(cudaStreamCreateWithFlags(&gpu->stream, cudaStreamNonBlocking));
+        DINARA_CUDA(cudaStreamCreateWithFlags(&gpu->upload, cudaStreamNonBlocking));
+        DINARA_CUDA(cudaMallocHost(&gpu->readback, dinara::kReadbackBytes));
         // The device's pool keeps what contexts free for their next growth instead of handing it back at
         // every synchronisation (this process's pool only; nothing outlives it).
         cudaMemPool_t pool = nullptr;
@@ -444,15 +909,20 @@ dinara_gpu *dinara_gpu_new(int64_t device) {
 
 void dinara_gpu_free(dinara_gpu *gpu) {
     if (!gpu) return;
+    if (gpu->partner) dinara_gpu_free(gpu->partner);
+    gpu->partner = nullptr;
     cudaSetDevice(gpu->device);
     AllocationScope scope(gpu->stream);
     if (gpu->stream) cudaStreamSynchronize(gpu->stream);
+    if (gpu->upload) cudaStreamSynchronize(gpu->upload);
     if (gpu->resident) gpu->resident_free(gpu->resident);
     gpu->for_each_buffer([](dinara::DeviceBuffer &buffer) { buffer.release(); });
     if (gpu->stream) cudaStreamSynchronize(gpu->stream);
     gpu->pinned_in.release();
     gpu->pinned_out.release();
     gpu->pinned_small.release();
+    for (dinara::PinnedBuffer &stage : gpu->stages) stage.release();
+    if (gpu->readback) cudaFreeHost(gpu->readback);
     if (gpu->start) cudaEventDestroy(gpu->start);
     if (gpu->stop) cudaEventDestroy(gpu->stop);
     if (gpu->fork) cudaEventDestroy(gpu->fork);
@@ -460,6 +930,7 @@ void dinara_gpu_free(dinara_gpu *gpu) {
         if (gpu->side[k]) cudaStreamDestroy(gpu->side[k]);
         if (gpu->joins[k]) cudaEventDestroy(gpu->joins[k]);
     }
+    if (gpu->upload) cudaStreamDestroy(gpu->upload);
     if (gpu->stream) cudaStreamDestroy(gpu->stream);
     delete gpu;
 }
@@ -485,14 +956,33 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
         check_offsets(pairs, offsets);
         if (pairs == 0) return 0;
         DINARA_CUDA(cudaSetDevice(gpu->device));
-        Packed packed = pack_batch(gpu, pairs, letters, offsets, checked.codes, checked.bits);
+        StreamedBatch streamed;
+        start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
+        const Packed &packed = streamed.packed;
         AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
-        int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
-        affine_scores(gpu, batch, checked.table, scores_device, 0, pairs);
-        std::vector<uint8_t> unknown(static_cast<size_t>(pairs));
-        to_host_now(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
-        to_host_now(gpu, unknown.data(), packed.unknown, size_t(pairs));
-        statuses_of(checked, local, pairs, offsets, unknown.data(), statuses);
+        int32_t *scores_device = streamed.scores;
+        const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
+        UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
+            std::memcpy(scores + unit.first, unit.stage + unit.layout.scores, size_t(unit.count) * sizeof(int32_t));
+            statuses_of(checked, local, unit.first, unit.count, offsets, unit.stage + unit.layout.unknown, statuses);
+        });
+        run_units(gpu, streamed, units.size(), kLanes, finisher, [&](dinara_gpu *ctx, size_t k) {
+            const int64_t first = units[k].first, count = units[k].second;
+            streamed.pack_unit(ctx, offsets, first, count);
+            affine_scores(ctx, batch, checked.table, scores_device, first, count);
+            StagedUnit unit;
+            unit.first = first;
+            unit.count = count;
+            unit.layout = StageLayout(count, 0, false);
+            uint8_t *stage = finisher.stage_for(int64_t(k), unit.layout.bytes);
+            unit.stage = stage;
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.scores, scores_device + first,
+                                        size_t(count) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.unknown, packed.unknown + first, size_t(count),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+            finisher.push(int64_t(k), unit, ctx->stream);
+        });
+        finisher.finish();
         return 0;
     });
 }
@@ -529,89 +1019,110 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
             return 0;
         }
         DINARA_CUDA(cudaSetDevice(gpu->device));
-        Packed packed = pack_batch(gpu, pairs, letters, offsets, checked.codes, checked.bits);
+        StreamedBatch streamed;
+        start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
+        const Packed &packed = streamed.packed;
         AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
-        int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(pairs));
-        // Chunks whose recorded decisions stay within a budget of device memory.
-        const int64_t budget_words = kDecisionBudget / 8;
+        int32_t *scores_device = streamed.scores;
+        // Units whose recorded decisions stay within a budget of device memory.
         const bool uniform = !checked.table.packed16 || checked.bits == 8;
         const bool band = band_serves(batch, checked.table);
-        // Every chunk's CIGAR bytes go straight into the caller's buffer, grown a chunk at a time.
-        char *bytes = nullptr;
-        size_t size = 0;
-        std::vector<int64_t> walk_spans(local ? size_t(4 * pairs) : 0);
-        std::vector<int64_t> ends(size_t(pairs + 1));
-        ends[0] = 0;
-        int64_t first = 0;
-        while (first < pairs) {
-            int64_t count = 0, words = 0;
-            while (first + count < pairs) {
-                const int64_t p = first + count;
-                const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-                const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                const int64_t w = record_words(rows, columns, uniform, band);
-                if (count > 0 && words + w > budget_words) break;
-                words += w;
-                ++count;
+        const auto units = plan_units(
+            pairs, offsets, true,
+            [&](int64_t p) {
+                return record_words(offsets[2 * p + 1] - offsets[2 * p], offsets[2 * p + 2] - offsets[2 * p + 1],
+                                    uniform, band);
+            },
+            true, kDecisionBudget / 8);
+        // Every unit's CIGAR bytes go straight into the caller's buffer.
+        std::unique_ptr<char, void (*)(void *)> bytes(nullptr, std::free);
+        size_t room = 0, size = 0;
+        reserve_cigars(bytes, room, 2 * size_t(offsets[2 * pairs] - offsets[0]) + 1);
+        if (cigar_offsets) cigar_offsets[0] = 0;
+        UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
+            if (size + size_t(unit.total) + 1 > room) {
+                char *grown = static_cast<char *>(std::realloc(bytes.get(), size + size_t(unit.total) + 1));
+                if (!grown) throw std::bad_alloc();
+                bytes.release();
+                bytes.reset(grown);
+                room = size + size_t(unit.total) + 1;
             }
-            int64_t *spans_device = gpu->ranges.ensure<int64_t>(size_t(4 * count));
-            const int64_t total = affine_alignments(gpu, batch, checked.table, eqx != 0, scores_device, spans_device,
-                                                    first, count);
-            const size_t at = size;
-            char *grown = static_cast<char *>(std::realloc(bytes, at + size_t(total) + 1));
-            if (!grown) {
-                std::free(bytes);
-                throw std::bad_alloc();
-            }
-            bytes = grown;
-            size = at + size_t(total);
-            std::vector<int64_t> chunk_offsets(size_t(count + 1));
-            to_host_now(gpu, bytes + at, gpu->cigar_bytes.as<char>(), size_t(total));
-            to_host_now(gpu, chunk_offsets.data(), gpu->cigar_offsets.as<int64_t>(),
-                        size_t(count + 1) * sizeof(int64_t));
+            parallel_copy(reinterpret_cast<uint8_t *>(bytes.get()) + size, unit.stage + unit.layout.cigars,
+                          size_t(unit.total));
+            const int64_t *ends = reinterpret_cast<const int64_t *>(unit.stage + unit.layout.cigar_offsets);
+            const int64_t *walked = reinterpret_cast<const int64_t *>(unit.stage + unit.layout.spans);
+            std::memcpy(scores + unit.first, unit.stage + unit.layout.scores, size_t(unit.count) * sizeof(int32_t));
+            statuses_of(checked, local, unit.first, unit.count, offsets, unit.stage + unit.layout.unknown, statuses);
+            const int64_t at = int64_t(size);
+            // Each pair's CIGAR end and spans, a share of the unit's pairs a thread.
+            split_work(unit.count, [&](int64_t begin, int64_t end) {
+                for (int64_t k = begin; k < end; ++k) {
+                    const int64_t p = unit.first + k;
+                    if (cigar_offsets) cigar_offsets[p + 1] = at + ends[k + 1];
+                    const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
+                    const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
+                    int64_t *span = spans + 4 * p;
+                    if (!local) {
+                        // A global walk spans the whole pair.
+                        span[0] = 0;
+                        span[1] = rows;
+                        span[2] = 0;
+                        span[3] = columns;
+                    } else {
+                        const int64_t *w = walked + 4 * k;
+                        const char *reference = letters + offsets[2 * p];
+                        const char *query = letters + offsets[2 * p + 1];
+                        const int64_t r0 = last_place(reference, rows, w[0], w[1]);
+                        const int64_t c0 = last_place(query, columns, w[2], w[3]);
+                        span[0] = r0;
+                        span[1] = r0 + (w[1] - w[0]);
+                        span[2] = c0;
+                        span[3] = c0 + (w[3] - w[2]);
+                    }
+                }
+            });
+            size += size_t(unit.total);
+        });
+        run_units(gpu, streamed, units.size(), kLanes, finisher, [&](dinara_gpu *ctx, size_t k) {
+            const int64_t first = units[k].first, count = units[k].second;
+            streamed.pack_unit(ctx, offsets, first, count);
+            int64_t *spans_device = ctx->ranges.ensure<int64_t>(size_t(4 * count));
+            StagedUnit unit;
+            unit.first = first;
+            unit.count = count;
+            unit.total = affine_alignments(ctx, batch, checked.table, eqx != 0, scores_device, spans_device, first,
+                                           count);
+            unit.layout = StageLayout(count, unit.total, local);
+            uint8_t *stage = finisher.stage_for(int64_t(k), unit.layout.bytes);
+            unit.stage = stage;
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.cigars, ctx->cigar_bytes.as<char>(), size_t(unit.total),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.cigar_offsets, ctx->cigar_offsets.as<int64_t>(),
+                                        size_t(count + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.scores, scores_device + first,
+                                        size_t(count) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.unknown, packed.unknown + first, size_t(count),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
             // A global walk spans the whole pair, known on the host; only a local one's spans come back.
             if (local)
-                to_host_now(gpu, walk_spans.data() + 4 * first, spans_device, size_t(4 * count) * sizeof(int64_t));
-            for (int64_t k = 0; k < count; ++k) ends[size_t(first + k + 1)] = int64_t(at) + chunk_offsets[size_t(k + 1)];
-            first += count;
-        }
-        std::vector<uint8_t> unknown(static_cast<size_t>(pairs));
-        to_host_now(gpu, scores, scores_device, size_t(pairs) * sizeof(int32_t));
-        to_host_now(gpu, unknown.data(), packed.unknown, size_t(pairs));
-        statuses_of(checked, local, pairs, offsets, unknown.data(), statuses);
-        // Each pair's spans, a share of the pairs a thread.
-        auto place_spans = [&](int64_t begin, int64_t end) {
-            for (int64_t p = begin; p < end; ++p) {
-                const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-                const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                int64_t *span = spans + 4 * p;
-                if (!local) {
-                    span[0] = 0;
-                    span[1] = rows;
-                    span[2] = 0;
-                    span[3] = columns;
-                } else {
-                    const int64_t *w = walk_spans.data() + 4 * p;
-                    const char *reference = letters + offsets[2 * p];
-                    const char *query = letters + offsets[2 * p + 1];
-                    const int64_t r0 = last_place(reference, rows, w[0], w[1]);
-                    const int64_t c0 = last_place(query, columns, w[2], w[3]);
-                    span[0] = r0;
-                    span[1] = r0 + (w[1] - w[0]);
-                    span[2] = c0;
-                    span[3] = c0 + (w[3] - w[2]);
-                }
-            }
-        };
-        split_work(pairs, place_spans);
-        if (cigar_offsets) std::memcpy(cigar_offsets, ends.data(), size_t(pairs + 1) * sizeof(int64_t));
-        if (!bytes) bytes = static_cast<char *>(std::malloc(1));
+                DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.spans, spans_device,
+                                            size_t(4 * count) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                            ctx->stream));
+            finisher.push(int64_t(k), unit, ctx->stream);
+        });
+        finisher.finish();
+        if (!bytes) bytes.reset(static_cast<char *>(std::malloc(1)));
         if (!bytes) throw std::bad_alloc();
-        bytes[size] = 0;
-        if (cigar_bytes)
-            *cigar_bytes = bytes;
-        else
-            std::free(bytes);
+        if (room > size + 1) {
+            // The reservation's untouched rest handed back.
+            char *shrunk = static_cast<char *>(std::realloc(bytes.get(), size + 1));
+            if (shrunk) {
+                bytes.release();
+                bytes.reset(shrunk);
+            }
+        }
+        bytes.get()[size] = 0;
+        if (cigar_bytes) *cigar_bytes = bytes.release();
         return 0;
     });
 }
@@ -786,24 +1297,23 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         if (!cigars) {
             affine_scores(gpu, batch, r.checked.table, scores_device, 0, r.pairs);
         } else {
-            const int64_t budget_words = kDecisionBudget / 8;
+            // The whole batch in one launch sequence, cut only where its decisions would pass the budget;
+            // the cuts are planned at the first pass.
             const bool uniform = !r.checked.table.packed16 || r.checked.bits == 8;
             const bool band = band_serves(batch, r.checked.table);
-            int64_t first = 0;
-            while (first < r.pairs) {
-                int64_t count = 0, words = 0;
-                while (first + count < r.pairs) {
-                    const int64_t p = first + count;
-                    const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
-                    const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
-                    const int64_t w = record_words(rows, columns, uniform, band);
-                    if (count > 0 && words + w > budget_words) break;
-                    words += w;
-                    ++count;
-                }
-                int64_t *spans_device = gpu->ranges.ensure<int64_t>(size_t(4 * count));
-                affine_alignments(gpu, batch, r.checked.table, eqx != 0, scores_device, spans_device, first, count);
-                first += count;
+            std::vector<std::pair<int64_t, int64_t>> &units = r.plans[local ? 1 : 0];
+            if (units.empty())
+                units = plan_units(
+                    r.pairs, offsets, false,
+                    [&](int64_t p) {
+                        return record_words(offsets[2 * p + 1] - offsets[2 * p],
+                                            offsets[2 * p + 2] - offsets[2 * p + 1], uniform, band);
+                    },
+                    true, kDecisionBudget / 8);
+            for (const auto &unit : units) {
+                int64_t *spans_device = gpu->ranges.ensure<int64_t>(size_t(4 * unit.second));
+                affine_alignments(gpu, batch, r.checked.table, eqx != 0, scores_device, spans_device, unit.first,
+                                  unit.second);
             }
         }
         r.last = 1;

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "dinara_gpu.h"
 
@@ -127,6 +128,8 @@ struct dinara_gpu {
     int multiprocessors = 0;
     char name[256] = {0};
     cudaStream_t stream = nullptr;
+    // Copies of the caller's letters, a piece at a time, alongside the kernels on `stream`.
+    cudaStream_t upload = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
     // Side streams that let a round's launches of different shapes run at once, joined by events.
     static constexpr int kSideStreams = 23;  // one for each band window shape
@@ -141,6 +144,9 @@ struct dinara_gpu {
     // Outputs and per-launch scratch.
     dinara::DeviceBuffer scores, carry, decisions, decision_offsets, walk_out, cigar_slots, cigar_lengths,
         cigar_offsets, cigar_bytes, spans;
+    // The host copies of what code_table and table32 hold.
+    uint8_t codes_host[256] = {0};
+    std::vector<int32_t> table32_host;
     // Unit-cost band state.
     dinara::DeviceBuffer planes, plane_offsets, thresholds, distances, pending, pending_next, counters, table32;
     // Learned band predictor.
@@ -150,11 +156,20 @@ struct dinara_gpu {
     double predictor_margins[4] = {1.25, 1.25, 1.25, 1.25};  // by mean length: < 300, < 1000, < 4096, more
     double predictor_slack = 0.0;
     dinara::PinnedBuffer pinned_in, pinned_out, pinned_small;
+    // Page-locked stages a batch's results come back through, a unit of pairs at a time.
+    static constexpr int kStages = 4;
+    dinara::PinnedBuffer stages[kStages];
+    // Page-locked words the host reads totals and counts into between launches (a read into pageable
+    // memory would wait on the driver's staging, which other threads' calls contend for).
+    int64_t *readback = nullptr;
     // Device timing of the sweep kernels, accumulated while `timing` is set.
     bool timing = false;
     double kernel_ms = 0.0, record_ms = 0.0;
     int64_t launches = 0;
     int64_t swept_cells = 0;  // cells the sweeps updated (bands, whole matrices, leftovers)
+    // A second stream with scratch buffers of its own, so that two units of a large batch run at once
+    // (capi.cu); set up at its first use.
+    dinara_gpu *partner = nullptr;
     // The resident batch (capi.cu), if one is loaded.
     void *resident = nullptr;
     void (*resident_free)(void *) = nullptr;
@@ -172,3 +187,19 @@ struct dinara_gpu {
         for (dinara::DeviceBuffer *buffer : all) visit(*buffer);
     }
 };
+
+namespace dinara {
+
+// Bytes the context's page-locked readback words hold.
+constexpr size_t kReadbackBytes = 512;
+
+// Copies `bytes` (at most kReadbackBytes) of device memory to `host` once the context's stream reaches
+// the copy, through its page-locked readback words, and waits for it.
+inline void read_back(dinara_gpu *gpu, void *host, const void *device, size_t bytes) {
+    if (bytes > kReadbackBytes) throw Failure(DINARA_DEVICE_FAILURE, "a read back past the readback words");
+    DINARA_CUDA(cudaMemcpyAsync(gpu->readback, device, bytes, cudaMemcpyDeviceToHost, gpu->stream));
+    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    std::memcpy(host, gpu->readback, bytes);
+}
+
+}  // namespace dinara

@@ -14,15 +14,16 @@ namespace dinara {
 // `codes` (255 for a byte outside the alphabet, which flags the pair), and writes the pair's shape and
 // its scheduling key (shape class, strips, rows; sorted descending so the longest go first).
 __global__ void pack_pairs_kernel(const uint8_t *__restrict__ letters, const int64_t *__restrict__ offsets,
-                                  int64_t pairs, const uint8_t *__restrict__ codes, int bits,
+                                  int64_t first_pair, int64_t count, const uint8_t *__restrict__ codes, int bits,
                                   uint32_t *__restrict__ tape, PairShape *__restrict__ shapes,
                                   uint8_t *__restrict__ unknown) {
     __shared__ uint8_t code_of[256];
     code_of[threadIdx.x & 255] = codes[threadIdx.x & 255];
     __syncthreads();
-    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nth = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (warp >= pairs) return;
+    if (nth >= count) return;
+    const int64_t warp = first_pair + nth;
     const int per_word = 32 / bits;
     const int per_chunk = 4 * per_word;
     const uint32_t mask = bits == 8 ? 0xFFu : ((1u << bits) - 1u);
@@ -132,13 +133,14 @@ __global__ void schedule_keys_kernel(const PairShape *__restrict__ shapes, const
 }
 
 
-void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
-                const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown) {
-    if (pairs <= 0) return;
+void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t first_pair,
+                int64_t count, const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes,
+                uint8_t *unknown) {
+    if (count <= 0) return;
     const int threads = 256;
-    const int64_t blocks = (pairs * 32 + threads - 1) / threads;
+    const int64_t blocks = (count * 32 + threads - 1) / threads;
     pack_pairs_kernel<<<dim3(unsigned(blocks)), threads, 0, gpu->stream>>>(
-        letters_device, offsets_device, pairs, codes_device, bits, tape, shapes, unknown);
+        letters_device, offsets_device, first_pair, count, codes_device, bits, tape, shapes, unknown);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
 }
@@ -167,8 +169,7 @@ Schedule schedule(dinara_gpu *gpu, const PairShape *shapes, const uint32_t *list
     DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(space, scratch, keys, keys_out, order, order_out,
                                                           int(count), 0, 32, gpu->stream));
     unsigned int host_counts[kClasses];
-    DINARA_CUDA(cudaMemcpyAsync(host_counts, class_counts, sizeof host_counts, cudaMemcpyDeviceToHost, gpu->stream));
-    DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+    read_back(gpu, host_counts, class_counts, sizeof host_counts);
     for (int c = 0; c < kClasses; ++c) out.counts[c] = host_counts[c];
     out.order = order_out;
     return out;

@@ -5,11 +5,14 @@
 
 namespace dinara {
 
-// Packs pairs of the device ASCII tape (offsets: 2 pairs + 1 entries) into `tape`, each letter through
+// Packs pairs [first_pair, first_pair + count) of the device ASCII tape (offsets: 2 entries a pair and
+// one more, from the batch's first letter) into their places on the batch's `tape`, each letter through
 // `codes` (256 entries, 255 for a byte outside the alphabet), `bits` a letter; writes each pair's shape
-// and flags a pair holding an unknown byte.
-void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t pairs,
-                const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes, uint8_t *unknown);
+// and flags a pair holding an unknown byte. Packing a batch a range at a time gives the tape, shapes and
+// flags packing it whole gives.
+void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *offsets_device, int64_t first_pair,
+                int64_t count, const uint8_t *codes_device, int bits, uint32_t *tape, PairShape *shapes,
+                uint8_t *unknown);
 
 // A batch's sweep order: pairs by class, classes in descending order, then strips and rows descending.
 // Classes: the whole-matrix shape classes 0-4 (affine_shape_for with `record`); with `band` the proven

@@ -47,18 +47,24 @@ struct Request {
     bool done = false;
 };
 
-// Device bytes a context holds in its buffers.
+// Device bytes a context holds in its buffers and its partner's (the second stream a large batch's units
+// alternate onto).
 int64_t resident_bytes(dinara_gpu *g) {
     int64_t total = 0;
     g->for_each_buffer([&](const dinara::DeviceBuffer &b) { total += int64_t(b.bytes); });
+    if (g->partner) total += resident_bytes(g->partner);
     return total;
 }
 
-// Gives a context's device buffers back to the device's pool, ordered after its own work.
+// Gives a context's device buffers (and its partner's) back to the device's pool, each ordered after its
+// own stream's work.
 void release_buffers(dinara_gpu *g) {
     cudaSetDevice(g->device);
-    dinara::AllocationScope scope(g->stream);
-    g->for_each_buffer([](dinara::DeviceBuffer &b) { b.release(); });
+    {
+        dinara::AllocationScope scope(g->stream);
+        g->for_each_buffer([](dinara::DeviceBuffer &b) { b.release(); });
+    }
+    if (g->partner) release_buffers(g->partner);
 }
 
 // What a request's scores may hold on the device: its letters and their packed copy, per-pair shapes,

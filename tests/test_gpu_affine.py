@@ -254,3 +254,57 @@ def test_band_proofs_and_leftovers(da, oracle, scoring_name):
     found = da.alignments(refs, queries, scoring)
     assert [a.score for a in found] == list(expected_scores)
     assert [a.cigar for a in found] == expected_cigars
+
+
+@pytest.mark.parametrize("local", [False, True])
+def test_a_batch_in_units(da, oracle, local):
+    """200,000 short pairs run as several units on two streams (letters sent a piece at a time, results
+    moved out a unit at a time): scores, CIGARs, spans and statuses are the oracle's, from pageable
+    letters, from page-locked letters, and from a tape whose offsets start past its first letter."""
+    import torch
+
+    from dinara_align import shards, workloads
+
+    rng = np.random.default_rng(31)
+    lengths = rng.integers(10, 90, size=200_000)
+    tape = workloads.pairs_with_errors(rng, lengths, np.full(len(lengths), 0.05), workloads.HALF_QUARTERS)
+    scoring = da.Scoring.uniform(0, -4, -6, -2)
+    mode = da.Mode.local() if local else da.Mode.GLOBAL
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, tape, scoring, local, True)
+    rows = tape.offsets[1::2] - tape.offsets[0:-1:2]
+    columns = tape.offsets[2::2] - tape.offsets[1::2]
+    # Spans of a few pairs from batches small enough to run as one unit.
+    probes = np.r_[0:500, 99_800:100_300, 199_500:200_000]
+    probe_spans = np.concatenate([da.alignments_tape(shards.subset(tape, part), scoring, mode)[1]
+                                  for part in (probes[:500], probes[500:1000], probes[1000:])])
+
+    def check(batch):
+        np.testing.assert_array_equal(da.scores_tape(batch, scoring, mode), expected_scores)
+        scores, spans, offsets, data, codes = da.alignments_tape(batch, scoring, mode)
+        np.testing.assert_array_equal(scores, expected_scores)
+        assert not codes.any()
+        assert offsets[0] == 0 and offsets[-1] == len(data)
+        cigars = data.tobytes().decode()
+        assert [cigars[offsets[p]:offsets[p + 1]] for p in range(batch.pairs)] == expected_cigars
+        if local:
+            np.testing.assert_array_equal(spans[probes], probe_spans)
+        else:
+            np.testing.assert_array_equal(spans, np.stack([np.zeros_like(rows), rows, np.zeros_like(rows), columns], 1))
+
+    check(tape)
+    shift = 7
+    pinned = torch.empty(len(tape.letters) + shift, dtype=torch.uint8, pin_memory=True).numpy()
+    pinned[:shift] = ord("A")
+    pinned[shift:] = tape.letters
+    check(da.Tape(pinned, tape.offsets + shift))
+
+    # A letter outside the alphabet in pairs of three different units flags those pairs alone.
+    flagged = [5, 100_000, 199_999]
+    letters = tape.letters.copy()
+    for pair in flagged:
+        letters[tape.offsets[2 * pair + 1]] = ord("N")
+    marked = da.Tape(letters, tape.offsets)
+    _, statuses = da.scores_tape(marked, scoring, mode, statuses=True)
+    assert np.flatnonzero(statuses).tolist() == flagged
+    codes = da.alignments_tape(marked, scoring, mode)[4]
+    assert np.flatnonzero(codes).tolist() == flagged
