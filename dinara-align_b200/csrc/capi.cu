@@ -374,8 +374,9 @@ constexpr size_t kUploadPiece = size_t(32) << 20;
 // the tails of the sweeps) do.
 constexpr int64_t kMaxUnits = 8;
 constexpr int64_t kUnitPairs = 32768;
-// Units run on this many lanes (the context, then its partner).
-constexpr size_t kLanes = 2;
+// Units run on this many lanes: the context, its partner, the partner's partner, and so on.
+constexpr size_t kLanes = 4;
+constexpr size_t kMaxLanes = 4;
 
 // The caller's letters copied to the device a piece at a time on the context's upload stream. From
 // page-locked memory every piece is queued at once; from pageable memory a helper thread stages each
@@ -763,15 +764,17 @@ dinara_gpu *partner_of(dinara_gpu *gpu) {
     return gpu->partner;
 }
 
-// Runs body(ctx, k) for every unit k of a batch. With `lanes` 2 (and more than one unit), units alternate
-// between the context and its partner (a second stream with scratch buffers of its own), each driven by
-// its own thread, so that one unit's last pairs, copies and host waits overlap the next unit's sweeps.
+// Runs body(ctx, k) for every unit k of a batch. With more than one lane (and unit), units go round the
+// context and its chain of partners (each a stream with scratch buffers of its own), each lane driven by
+// its own thread, so that one unit's latency-bound phases (the last pairs of a sweep, the walk, copies
+// and host waits) overlap other units' sweeps.
 template <class F>
 void run_units(dinara_gpu *gpu, const StreamedBatch &streamed, size_t units, size_t lanes, UnitFinisher &finisher,
                F &&body) {
-    if (units < 2) lanes = 1;
-    dinara_gpu *contexts[2] = {gpu, lanes > 1 ? partner_of(gpu) : nullptr};
-    std::exception_ptr failures[2];
+    lanes = std::min({lanes, kMaxLanes, std::max<size_t>(units, 1)});
+    dinara_gpu *contexts[kMaxLanes] = {gpu};
+    for (size_t l = 1; l < lanes; ++l) contexts[l] = partner_of(contexts[l - 1]);
+    std::exception_ptr failures[kMaxLanes];
     auto lane = [&](size_t l) {
         try {
             dinara_gpu *ctx = contexts[l];
@@ -784,18 +787,18 @@ void run_units(dinara_gpu *gpu, const StreamedBatch &streamed, size_t units, siz
             finisher.fail(failures[l]);
         }
     };
-    std::thread helper;
-    if (lanes > 1) helper = std::thread(lane, size_t(1));
+    std::thread helpers[kMaxLanes];
+    for (size_t l = 1; l < lanes; ++l) helpers[l] = std::thread(lane, l);
     lane(0);
-    if (helper.joinable()) helper.join();
-    if (lanes > 1) {
-        // Later work on the context's stream comes after everything the partner queued.
+    for (size_t l = 1; l < lanes; ++l) helpers[l].join();
+    for (size_t l = 1; l < lanes; ++l) {
+        // Later work on the context's stream comes after everything the partners queued.
         cudaEvent_t joined = nullptr;
         if (cudaEventCreateWithFlags(&joined, cudaEventDisableTiming) == cudaSuccess) {
-            if (cudaEventRecord(joined, contexts[1]->stream) == cudaSuccess) cudaStreamWaitEvent(gpu->stream, joined, 0);
+            if (cudaEventRecord(joined, contexts[l]->stream) == cudaSuccess) cudaStreamWaitEvent(gpu->stream, joined, 0);
             cudaEventDestroy(joined);
         } else {
-            cudaStreamSynchronize(contexts[1]->stream);
+            cudaStreamSynchronize(contexts[l]->stream);
         }
     }
     for (std::exception_ptr &failure : failures)

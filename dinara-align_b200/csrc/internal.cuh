@@ -157,7 +157,7 @@ struct dinara_gpu {
     double predictor_slack = 0.0;
     dinara::PinnedBuffer pinned_in, pinned_out, pinned_small;
     // Page-locked stages a batch's results come back through, a unit of pairs at a time.
-    static constexpr int kStages = 4;
+    static constexpr int kStages = 6;
     dinara::PinnedBuffer stages[kStages];
     // Page-locked words the host reads totals and counts into between launches (a read into pageable
     // memory would wait on the driver's staging, which other threads' calls contend for).
@@ -167,8 +167,8 @@ struct dinara_gpu {
     double kernel_ms = 0.0, record_ms = 0.0;
     int64_t launches = 0;
     int64_t swept_cells = 0;  // cells the sweeps updated (bands, whole matrices, leftovers)
-    // A second stream with scratch buffers of its own, so that two units of a large batch run at once
-    // (capi.cu); set up at its first use.
+    // Another stream with scratch buffers of its own, so that units of a large batch run at once
+    // (capi.cu; a chain of them for more than two); set up at its first use.
     dinara_gpu *partner = nullptr;
     // The resident batch (capi.cu), if one is loaded.
     void *resident = nullptr;
