@@ -406,8 +406,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
     DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, plane_words, plane_offsets, int(pairs + 1), stream));
     int64_t plane_total = 0;
-    DINARA_CUDA(cudaMemcpyAsync(&plane_total, plane_offsets + pairs, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
-    DINARA_CUDA(cudaStreamSynchronize(stream));
+    read_back(gpu, &plane_total, plane_offsets + pairs, sizeof(int64_t));
     uint64_t *planes = gpu->planes.ensure<uint64_t>(size_t(plane_total) + 4);
     planes_kernel<<<warp_blocks, threads, 0, stream>>>(letters, info, pairs, plane_offsets, planes);
     gpu->launches += 1;
@@ -435,8 +434,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     uint32_t *keys_sorted = gpu->keys_sorted.ensure<uint32_t>(size_t(pairs));
     uint32_t *order_sorted = gpu->order_sorted.ensure<uint32_t>(size_t(pairs));
     unsigned int host_counts[2 + kBandShapes];
-    DINARA_CUDA(cudaMemcpyAsync(host_counts, counters, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
-    DINARA_CUDA(cudaStreamSynchronize(stream));
+    read_back(gpu, host_counts, counters, sizeof(unsigned int));
     int64_t count = host_counts[0];
     int64_t launches = 0;
     float kernel_ms = 0.f;
@@ -462,9 +460,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         space = gpu->sort_scratch.ensure<uint8_t>(sort_bytes + 256);
         DINARA_CUDA(cub::DeviceRadixSort::SortPairsDescending(space, sort_bytes, keys, keys_sorted, pending,
                                                               order_sorted, int(count), 0, 32, stream));
-        DINARA_CUDA(cudaMemcpyAsync(host_counts, counters, (2 + kBandShapes) * sizeof(unsigned int),
-                                    cudaMemcpyDeviceToHost, stream));
-        DINARA_CUDA(cudaStreamSynchronize(stream));
+        read_back(gpu, host_counts, counters, (2 + kBandShapes) * sizeof(unsigned int));
         DINARA_CUDA(cudaEventRecord(gpu->start, stream));
         // Each shape's launch on a side stream, all forked from and joined back to the context's stream:
         // a launch lasts as long as its longest pair, so running the shapes at once overlaps those tails.
@@ -517,8 +513,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         DINARA_CUDA(cudaMemcpyAsync(counters, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToDevice, stream));
-        DINARA_CUDA(cudaMemcpyAsync(host_counts, counters + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
-        DINARA_CUDA(cudaStreamSynchronize(stream));
+        read_back(gpu, host_counts, counters + 1, sizeof(unsigned int));
         float ms = 0.f;
         DINARA_CUDA(cudaEventElapsedTime(&ms, gpu->start, gpu->stop));
         kernel_ms += ms;
@@ -538,8 +533,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         gpu->launches += 1;
         DINARA_CUDA(cudaGetLastError());
         unsigned long long host[5] = {0, 0, 0, 0, 0};
-        DINARA_CUDA(cudaMemcpyAsync(host, swept, sizeof(host), cudaMemcpyDeviceToHost, stream));
-        DINARA_CUDA(cudaStreamSynchronize(stream));
+        read_back(gpu, host, swept, sizeof(host));
         report->rounds = launches;
         report->words_swept = int64_t(host[0]);
         report->pair_rounds = int64_t(host[1]);

@@ -82,3 +82,42 @@ def test_bytes_and_refusals(da, oracle):
         da.distances(["ACGT"], ["ACGT"], mode=da.Mode.INFIX)
     with pytest.raises(ValueError):
         da.distances(["ACGT"], ["ACGT"], band=da.Band.around(3))
+
+
+def test_a_large_batch(da, oracle):
+    """100,000 pairs: distances are the oracle's from plain and from given first thresholds, from pageable
+    and page-locked letters, and from a tape whose offsets start past its first letter; refused pairs far
+    apart are refused alone, and the report's tallies cover every pair."""
+    import torch
+
+    from dinara_align import workloads
+
+    rng = np.random.default_rng(41)
+    lengths = rng.integers(20, 400, size=100_000)
+    tape = workloads.pairs_with_errors(rng, lengths, rng.uniform(0.0, 0.15, size=len(lengths)),
+                                       workloads.HALF_QUARTERS)
+    expected = _oracle_distances(oracle, tape)
+    got, report = da.distances_tape(tape, report=True)
+    np.testing.assert_array_equal(got, expected)
+    rows = tape.offsets[1::2] - tape.offsets[0:-1:2]
+    columns = tape.offsets[2::2] - tape.offsets[1::2]
+    assert report["full_cells"] == int((rows * columns).sum())
+    assert report["pair_rounds"] >= tape.pairs and report["words_swept"] > 0
+    given = np.full(tape.pairs, 1, dtype=np.int64)
+    np.testing.assert_array_equal(
+        da.distances_tape(tape, policy=da._native.BAND_GIVEN, start_thresholds=given), expected)
+
+    shift = 5
+    pinned = torch.empty(len(tape.letters) + shift, dtype=torch.uint8, pin_memory=True).numpy()
+    pinned[:shift] = ord("C")
+    pinned[shift:] = tape.letters
+    np.testing.assert_array_equal(da.distances_tape(da.Tape(pinned, tape.offsets + shift)), expected)
+
+    refused = [3, 50_000, 99_999]
+    letters = tape.letters.copy()
+    for pair in refused:
+        letters[tape.offsets[2 * pair]] = 0xFE
+    got = da.distances_tape(da.Tape(letters, tape.offsets))
+    assert (got[refused] == -1).all()
+    keep = np.setdiff1d(np.arange(tape.pairs), refused)
+    np.testing.assert_array_equal(got[keep], expected[keep])
