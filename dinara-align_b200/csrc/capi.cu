@@ -10,9 +10,11 @@
 #include <mutex>
 #include <cstdio>
 #include <cstdlib>
+#include <initializer_list>
 #include <new>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include <sys/mman.h>
@@ -805,7 +807,9 @@ void run_units(dinara_gpu *gpu, const StreamedBatch &streamed, size_t units, siz
         if (failure) std::rethrow_exception(failure);
 }
 
-// The resident batch: packed letters kept on the device between calls.
+// The resident batch: packed letters kept on the device between calls. It owns its buffers (taken over
+// from the context once loaded) and its results, so the context's other calls, which reuse the context's
+// buffers, leave it as it was.
 struct Resident {
     int64_t pairs = 0;
     bool scoring = false;
@@ -818,9 +822,17 @@ struct Resident {
     int last = 0;  // 1 scores, 2 distances
     // The cuts of a recording pass (global, then local), planned at the first one.
     std::vector<std::pair<int64_t, int64_t>> plans[2];
+    dinara::DeviceBuffer held_letters, held_offsets, held_tape, held_shapes, held_flags, results;
 };
 
-void free_resident(void *pointer) { delete static_cast<Resident *>(pointer); }
+// Frees a resident batch, its buffers ordered on the calling scope's allocation stream.
+void free_resident(void *pointer) {
+    Resident *r = static_cast<Resident *>(pointer);
+    for (dinara::DeviceBuffer *buffer :
+         {&r->held_letters, &r->held_offsets, &r->held_tape, &r->held_shapes, &r->held_flags, &r->results})
+        buffer->release();
+    delete r;
+}
 
 Resident &resident_of(dinara_gpu *gpu) {
     if (!gpu || !gpu->resident) throw Failure(DINARA_INVALID_MODE, "no resident batch loaded");
@@ -1270,6 +1282,9 @@ int64_t dinara_gpu_resident_load(dinara_gpu *gpu, int64_t pairs, const char *let
             r->scoring = true;
             r->checked = check_scoring(scoring, false);
             r->packed = pack_batch(gpu, pairs, letters, offsets, r->checked.codes, r->checked.bits);
+            std::swap(r->held_tape, gpu->tape);
+            std::swap(r->held_shapes, gpu->shapes);
+            std::swap(r->held_flags, gpu->flags);
         } else {
             const int64_t total = offsets[2 * pairs] - offsets[0];
             uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
@@ -1279,6 +1294,8 @@ int64_t dinara_gpu_resident_load(dinara_gpu *gpu, int64_t pairs, const char *let
             r->letters_device = letters_device;
             r->offsets_device = offsets_device;
         }
+        std::swap(r->held_letters, gpu->letters);
+        std::swap(r->held_offsets, gpu->offsets);
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         return 0;
     });
@@ -1295,7 +1312,7 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         Timer timer(gpu);
         AffineBatch batch{r.pairs, r.checked.bits, local, r.packed.tape, r.packed.shapes, r.packed.max_rows,
                           r.packed.max_columns};
-        int32_t *scores_device = gpu->scores.ensure<int32_t>(size_t(r.pairs));
+        int32_t *scores_device = r.results.ensure<int32_t>(size_t(r.pairs));
         const int64_t *offsets = r.offsets.data();
         if (!cigars) {
             affine_scores(gpu, batch, r.checked.table, scores_device, 0, r.pairs);
@@ -1346,7 +1363,7 @@ int64_t dinara_gpu_resident_distances(dinara_gpu *gpu, const dinara_band_plan *p
         double predict_ms = 0.0;
         if (policy == DINARA_BAND_LEARNED)
             starts = timed_predictions(gpu, r.pairs, r.letters_device, r.offsets_device, &predict_ms);
-        int64_t *results_device = gpu->scores.ensure<int64_t>(size_t(r.pairs));
+        int64_t *results_device = r.results.ensure<int64_t>(size_t(r.pairs));
         band_doubling(gpu, r.pairs, r.letters_device, r.offsets_device, starts, plan ? plan->default_start : 0,
                       results_device, report);
         if (report) report->predict_ms = predict_ms;
@@ -1362,9 +1379,9 @@ int64_t dinara_gpu_resident_fetch(dinara_gpu *gpu, int32_t *scores, int64_t *dis
     return guard(gpu, [&]() -> int64_t {
         Resident &r = resident_of(gpu);
         if (r.pairs == 0) return 0;
-        if (r.last == 1 && scores) to_host(gpu, scores, gpu->scores.as<int32_t>(), size_t(r.pairs) * sizeof(int32_t));
+        if (r.last == 1 && scores) to_host(gpu, scores, r.results.as<int32_t>(), size_t(r.pairs) * sizeof(int32_t));
         if (r.last == 2 && distances)
-            to_host(gpu, distances, gpu->scores.as<int64_t>(), size_t(r.pairs) * sizeof(int64_t));
+            to_host(gpu, distances, r.results.as<int64_t>(), size_t(r.pairs) * sizeof(int64_t));
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         return 0;
     });

@@ -110,6 +110,15 @@ def lib() -> ctypes.CDLL:
         handle.dinara_gpu_distances_tape.restype = i64
         handle.dinara_gpu_distances_tape.argtypes = [vp, i64, vp, i64p, ctypes.POINTER(CBandPlan), i64p,
                                                      ctypes.POINTER(CBandReport)]
+        handle.dinara_gpu_resident_load.restype = i64
+        handle.dinara_gpu_resident_load.argtypes = [vp, i64, vp, i64p, ctypes.POINTER(CScoring)]
+        handle.dinara_gpu_resident_align.restype = i64
+        handle.dinara_gpu_resident_align.argtypes = [vp, ctypes.POINTER(CMode), i64, i64, vp]
+        handle.dinara_gpu_resident_distances.restype = i64
+        handle.dinara_gpu_resident_distances.argtypes = [vp, ctypes.POINTER(CBandPlan), ctypes.POINTER(CBandReport),
+                                                         vp]
+        handle.dinara_gpu_resident_fetch.restype = i64
+        handle.dinara_gpu_resident_fetch.argtypes = [vp, i32p, i64p]
         _lib = handle
         return _lib
 

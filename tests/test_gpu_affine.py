@@ -308,3 +308,44 @@ def test_a_batch_in_units(da, oracle, local):
     assert np.flatnonzero(statuses).tolist() == flagged
     codes = da.alignments_tape(marked, scoring, mode)[4]
     assert np.flatnonzero(codes).tolist() == flagged
+
+
+def test_resident_batch_kept_across_other_calls(da):
+    """A resident batch (letters packed once and kept on the device) keeps its letters and its results while
+    the same context aligns other batches, large ones run in units included."""
+    import ctypes
+
+    from dinara_align import _native as native, workloads
+
+    lib = native.lib()
+    handle = native.context(0)
+    scoring = da.Scoring.uniform(0, -4, -6, -2)
+    struct, _table, _alphabet = scoring._struct()
+    mode = da.Mode.GLOBAL._struct()
+    kept = workloads.affine_global(3000, seed=61)
+    expected = da.scores_tape(kept, scoring)
+    other = workloads.affine_global(80_000, seed=62)
+
+    native.check(lib.dinara_gpu_resident_load(handle, kept.pairs, kept.letters.ctypes.data,
+                                              native.pointer(kept.offsets, ctypes.c_int64), ctypes.byref(struct)),
+                 handle)
+    got = np.zeros(kept.pairs, dtype=np.int32)
+    for cigars in (1, 0):
+        native.check(lib.dinara_gpu_resident_align(handle, ctypes.byref(mode), cigars, 1, None), handle)
+        da.alignments_tape(other, scoring)  # between the run and its fetch
+        got[:] = 0
+        native.check(lib.dinara_gpu_resident_fetch(handle, native.pointer(got, ctypes.c_int32), None), handle)
+        np.testing.assert_array_equal(got, expected)
+        da.scores_tape(other, scoring)  # between two runs
+
+    unit = workloads.unit_cost_uniform(2000, seed=63)
+    expected_distances = da.distances_tape(unit)
+    native.check(lib.dinara_gpu_resident_load(handle, unit.pairs, unit.letters.ctypes.data,
+                                              native.pointer(unit.offsets, ctypes.c_int64), None), handle)
+    plan = native.CBandPlan(native.BAND_PLAIN, None, 0)
+    report = native.CBandReport()
+    native.check(lib.dinara_gpu_resident_distances(handle, ctypes.byref(plan), ctypes.byref(report), None), handle)
+    da.distances_tape(workloads.unit_cost_uniform(5000, seed=64))
+    distances = np.zeros(unit.pairs, dtype=np.int64)
+    native.check(lib.dinara_gpu_resident_fetch(handle, None, native.pointer(distances, ctypes.c_int64)), handle)
+    np.testing.assert_array_equal(distances, expected_distances)
