@@ -164,21 +164,22 @@ void to_host(dinara_gpu *gpu, void *host, const void *device, size_t bytes) {
     DINARA_CUDA(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, gpu->stream));
 }
 
-// A host copy shared by four threads.
-void parallel_copy(uint8_t *to, const uint8_t *from, size_t bytes) {
-    constexpr int kThreads = 4;
-    if (bytes < (size_t(1) << 20)) {
+// A host copy shared by `threads` threads (at most 8).
+void parallel_copy(uint8_t *to, const uint8_t *from, size_t bytes, int threads = 4) {
+    constexpr int kMostThreads = 8;
+    threads = std::max(1, std::min(threads, kMostThreads));
+    if (bytes < (size_t(1) << 20) || threads == 1) {
         std::memcpy(to, from, bytes);
         return;
     }
-    const size_t part = (bytes + kThreads - 1) / kThreads;
-    std::thread helpers[kThreads - 1];
-    for (int t = 1; t < kThreads; ++t) {
+    const size_t part = (bytes + threads - 1) / threads;
+    std::thread helpers[kMostThreads - 1];
+    for (int t = 1; t < threads; ++t) {
         const size_t begin = std::min(bytes, size_t(t) * part), end = std::min(bytes, begin + part);
         helpers[t - 1] = std::thread([=] { std::memcpy(to + begin, from + begin, end - begin); });
     }
     std::memcpy(to, from, std::min(bytes, part));
-    for (auto &helper : helpers) helper.join();
+    for (int t = 1; t < threads; ++t) helpers[t - 1].join();
 }
 
 // Copies `bytes` of device memory to host memory and waits for them. Large copies into pageable memory
@@ -449,7 +450,8 @@ class LetterUpload {
                 // This half's previous copy has left it.
                 if (piece >= 2) DINARA_CUDA(cudaEventSynchronize(events_[piece - 2]));
                 const size_t at = piece * kUploadPiece;
-                parallel_copy(buffer, host_ + at, std::min(kUploadPiece, bytes_ - at));
+                // Eight threads: from pageable memory this copy, not the bus, sets the upload's pace.
+                parallel_copy(buffer, host_ + at, std::min(kUploadPiece, bytes_ - at), 8);
                 queue(piece, buffer);
                 {
                     std::lock_guard<std::mutex> lock(mutex_);
