@@ -225,11 +225,11 @@ struct Packed {
     uint32_t max_rows = 0, max_columns = 0;
 };
 
-// Runs work(begin, end) over [0, count) on four threads when the count is large, else on this one; each
+// Runs work(begin, end) over [0, count) on eight threads when the count is large, else on this one; each
 // share is contiguous and the shares do not overlap.
 template <class F>
 void split_work(int64_t count, F &&work) {
-    constexpr int kThreads = 4;
+    constexpr int kThreads = 8;
     if (count < 65536) {
         work(int64_t(0), count);
         return;
@@ -383,7 +383,7 @@ constexpr size_t kMaxLanes = 4;
 
 // The caller's letters copied to the device a piece at a time on the context's upload stream. From
 // page-locked memory every piece is queued at once; from pageable memory a helper thread stages each
-// piece through page-locked memory (a four-thread copy) and queues it.
+// piece through page-locked memory (an eight-thread copy) and queues it.
 class LetterUpload {
   public:
     LetterUpload(dinara_gpu *gpu, uint8_t *device, const uint8_t *host, size_t bytes)
