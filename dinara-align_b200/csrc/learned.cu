@@ -122,8 +122,14 @@ __device__ __forceinline__ int code_of(uint32_t byte) {
     return dna ? int(((byte >> 1) & 3u) ^ ((byte >> 2) & 1u)) : -1;
 }
 
-// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints), `sign` +1 or -1; a 4-mer holding
-// another letter is skipped.
+// A 4-mer's count index: its letters' 2-bit codes, the first letter in the lowest bits.
+// `reversed_kmer` maps between that and the features' order, the first letter in the highest bits.
+__device__ __forceinline__ uint32_t reversed_kmer(uint32_t k) {
+    return ((k & 3u) << 6) | (((k >> 2) & 3u) << 4) | (((k >> 4) & 3u) << 2) | ((k >> 6) & 3u);
+}
+
+// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints, indexed with the first letter in
+// the lowest bits), `sign` +1 or -1; a 4-mer holding another letter is skipped.
 __device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, int *counts) {
     // The warp reads the sequence 512 letters at a time, lane i the 4-mers starting at the 16 letters from
     // 16i, through six aligned words that hold those letters and the three after them (a word may reach
@@ -144,12 +150,35 @@ __device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, i
         uint32_t a[5];
 #pragma unroll
         for (int i = 0; i < 5; ++i) a[i] = __funnelshift_r(w[i], w[i + 1], shift);
+        if (first + 19 <= length) {
+            // The lane's 19 letters, four a word at once: each byte's 2-bit code, the letters rebuilt from
+            // the codes (A, C, G, T by a byte permute) to check that every byte was one of the four, and
+            // the codes packed two bits a letter, the first letter lowest.
+            bool valid = true;
+            uint64_t packed = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const uint32_t c = ((a[q] >> 1) & 0x03030303u) ^ ((a[q] >> 2) & 0x01010101u);
+                const uint32_t t = c | (c >> 4);
+                const uint32_t rebuilt = __byte_perm(0x54474341u, 0u, (t & 0xFFu) | ((t >> 8) & 0xFF00u));
+                const uint32_t used = q < 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;  // 16 + 3 letters
+                valid = valid && ((rebuilt ^ a[q]) & used) == 0u;
+                const uint32_t x = c | (c >> 6);
+                packed |= uint64_t((x & 0xFu) | ((x >> 12) & 0xF0u)) << (8 * q);
+            }
+            if (valid) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) atomicAdd(&counts[uint32_t(packed >> (2 * j)) & 0xFFu], sign);
+                continue;
+            }
+        }
+        // Near the sequence's end or another letter in reach: letter by letter.
         uint32_t kmer = 0;
         int run = 0;
 #pragma unroll
         for (int j = 0; j < 19; ++j) {
             const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
-            kmer = ((kmer << 2) | uint32_t(c & 3)) & 0xFFu;
+            kmer = (kmer >> 2) | (uint32_t(c & 3) << 6);
             run = c < 0 ? 0 : run + 1;
             if (j >= 3 && run >= 4) atomicAdd(&counts[kmer], sign);
         }
@@ -165,7 +194,7 @@ __device__ void features_of(const int *counts, int64_t reference, int64_t query,
     const float mean = 0.5f * float(reference + query);
     const float scale = 32.0f / (mean > 1.0f ? mean : 1.0f);
     for (int k = lane; k < 256; k += 32) {
-        const float difference = float(counts[k]);
+        const float difference = float(counts[reversed_kmer(uint32_t(k))]);
         out[int64_t(k) * stride] = difference * difference * scale;
     }
     if (lane == 0) {
