@@ -323,7 +323,7 @@ int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const uint32_t *
                                  const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, void *stream);
 
 /* The device's measured integer issue rate (no reference counterpart: the roofline the sweeps are
- * judged against): `kind` 0 DPX add-and-max, 1 min/max with an add (counted as two), 2 three-input add,
+ * measured against): `kind` 0 DPX add-and-max, 1 min/max with an add (counted as two), 2 three-input add,
  * 3 DPX add-and-max on 16-bit pairs, 4 three-way max, 5 three-way max on 16-bit pairs, 6 byte permute,
  * 7 max alone, 8 16-bit pair compare to a mask, 9 16-bit pair max with predicates, 10 kind 3 floored at
  * zero, 11 16-bit pair subtraction; instructions per second into *instructions_per_second, from independent chains on every SM. */
