@@ -46,6 +46,7 @@ struct WalkArgs {
     const int64_t *slot_offsets;  // per pair: its CIGAR slot, 2 (rows + columns) + 1 bytes
     char *slots;
     int64_t *lengths;             // per pair: the CIGAR's bytes
+    uint8_t *failed;              // per pair of the batch: set to kWalkFailed when a path leaves its band
     int64_t *spans;               // per pair: first row, last row, first column, last column
     int64_t first_pair, count;
     int bits;
@@ -113,8 +114,12 @@ __global__ void walk_kernel(WalkArgs a) {
                 // The band's layout: place o = column - row - low, a lane of 16 places a block of rows.
                 const int place = column - row - low;
                 // The proof keeps every optimal path inside the band; a place outside it would read
-                // another pair's decisions, so the walk stops there instead.
-                if (place < 0 || place >= kBandWidth) break;
+                // another pair's decisions, so the walk stops there instead and flags the pair, whose
+                // CIGAR the host then reports as a device failure rather than a result.
+                if (place < 0 || place >= kBandWidth) {
+                    if (a.failed) a.failed[pair] = kWalkFailed;
+                    break;
+                }
                 slot_in = place % 16;
                 at = base + int64_t(place / 16) * rows_pad + (row - 1);
             } else {
@@ -212,23 +217,29 @@ __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t 
     layouts[k] = layout;
 }
 
-// Cells a batch's sweeps update: 64 a row for a banded pair, the whole matrix for the rest and again for
-// each leftover of the band.
+// Cells a batch's sweeps update: 64 a row for a banded pair (out[0]), the whole matrix for the rest and
+// again for each leftover of the band (out[1]).
 __global__ void swept_cells_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count, bool band,
                                    const uint32_t *__restrict__ leftovers, int64_t left,
                                    unsigned long long *__restrict__ out) {
-    unsigned long long sum = 0;
+    unsigned long long banded = 0, whole = 0;
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < count + left;
          k += int64_t(gridDim.x) * blockDim.x) {
         const PairShape sh = k < count ? shapes[first + k] : shapes[leftovers[k - count]];
         if (k < count && band && band_eligible(sh.rows, sh.columns))
-            sum += (unsigned long long)sh.rows * kBandWidth;
+            banded += (unsigned long long)sh.rows * kBandWidth;
         else
-            sum += (unsigned long long)sh.rows * sh.columns;
+            whole += (unsigned long long)sh.rows * sh.columns;
     }
 #pragma unroll
-    for (int span = 16; span > 0; span >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, span);
-    if ((threadIdx.x & 31) == 0) atomicAdd(out, sum);
+    for (int span = 16; span > 0; span >>= 1) {
+        banded += __shfl_xor_sync(0xffffffffu, banded, span);
+        whole += __shfl_xor_sync(0xffffffffu, whole, span);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, banded);
+        atomicAdd(out + 1, whole);
+    }
 }
 
 // The whole-matrix words of each leftover pair of the band.
@@ -440,8 +451,10 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
         }
         args.begin = uint32_t(b.begin[bucket]);
         args.end = uint32_t(b.end[bucket]);
+        ClockSpan clock(gpu, kClassWhole, gpu->stream);
         fn<<<dim3(unsigned(blocks)), kBlock, 0, gpu->stream>>>(args, targs, table32);
         DINARA_CUDA(cudaGetLastError());
+        clock.stop();
         gpu->launches += 1;
     }
 }
@@ -539,13 +552,15 @@ void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_
                  const uint32_t *leftovers, int64_t left) {
     if (!gpu->timing) return;
     unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(16) + 12);
-    DINARA_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long), gpu->stream));
+    DINARA_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), gpu->stream));
     swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, out);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
-    unsigned long long host = 0;
-    read_back(gpu, &host, out, sizeof host);
-    gpu->swept_cells += int64_t(host);
+    unsigned long long host[2] = {0, 0};
+    read_back(gpu, host, out, sizeof host);
+    gpu->swept_cells += int64_t(host[0] + host[1]);
+    gpu->band_cells += int64_t(host[0]);
+    gpu->whole_cells += int64_t(host[1]);
 }
 
 }  // namespace
@@ -725,6 +740,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.slot_offsets = slot_offsets;
     w.slots = slots;
     w.lengths = lengths;
+    w.failed = batch.flags;
     w.spans = spans;
     w.first_pair = first_pair;
     w.count = count;
@@ -732,11 +748,13 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.local = batch.local;
     w.eqx = eqx;
     w.uniform = uniform;
+    ClockSpan walk_clock(gpu, kClassWalk, gpu->stream);
     if (batch.bits == 8)
         walk_kernel<8><<<blocks, threads, 0, gpu->stream>>>(w);
     else
         walk_kernel<2><<<blocks, threads, 0, gpu->stream>>>(w);
     DINARA_CUDA(cudaGetLastError());
+    walk_clock.stop();
     gpu->launches += 1;
     timer.stop();
     tally_swept(gpu, batch.shapes, first_pair, count, band, leftovers, left);

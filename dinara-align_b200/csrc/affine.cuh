@@ -44,7 +44,13 @@ struct AffineBatch {
     const uint32_t *tape;
     const PairShape *shapes;
     uint32_t max_rows, max_columns;
+    // Per-pair flags (the packing's unknown-letter flags): a walk that finds its path leaving the proven
+    // band sets its pair's to kWalkFailed, which the host reports as DINARA_DEVICE_FAILURE. May be null.
+    uint8_t *flags = nullptr;
 };
+
+// The flag value a failed walk leaves (1 is a letter outside the alphabet).
+constexpr uint8_t kWalkFailed = 2;
 
 // Whether a batch's global pairs may be swept over proven bands (a 2-bit alphabet, the 16-bit table and
 // a bound that holds for its table): pairs the band does not prove are swept whole.

@@ -474,8 +474,10 @@ void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool 
     int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
     const int64_t needed = (batch.count + pairs_per_block - 1) / pairs_per_block;
     if (blocks > needed) blocks = needed;
+    ClockSpan clock(gpu, record ? kClassBandRecord : kClassBandScore, gpu->stream);
     fn<<<unsigned(blocks), kBlock, 0, gpu->stream>>>(batch);
     DINARA_CUDA(cudaGetLastError());
+    clock.stop();
     gpu->launches += 1;
 }
 

@@ -312,8 +312,8 @@ int64_t record_words(int64_t rows, int64_t columns, bool uniform, bool band) {
     return (columns + lanes * 16 - 1) / (lanes * 16) * lanes * (((rows + 2) | 3) + 1);
 }
 
-// Per-pair statuses of pairs [first, first + count): scores that could pass 2^28 (-3), then a letter
-// outside the alphabet (-1); `unknown_host` holds the range's flags.
+// Per-pair statuses of pairs [first, first + count): scores that could pass 2^28 (-3), then a walk that
+// left its band (-8), then a letter outside the alphabet (-1); `unknown_host` holds the range's flags.
 void statuses_of(const CheckedScoring &checked, bool local, int64_t first, int64_t count, const int64_t *offsets,
                  const uint8_t *unknown_host, int64_t *statuses) {
     if (!statuses) return;
@@ -325,6 +325,8 @@ void statuses_of(const CheckedScoring &checked, bool local, int64_t first, int64
             int64_t status = 0;
             if (checked.reach_opening + 2 * (letters + 2) * checked.reach_step >= (int64_t(1) << 28))
                 status = DINARA_INVALID_COSTS;
+            else if (unknown_host[p - first] == kWalkFailed)
+                status = DINARA_DEVICE_FAILURE;  // a walk whose path left its proven band
             else if (unknown_host[p - first])
                 status = DINARA_UNSUPPORTED_SYMBOLS;
             statuses[p] = status;
@@ -852,6 +854,8 @@ struct Timer {
         gpu->kernel_ms = gpu->record_ms = 0.0;
         gpu->launches = 0;
         gpu->swept_cells = 0;
+        gpu->band_cells = gpu->whole_cells = 0;
+        gpu->clock_used = 0;
     }
     void finish(dinara_timing *timing, int64_t cells) {
         DINARA_CUDA(cudaEventRecord(end, gpu->stream));
@@ -864,6 +868,18 @@ struct Timer {
             timing->record_ms = gpu->record_ms;
             timing->launches = gpu->launches;
             timing->cells = gpu->swept_cells > 0 ? gpu->swept_cells : cells;
+            for (int k = 0; k < 8; ++k) {
+                timing->class_ms[k] = 0.0;
+                timing->class_launches[k] = 0;
+            }
+            timing->band_cells = gpu->band_cells;
+            timing->whole_cells = gpu->whole_cells;
+            for (int slot = 0; slot < gpu->clock_used; ++slot) {
+                float span = 0.f;
+                DINARA_CUDA(cudaEventElapsedTime(&span, gpu->clock_events[2 * slot], gpu->clock_events[2 * slot + 1]));
+                timing->class_ms[gpu->clock_class[slot]] += span;
+                timing->class_launches[gpu->clock_class[slot]] += 1;
+            }
         }
     }
     ~Timer() {
@@ -877,7 +893,9 @@ struct Timer {
 const int64_t *timed_predictions(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
                                  double *ms) {
     DINARA_CUDA(cudaEventRecord(gpu->start, gpu->stream));
+    ClockSpan clock(gpu, kClassPredict, gpu->stream);
     const int64_t *starts = predict_thresholds(gpu, pairs, letters, offsets);
+    clock.stop();
     DINARA_CUDA(cudaEventRecord(gpu->stop, gpu->stream));
     DINARA_CUDA(cudaEventSynchronize(gpu->stop));
     float elapsed = 0.f;
@@ -943,6 +961,8 @@ void dinara_gpu_free(dinara_gpu *gpu) {
     if (gpu->start) cudaEventDestroy(gpu->start);
     if (gpu->stop) cudaEventDestroy(gpu->stop);
     if (gpu->fork) cudaEventDestroy(gpu->fork);
+    for (cudaEvent_t event : gpu->clock_events)
+        if (event) cudaEventDestroy(event);
     for (int k = 0; k < dinara_gpu::kSideStreams; ++k) {
         if (gpu->side[k]) cudaStreamDestroy(gpu->side[k]);
         if (gpu->joins[k]) cudaEventDestroy(gpu->joins[k]);
@@ -1039,7 +1059,8 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
         StreamedBatch streamed;
         start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
         const Packed &packed = streamed.packed;
-        AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
+        AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns,
+                          packed.unknown};
         int32_t *scores_device = streamed.scores;
         // Units whose recorded decisions stay within a budget of device memory.
         const bool uniform = !checked.table.packed16 || checked.bits == 8;
@@ -1313,7 +1334,7 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         DINARA_CUDA(cudaSetDevice(gpu->device));
         Timer timer(gpu);
         AffineBatch batch{r.pairs, r.checked.bits, local, r.packed.tape, r.packed.shapes, r.packed.max_rows,
-                          r.packed.max_columns};
+                          r.packed.max_columns, r.packed.unknown};
         int32_t *scores_device = r.results.ensure<int32_t>(size_t(r.pairs));
         const int64_t *offsets = r.offsets.data();
         if (!cigars) {

@@ -462,6 +462,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
                                                               order_sorted, int(count), 0, 32, stream));
         read_back(gpu, host_counts, counters, (2 + kBandShapes) * sizeof(unsigned int));
         DINARA_CUDA(cudaEventRecord(gpu->start, stream));
+        ClockSpan clock(gpu, kClassUnitBand, stream);
         // Each shape's launch on a side stream, all forked from and joined back to the context's stream:
         // a launch lasts as long as its longest pair, so running the shapes at once overlaps those tails.
         DINARA_CUDA(cudaEventRecord(gpu->fork, stream));
@@ -507,6 +508,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
             DINARA_CUDA(cudaStreamWaitEvent(stream, gpu->joins[side], 0));
         }
         DINARA_CUDA(cudaEventRecord(gpu->stop, stream));
+        clock.stop();
         DINARA_CUDA(cudaMemsetAsync(counters + 1, 0, sizeof(unsigned int), stream));
         settle_kernel<<<blocks, threads, 0, stream>>>(info, order_sorted, counters, thresholds, cheapest, banded,
                                                       results, rounds, latency, next, counters + 1);

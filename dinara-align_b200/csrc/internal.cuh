@@ -165,8 +165,15 @@ struct dinara_gpu {
     // Device timing of the sweep kernels, accumulated while `timing` is set.
     bool timing = false;
     double kernel_ms = 0.0, record_ms = 0.0;
+    // While `timing` is set, a pair of events around each launch of a kernel class (dinara::ClockSpan),
+    // summed per class when the call's timer finishes.
+    static constexpr int kClockSpans = 512;
+    cudaEvent_t clock_events[2 * kClockSpans] = {nullptr};
+    int clock_class[kClockSpans] = {0};
+    int clock_used = 0;
     int64_t launches = 0;
     int64_t swept_cells = 0;  // cells the sweeps updated (bands, whole matrices, leftovers)
+    int64_t band_cells = 0, whole_cells = 0;  // the same, the proven bands' and the whole matrices' apart
     // Another stream with scratch buffers of its own, so that units of a large batch run at once
     // (capi.cu; a chain of them for more than two); set up at its first use.
     dinara_gpu *partner = nullptr;
@@ -189,6 +196,41 @@ struct dinara_gpu {
 };
 
 namespace dinara {
+
+// Kernel classes a timed call reports apart (dinara_timing.class_ms).
+enum KernelClass {
+    kClassBandRecord = 0,  // the proven-band sweep, recording decisions
+    kClassBandScore = 1,   // the proven-band sweep, scores only
+    kClassWhole = 2,       // whole-matrix sweeps (strips, 16-bit pairs, a block a pair)
+    kClassWalk = 3,        // the walk back from recorded decisions
+    kClassUnitBand = 4,    // unit-cost band rounds (every window shape of a round, first launch to last)
+    kClassPredict = 5,     // the learned band's sketch and prediction
+    kClassTrace = 6,       // unit-cost CIGARs: the recording band and its trace
+    kClassOther = 7,
+};
+
+// Device time of one launch (or one round of launches) on `stream`, kept while the context times.
+struct ClockSpan {
+    dinara_gpu *gpu;
+    cudaStream_t stream;
+    int slot = -1;
+    ClockSpan(dinara_gpu *g, int cls, cudaStream_t s) : gpu(g), stream(s) {
+        if (!gpu->timing || gpu->clock_used >= dinara_gpu::kClockSpans) return;
+        slot = gpu->clock_used++;
+        for (int k = 0; k < 2; ++k)
+            if (!gpu->clock_events[2 * slot + k]) DINARA_CUDA(cudaEventCreate(&gpu->clock_events[2 * slot + k]));
+        gpu->clock_class[slot] = cls;
+        DINARA_CUDA(cudaEventRecord(gpu->clock_events[2 * slot], stream));
+    }
+    void stop() {
+        if (slot < 0) return;
+        DINARA_CUDA(cudaEventRecord(gpu->clock_events[2 * slot + 1], stream));
+        slot = -1;
+    }
+    ~ClockSpan() {
+        if (slot >= 0) cudaEventRecord(gpu->clock_events[2 * slot + 1], stream);
+    }
+};
 
 // Bytes the context's page-locked readback words hold.
 constexpr size_t kReadbackBytes = 512;

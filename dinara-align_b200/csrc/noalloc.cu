@@ -24,7 +24,8 @@ constexpr int kStaticSlots = kStaticBlocks * 8;    // 256 pair groups at once
 constexpr int64_t kStaticOrder = 1 << 20;          // pairs a launch takes; larger batches go in turns
 constexpr size_t kOrderBytes = size_t(kStaticOrder) * sizeof(uint32_t);
 constexpr size_t kCarryBytes = size_t(kStaticSlots) * (kStaticRows + 1) * sizeof(int2);
-constexpr size_t kStaticBytes = kOrderBytes + kCarryBytes;  // 4 MiB + 16 MiB
+constexpr size_t kVerdictBytes = 256;              // the size check's verdict word, then padding
+constexpr size_t kStaticBytes = kOrderBytes + kCarryBytes + kVerdictBytes;  // 4 MiB + 16 MiB + 256 B
 
 static __device__ __align__(256) unsigned char static_scratch[kStaticBytes];
 
@@ -32,24 +33,24 @@ static __device__ __align__(256) unsigned char static_scratch[kStaticBytes];
 std::mutex setup_lock;
 void *scratch_address[64] = {nullptr};
 
-// Host room to read the caller's pair shapes back a slice at a time, for the size check.
-constexpr int kCheckSlice = 4096;
-dinara_packed_pair check_slice[kCheckSlice];
+// Verdict bits the check kernel sets.
+constexpr unsigned kPastCarry = 1u;  // a pair wider than one strip with more than kStaticRows rows
+constexpr unsigned kPastReach = 2u;  // a pair whose scores could pass 2^28 (ScoreReach, scoring.mojo:218-249)
 
-// Whether every pair fits the carried column: a pair wider than 512 columns (one strip) may have at
-// most kStaticRows reference letters. Reads the shapes back under the set-up lock.
-cudaError_t pairs_fit(const dinara_packed_pair *shapes, int64_t pairs, bool *fits) {
-    std::lock_guard<std::mutex> hold(setup_lock);
-    *fits = true;
-    for (int64_t first = 0; first < pairs; first += kCheckSlice) {
-        const int64_t count = std::min<int64_t>(kCheckSlice, pairs - first);
-        cudaError_t status = cudaMemcpy(check_slice, shapes + first, size_t(count) * sizeof(dinara_packed_pair),
-                                        cudaMemcpyDeviceToHost);
-        if (status != cudaSuccess) return status;
-        for (int64_t k = 0; k < count; ++k)
-            if (check_slice[k].columns > 512 && check_slice[k].rows > uint32_t(kStaticRows)) *fits = false;
+// Reads every pair's shape on the device and sets the verdict's bits for pairs the sweep cannot take:
+// one past the carried column, or one whose scores could pass 2^28 as the main entry points refuse them
+// per pair (letters = rows + columns globally, the shorter side locally).
+__global__ void check_kernel(const dinara_packed_pair *__restrict__ shapes, int64_t pairs, bool local,
+                             int64_t reach_opening, int64_t reach_step, unsigned *__restrict__ verdict) {
+    unsigned bits = 0;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < pairs; k += int64_t(gridDim.x) * blockDim.x) {
+        const dinara_packed_pair s = shapes[k];
+        if (s.columns > 512 && s.rows > uint32_t(kStaticRows)) bits |= kPastCarry;
+        const int64_t letters = local ? int64_t(min(s.rows, s.columns)) : int64_t(s.rows) + s.columns;
+        if (reach_opening + 2 * (letters + 2) * reach_step >= (int64_t(1) << 28)) bits |= kPastReach;
     }
-    return cudaSuccess;
+    bits = __reduce_or_sync(0xffffffffu, bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicOr(verdict, bits);
 }
 
 __global__ void identity_order_kernel(uint32_t *order, int64_t count) {
@@ -101,21 +102,26 @@ extern "C" int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const
                  mode->query_end)
             return DINARA_INVALID_MODE;
     }
+    // The gap scores as the main entry points check them (scoring.mojo:202-215 gap_scores).
     const int64_t opening = scoring->opening, extension = scoring->extension;
     if (opening > 0 || extension > 0 || opening + extension < -int64_t(INT32_MAX) || extension < -int64_t(INT32_MAX))
         return DINARA_INVALID_COSTS;
     const int32_t open = int32_t(opening + extension), extend = int32_t(extension);
-    if (pairs == 0) return 0;
-    if (!tape || !shapes || !scores) return DINARA_INVALID_LENGTH;
     // The table in two registers a row letter, 16 bits an entry, shifted for a global sweep.
     TableArgs table;
     std::memset(&table, 0, sizeof table);
     const int64_t size = scoring->alphabet_size;
+    int64_t highest = -128, lowest = 127;
     for (int r = 0; r < 4; ++r) {
         uint16_t entries[4] = {0, 0, 0, 0};
         for (int c = 0; c < 4; ++c) {
             int64_t v = 0;
-            if (r < size && c < size) v = scoring->table[r * size + c] - (local ? 0 : 2 * int64_t(extend));
+            if (r < size && c < size) {
+                const int64_t entry = scoring->table[r * size + c];
+                highest = std::max(highest, entry);
+                lowest = std::min(lowest, entry);
+                v = entry - (local ? 0 : 2 * int64_t(extend));
+            }
             if (v < -32768 || v > 32767) return DINARA_INVALID_COSTS;
             entries[c] = uint16_t(int16_t(v));
         }
@@ -123,6 +129,11 @@ extern "C" int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const
                                      uint32_t(entries[2]) | (uint32_t(entries[3]) << 16));
     }
     table.size = int32_t(size);
+    // ScoreReach (scoring.mojo:228-249): what a score can move by at an opening and at a letter.
+    const int64_t reach_opening = 2 * -int64_t(open);
+    const int64_t reach_step = std::max(std::max(highest, -lowest), -int64_t(extend));
+    if (pairs == 0) return 0;
+    if (!tape || !shapes || !scores) return DINARA_INVALID_LENGTH;
     cudaStream_t on = static_cast<cudaStream_t>(stream);
     int current = 0;
     if (cudaGetDevice(&current) != cudaSuccess) return DINARA_DEVICE_FAILURE;
@@ -130,12 +141,27 @@ extern "C" int64_t dinara_gpu_scores_static(int64_t device, int64_t pairs, const
     void *scratch = nullptr;
     cudaError_t status = scratch_on(int(device), on, &scratch);
     int64_t code = 0;
-    bool fits = true;
-    if (status == cudaSuccess) status = cudaStreamSynchronize(on);
-    if (status == cudaSuccess) status = pairs_fit(shapes, pairs, &fits);
+    unsigned verdict = 0;
+    unsigned *verdict_device =
+        reinterpret_cast<unsigned *>(static_cast<unsigned char *>(scratch) + kOrderBytes + kCarryBytes);
+    if (status == cudaSuccess) {
+        // The check runs on the caller's stream, after whatever wrote the shapes there; its one word comes
+        // back before any sweep is launched, so a refused batch runs nothing.
+        status = cudaMemsetAsync(verdict_device, 0, sizeof(unsigned), on);
+        if (status == cudaSuccess) {
+            check_kernel<<<kStaticBlocks * 4, 256, 0, on>>>(shapes, pairs, local, reach_opening, reach_step,
+                                                           verdict_device);
+            status = cudaGetLastError();
+        }
+        if (status == cudaSuccess)
+            status = cudaMemcpyAsync(&verdict, verdict_device, sizeof(unsigned), cudaMemcpyDeviceToHost, on);
+        if (status == cudaSuccess) status = cudaStreamSynchronize(on);
+    }
     if (status != cudaSuccess) {
         code = DINARA_DEVICE_FAILURE;
-    } else if (!fits) {
+    } else if (verdict & kPastReach) {
+        code = DINARA_INVALID_COSTS;  // scores that could pass 2^28, refused as ScoreReach refuses them
+    } else if (verdict & kPastCarry) {
         code = DINARA_OUT_OF_MEMORY;  // a pair past the fixed scratch: more than 8191 rows and 512 columns
     } else {
         KernelArgs args;

@@ -50,9 +50,11 @@ def subset(tape: Tape, pairs: np.ndarray) -> Tape:
     offsets[0:-1:2] = at[:-1]
     offsets[1::2] = at[:-1] + (middles - starts)
     offsets[-1] = at[-1]
-    letters = np.zeros(max(int(at[-1]), 1), dtype=np.uint8)
-    for k, (start, end) in enumerate(zip(starts, ends)):
-        letters[at[k]:at[k + 1]] = tape.letters[start:end]
+    # One gather: letter j of the new tape comes from its pair's start plus its place within the pair.
+    total = int(at[-1])
+    source = np.arange(total, dtype=np.int64) + np.repeat(starts - at[:-1], lengths)
+    letters = np.zeros(max(total, 1), dtype=np.uint8)
+    letters[:total] = tape.letters[source]
     return Tape(letters, offsets)
 
 
@@ -73,9 +75,17 @@ def run(tape: Tape, align: Callable[[Tape], np.ndarray], group=None, costs: Opti
     dist.gather_object((mine, found), gathered, dst=root, group=group)
     if rank != root:
         return None
-    out = None
+    # One dtype for every rank's values: numbers promote to a common type, anything else (CIGAR strings,
+    # alignments) is kept as objects, so no rank's values are cut to another's width.
+    filled = [np.asarray(values) for _, values in gathered if len(values)]
+    if filled and all(v.dtype.kind in "biuf" for v in filled):
+        dtype = np.result_type(*filled)
+    elif filled:
+        dtype = object
+    else:
+        dtype = np.int64
+    out = np.zeros(tape.pairs, dtype=dtype) if dtype is not object else np.empty(tape.pairs, dtype=object)
     for pairs, values in gathered:
-        if out is None:
-            out = np.zeros(tape.pairs, dtype=values.dtype if len(values) else np.int64)
-        out[pairs] = values
+        if len(pairs):
+            out[pairs] = np.asarray(values, dtype=dtype) if dtype is not object else list(values)
     return out

@@ -238,6 +238,14 @@ typedef struct {
     double record_ms;      /* device time of the recording sweep and walk (alignments) */
     int64_t launches;      /* kernels this library launched in the call */
     int64_t cells;         /* matrix cells the sweeps updated */
+    /* Device time and launches by kernel class, each launch timed on its own stream: 0 the proven-band
+     * sweep recording decisions, 1 the proven-band sweep for scores, 2 whole-matrix sweeps, 3 the walk,
+     * 4 unit-cost band rounds (a round's window shapes, first launch to last), 5 the learned band's
+     * sketch and prediction, 6 unit-cost CIGARs (recording band and trace), 7 other. */
+    double class_ms[8];
+    int64_t class_launches[8];
+    int64_t band_cells;    /* of `cells`, those of proven bands (64 diagonals a row) */
+    int64_t whole_cells;   /* of `cells`, those of whole matrices (including the bands' leftovers) */
 } dinara_timing;
 
 /* Uploads and packs `pairs` pairs for a Scoring (or, with `scoring` null, as bytes for unit-cost
@@ -306,11 +314,17 @@ int64_t dinara_server_stats(dinara_server *server, dinara_server_stats_t *stats)
  * `tape` holds each sequence's letters as 2-bit codes in the Scoring's alphabet order (alphabets of up
  * to 4 letters), 16 a 32-bit word, lowest bits first, each sequence from a 16-byte boundary; pair i is
  * described by shapes[i] (word offsets into `tape` and lengths). Writes scores[i] (int32, device) on
- * `stream` (a cudaStream_t; null is the default stream) and returns once the work is enqueued.
- * Limits: a pair wider than 512 columns may have at most 8,191 reference letters (else
- * DINARA_OUT_OF_MEMORY and nothing runs); a shifted table entry must fit 16 bits.
- * The first call on a device sets its array up (and synchronizes the stream), so make it before any
- * stream capture. Calls share the array: two calls that overlap on the GPU race, so serialize them.
+ * `stream` (a cudaStream_t; null is the default stream).
+ * Every call first checks the pairs' shapes with a small kernel on `stream` and waits for that stream
+ * to reach it, reading back one 4-byte verdict; it then enqueues the sweep and returns without waiting
+ * for it. A refused batch runs nothing and writes no score:
+ *   - DINARA_OUT_OF_MEMORY: a pair wider than 512 columns with more than 8,191 reference letters (past
+ *     the fixed array);
+ *   - DINARA_INVALID_COSTS: a pair whose scores could pass 2^28 (the reference's ScoreReach,
+ *     scoring.mojo:218-249, which the other entry points report per pair), or a shifted table entry
+ *     past 16 bits.
+ * The first call on a device also sets its array up, so make it before any stream capture. Calls share
+ * the array: two calls that overlap on the GPU race, so serialize them.
  */
 typedef struct {
     uint32_t first_word; /* the reference's first word in `tape` */

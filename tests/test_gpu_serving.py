@@ -48,3 +48,22 @@ def test_budget_refusal_and_bounded_wait(da):
         code, scores, _, _ = server.wait(ticket, timeout=600)
         assert code == 0
         np.testing.assert_array_equal(scores, da.scores_tape(tape, da.Scoring.dna()))
+
+
+def test_wait_runs_out_then_completes(da):
+    """A wait shorter than the request's run gives DINARA_DEVICE_TIMEOUT and leaves the request queued or
+    running; a later wait collects the same scores the request gets alone."""
+    from dinara_align import serving, workloads
+
+    rng = np.random.default_rng(25)
+    tape = workloads.pairs_with_errors(rng, np.full(48, 10_000), 0.05, workloads.HALF_QUARTERS)
+    scoring = da.Scoring.uniform(0, -4, -6, -2)
+    expected = da.scores_tape(tape, scoring)
+    with serving.Server(slots=1) as server:
+        ticket = server.submit(tape, scoring)
+        code, _, _, _ = server.wait(ticket, timeout=0.001)
+        assert code == da._native.DEVICE_TIMEOUT
+        code, scores, statuses, _ = server.wait(ticket, timeout=600)
+        assert code == 0
+        np.testing.assert_array_equal(scores, expected)
+        assert (statuses == 0).all()
