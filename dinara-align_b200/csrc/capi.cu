@@ -25,6 +25,7 @@
 #include "internal.cuh"
 #include "learned.cuh"
 #include "pack.cuh"
+#include "ties.cuh"
 
 using namespace dinara;
 
@@ -1427,6 +1428,42 @@ void upload_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int6
     *offsets_out = offsets_device;
 }
 
+// A global mode, as the GPU takes Costs: free ends of none, no match score (null is global).
+void check_global(const dinara_mode *mode) {
+    if (mode && (mode->kind != DINARA_ENDS_FREE || mode->reference_start || mode->reference_end ||
+                 mode->query_start || mode->query_end || mode->match_score))
+        throw Failure(DINARA_INVALID_MODE, "on the GPU, Costs align globally");
+}
+
+// Whether costs and options are unit costs with no band or cap (api.mojo:1240-1246), which band doubling
+// serves; *scale is the factor the costs are of unit costs.
+bool unit_costs(const dinara_costs *costs, const dinara_options *options, int64_t *scale) {
+    *scale = 1;
+    if (options && (options->band_low > INT64_MIN || options->band_high < INT64_MAX || options->max_cost >= 0))
+        return false;
+    if (!costs) return true;
+    const bool symmetric = costs->deletion_extension == 0 ||
+                           (costs->deletion_opening == costs->opening && costs->deletion_extension == costs->extension);
+    if (costs->opening2 >= 0 || costs->opening != 0 || costs->mismatch != costs->extension || costs->mismatch <= 0 ||
+        !symmetric)
+        return false;
+    *scale = costs->mismatch;
+    return true;
+}
+
+// The process's context for the entry points under the reference's own names, which take none: device
+// 0, opened at the first call and kept; calls from several threads take turns on it.
+std::mutex default_lock;
+dinara_gpu *default_context = nullptr;
+
+dinara_gpu *default_gpu() {
+    if (!default_context) {
+        default_context = dinara_gpu_new(0);
+        if (!default_context) throw Failure(DINARA_DEVICE_FAILURE, "no GPU: " + new_error);
+    }
+    return default_context;
+}
+
 }  // namespace
 
 int64_t dinara_gpu_predictor_train(dinara_gpu *gpu, const dinara_train_options *options, dinara_train_report *report) {
@@ -1563,6 +1600,161 @@ int64_t dinara_gpu_predictor_predict(dinara_gpu *gpu, int64_t pairs, const char 
         DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
         return 0;
     });
+}
+
+int64_t dinara_gpu_cost_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                        const dinara_costs *costs, const dinara_mode *mode,
+                                        const dinara_options *options, int64_t *results, int64_t *cigar_offsets,
+                                        char **cigar_bytes) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+        check_global(mode);
+        const CostPlan plan = cost_plan(costs, options);
+        check_offsets(pairs, offsets);
+        const bool eqx = options ? options->eqx != 0 : true;
+        const bool right = options ? options->right_ties != 0 : false;
+        if (cigar_bytes) *cigar_bytes = nullptr;
+        if (pairs == 0) {
+            if (cigar_offsets) cigar_offsets[0] = 0;
+            if (cigar_bytes) *cigar_bytes = static_cast<char *>(std::calloc(1, 1));
+            return 0;
+        }
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        const uint8_t *letters_device;
+        const int64_t *offsets_device;
+        upload_tape(gpu, pairs, letters, offsets, &letters_device, &offsets_device);
+        int64_t *results_device = gpu->scores.ensure<int64_t>(size_t(pairs));
+        const bool trace = cigar_bytes != nullptr;
+        const int64_t total = cost_alignments(gpu, pairs, letters_device, offsets_device, plan, right, eqx, trace,
+                                              results_device);
+        to_host(gpu, results, results_device, size_t(pairs) * sizeof(int64_t));
+        if (trace) {
+            std::unique_ptr<char, void (*)(void *)> bytes(static_cast<char *>(std::malloc(size_t(total) + 1)), std::free);
+            if (!bytes) throw std::bad_alloc();
+            if (cigar_offsets)
+                to_host(gpu, cigar_offsets, gpu->cigar_offsets.as<int64_t>(), size_t(pairs + 1) * sizeof(int64_t));
+            DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+            to_host_now(gpu, bytes.get(), gpu->cigar_bytes.as<char>(), size_t(total));
+            bytes.get()[total] = 0;
+            *cigar_bytes = bytes.release();
+        }
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        return 0;
+    });
+}
+
+// ------------------------------------------------------------------------------------------------------
+// The reference's own C entry points (c/dinara.h:141-228), on the GPU of the process's default context.
+
+int64_t dinara_distances(int64_t pairs, const char *const *references, const int64_t *reference_lengths,
+                         const char *const *queries, const int64_t *query_lengths, const dinara_costs *costs,
+                         const dinara_mode *mode, const dinara_options *options, int64_t threads, int64_t *results) {
+    (void)threads;  // the device's own parallelism; the host does no per-pair work
+    std::lock_guard<std::mutex> hold(default_lock);
+    dinara_gpu *gpu = nullptr;
+    try {
+        gpu = default_gpu();
+    } catch (const Failure &failure) {
+        return failure.code;
+    }
+    return guard(gpu, [&]() -> int64_t {
+        check_global(mode);
+        int64_t scale = 1;
+        if (unit_costs(costs, options, &scale)) {
+            const int64_t code = dinara_gpu_distances(gpu, pairs, references, reference_lengths, queries,
+                                                      query_lengths, costs, mode, options, results);
+            if (code != 0) throw Failure(code, gpu->error);
+            return 0;
+        }
+        (void)cost_plan(costs, options);
+        std::vector<char> letters;
+        std::vector<int64_t> offsets;
+        gather_tape(pairs, references, reference_lengths, queries, query_lengths, letters, offsets);
+        const int64_t code = dinara_gpu_cost_alignments_tape(gpu, pairs, letters.data(), offsets.data(), costs, mode,
+                                                             options, results, nullptr, nullptr);
+        if (code != 0) throw Failure(code, gpu->error);
+        return 0;
+    });
+}
+
+int64_t dinara_alignments(int64_t pairs, const char *const *references, const int64_t *reference_lengths,
+                          const char *const *queries, const int64_t *query_lengths, const dinara_costs *costs,
+                          const dinara_mode *mode, const dinara_options *options, int64_t threads,
+                          dinara_alignment *alignments, int64_t *statuses) {
+    (void)threads;
+    std::lock_guard<std::mutex> hold(default_lock);
+    dinara_gpu *gpu = nullptr;
+    try {
+        gpu = default_gpu();
+    } catch (const Failure &failure) {
+        return failure.code;
+    }
+    return guard(gpu, [&]() -> int64_t {
+        check_global(mode);
+        (void)cost_plan(costs, options);
+        std::vector<char> letters;
+        std::vector<int64_t> offsets;
+        gather_tape(pairs, references, reference_lengths, queries, query_lengths, letters, offsets);
+        std::vector<int64_t> results(size_t(std::max<int64_t>(pairs, 1)));
+        std::vector<int64_t> cigar_offsets(size_t(pairs + 1));
+        char *bytes = nullptr;
+        const int64_t code = dinara_gpu_cost_alignments_tape(gpu, pairs, letters.data(), offsets.data(), costs, mode,
+                                                             options, results.data(), cigar_offsets.data(), &bytes);
+        if (code != 0) throw Failure(code, gpu->error);
+        std::unique_ptr<char, void (*)(void *)> owned(bytes, std::free);
+        for (int64_t p = 0; p < pairs; ++p) {
+            dinara_alignment &a = alignments[p];
+            std::memset(&a, 0, sizeof a);
+            const int64_t cost = results[size_t(p)];
+            if (statuses) statuses[p] = cost < 0 ? cost : 0;
+            if (cost < 0) continue;
+            const int64_t length = cigar_offsets[size_t(p + 1)] - cigar_offsets[size_t(p)];
+            a.cigar = static_cast<char *>(std::malloc(size_t(length) + 1));
+            if (!a.cigar) throw std::bad_alloc();
+            std::memcpy(a.cigar, bytes + cigar_offsets[size_t(p)], size_t(length));
+            a.cigar[length] = 0;
+            a.cigar_length = length;
+            a.cost = cost;
+            a.score = -cost;
+            a.reference_start = 0;
+            a.reference_end = reference_lengths[p];
+            a.query_start = 0;
+            a.query_end = query_lengths[p];
+        }
+        return 0;
+    });
+}
+
+int64_t dinara_distance(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                        const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options) {
+    int64_t result = 0;
+    const int64_t code = dinara_distances(1, &reference, &reference_length, &query, &query_length, costs, mode,
+                                          options, 0, &result);
+    return code != 0 ? code : result;
+}
+
+int64_t dinara_align(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                     const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options,
+                     dinara_alignment *alignment) {
+    int64_t status = 0;
+    const int64_t code = dinara_alignments(1, &reference, &reference_length, &query, &query_length, costs, mode,
+                                           options, 0, alignment, &status);
+    return code != 0 ? code : status;
+}
+
+int64_t dinara_score(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                     const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options,
+                     int64_t *score) {
+    // The options' cap, eqx, ties and memory change nothing (c/dinara.h:172-177).
+    dinara_options plain = {INT64_MIN, INT64_MAX, -1, 1, 0, 0};
+    if (options) {
+        plain.band_low = options->band_low;
+        plain.band_high = options->band_high;
+    }
+    const int64_t cost = dinara_distance(reference, reference_length, query, query_length, costs, mode, &plain);
+    if (cost < 0) return cost;
+    if (score) *score = -cost;
+    return 0;
 }
 
 }  // extern "C"

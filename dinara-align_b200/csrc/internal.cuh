@@ -151,6 +151,8 @@ struct dinara_gpu {
     dinara::DeviceBuffer planes, plane_offsets, thresholds, distances, pending, pending_next, counters, table32;
     // Learned band predictor.
     dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations, sketches;
+    // Alignments under Costs: each warp's arena of kept fronts (ties.cu).
+    dinara::DeviceBuffer wavefront;
     bool predictor_ready = false;
     double predictor_margin = 1.25;    // the largest of the classes' margins (reported)
     double predictor_margins[4] = {1.25, 1.25, 1.25, 1.25};  // by mean length: < 300, < 1000, < 4096, more
@@ -190,7 +192,8 @@ struct dinara_gpu {
             &leftovers, &decisions_extra, &scores,  &carry,         &decisions,     &decision_offsets, &walk_out,
             &cigar_slots, &cigar_lengths, &cigar_offsets, &cigar_bytes, &spans,      &planes,        &plane_offsets,
             &thresholds, &distances,   &pending,    &pending_next,  &counters,      &table32,       &features,
-            &weights,   &gradients,    &optimizer,  &predictions,   &targets,       &activations,   &sketches};
+            &weights,   &gradients,    &optimizer,  &predictions,   &targets,       &activations,   &sketches,
+            &wavefront};
         for (dinara::DeviceBuffer *buffer : all) visit(*buffer);
     }
 };

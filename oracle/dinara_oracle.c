@@ -632,3 +632,423 @@ void oracle_batch_distances(int64_t pairs, const uint8_t *tape, const int64_t *o
     job.distances = results;
     run_batch(&job, threads);
 }
+
+/* ---------------------------------------------------------------------------------------------- */
+/* CIGARs under Costs, by the Ties rule                                                             */
+/* ---------------------------------------------------------------------------------------------- */
+
+/* Runs of one CIGAR letter, joined when the same letter comes again (cigar.mojo:183-200 CigarWriter). */
+typedef struct {
+    char *letters;
+    int64_t *lengths;
+    int64_t count, capacity;
+} cigar_runs;
+
+static int runs_init(cigar_runs *r, int64_t capacity) {
+    r->count = 0;
+    r->capacity = capacity > 4 ? capacity : 4;
+    r->letters = (char *)malloc((size_t)r->capacity);
+    r->lengths = (int64_t *)malloc((size_t)r->capacity * sizeof(int64_t));
+    return r->letters && r->lengths;
+}
+
+static void runs_free(cigar_runs *r) {
+    free(r->letters);
+    free(r->lengths);
+}
+
+static void runs_add(cigar_runs *r, char letter, int64_t length) {
+    if (length <= 0) return;
+    if (r->count > 0 && r->letters[r->count - 1] == letter) {
+        r->lengths[r->count - 1] += length;
+        return;
+    }
+    if (r->count == r->capacity) {
+        r->capacity *= 2;
+        r->letters = (char *)realloc(r->letters, (size_t)r->capacity);
+        r->lengths = (int64_t *)realloc(r->lengths, (size_t)r->capacity * sizeof(int64_t));
+    }
+    r->letters[r->count] = letter;
+    r->lengths[r->count] = length;
+    r->count += 1;
+}
+
+/* The runs as CIGAR text, first to last or (`backwards`) last to first; returns the text's length. */
+static int64_t runs_text(const cigar_runs *r, int backwards, char *out, int64_t capacity) {
+    int64_t at = 0;
+    for (int64_t i = 0; i < r->count; ++i) {
+        const int64_t k = backwards ? r->count - 1 - i : i;
+        char digits[24];
+        int d = 0;
+        int64_t v = r->lengths[k];
+        do {
+            digits[d++] = (char)('0' + v % 10);
+            v /= 10;
+        } while (v > 0);
+        if (at + d + 2 > capacity) return -1;
+        while (d > 0) out[at++] = digits[--d];
+        out[at++] = r->letters[k];
+    }
+    if (at + 1 > capacity) return -1;
+    out[at] = 0;
+    return at;
+}
+
+static uint8_t *reversed_copy(const uint8_t *s, int64_t n) {
+    uint8_t *out = (uint8_t *)malloc((size_t)(n > 0 ? n : 1));
+    for (int64_t i = 0; i < n; ++i) out[i] = s[n - 1 - i];
+    return out;
+}
+
+/* Every cost's front on diagonals lo ..= hi (a diagonal is the first sequence's letters less the
+ * second's), its columns (the first sequence's letters) from cols[0]. */
+typedef struct {
+    int64_t lo, hi;
+    int64_t *cols;
+} dt_front;
+
+#define DT_UNREACHED (-1)
+
+static inline int64_t dt_at(const dt_front *f, int64_t k) {
+    return k < f->lo || k > f->hi ? DT_UNREACHED : f->cols[k - f->lo];
+}
+
+/* furthest_source, diagonal.mojo:286-303: the furthest column a path of one more edit reaches on
+ * `diagonal` before its matches, and its last move (0 a substitution, 1 a letter of the first sequence
+ * alone, 2 one of the second); ties go to a substitution, then the first sequence's letter. */
+static inline int64_t dt_source(int64_t same, int64_t left, int64_t up, int64_t diagonal, int64_t columns,
+                                int64_t rows, int *move) {
+    int64_t best = -1;
+    *move = 0;
+    if (same >= 0 && same < columns && same - diagonal < rows) best = same + 1;
+    if (left >= 0 && left < columns && left + 1 > best) {
+        best = left + 1;
+        *move = 1;
+    }
+    if (up >= 0 && up - diagonal - 1 < rows && up > best) {
+        best = up;
+        *move = 2;
+    }
+    return best;
+}
+
+static inline int64_t slide(const uint8_t *first, int64_t columns, const uint8_t *second, int64_t rows, int64_t column,
+                            int64_t diagonal) {
+    int64_t row = column - diagonal;
+    while (column < columns && row < rows && first[column] == second[row]) {
+        ++column;
+        ++row;
+    }
+    return column;
+}
+
+/* The unit-cost distance and the CIGAR `edit_cigar` gives (edit_distance.mojo:265-330): the fronts of
+ * diagonal transition, each cost's furthest column on each diagonal after sliding over matches, traced
+ * back from the corner by `best_source` (diagonal.mojo:306-316) as diagonal_cigar writes it
+ * (traceback.mojo:803-900). Ties.RIGHT traces the pair itself; Ties.LEFT (`right` zero) traces both
+ * sequences reversed, whose moves back from their corner run forward over the pair. */
+static int64_t dt_cigar(const uint8_t *first, int64_t columns, const uint8_t *second, int64_t rows, int backwards,
+                        int eqx, cigar_runs *runs) {
+    int64_t capacity = 64, count = 0;
+    dt_front *fronts = (dt_front *)malloc((size_t)capacity * sizeof(dt_front));
+    const int64_t target = columns - rows;
+    fronts[0].lo = fronts[0].hi = 0;
+    fronts[0].cols = (int64_t *)malloc(sizeof(int64_t));
+    fronts[0].cols[0] = slide(first, columns, second, rows, 0, 0);
+    count = 1;
+    int64_t distance = 0;
+    while (!(target >= fronts[distance].lo && target <= fronts[distance].hi &&
+             fronts[distance].cols[target - fronts[distance].lo] >= columns)) {
+        const dt_front *last = &fronts[distance];
+        if (count == capacity) {
+            capacity *= 2;
+            fronts = (dt_front *)realloc(fronts, (size_t)capacity * sizeof(dt_front));
+            last = &fronts[distance];
+        }
+        dt_front *next = &fronts[count];
+        next->lo = last->lo - 1 > -rows ? last->lo - 1 : -rows;
+        next->hi = last->hi + 1 < columns ? last->hi + 1 : columns;
+        next->cols = (int64_t *)malloc((size_t)(next->hi - next->lo + 1) * sizeof(int64_t));
+        for (int64_t k = next->lo; k <= next->hi; ++k) {
+            int move;
+            int64_t best = dt_source(dt_at(last, k), dt_at(last, k - 1), dt_at(last, k + 1), k, columns, rows, &move);
+            next->cols[k - next->lo] = best < 0 ? DT_UNREACHED : slide(first, columns, second, rows, best, k);
+        }
+        ++count;
+        ++distance;
+    }
+    const char matched = eqx ? '=' : 'M', substituted = eqx ? 'X' : 'M';
+    int64_t diagonal = target, column = columns;
+    for (int64_t score = distance; score > 0; --score) {
+        const dt_front *back = &fronts[score - 1];
+        int move;
+        const int64_t best = dt_source(dt_at(back, diagonal), dt_at(back, diagonal - 1), dt_at(back, diagonal + 1),
+                                       diagonal, columns, rows, &move);
+        if (column > best) runs_add(runs, matched, column - best);
+        if (move == 0) {
+            runs_add(runs, substituted, 1);
+            column = best - 1;
+        } else if (move == 1) {
+            runs_add(runs, 'D', 1);
+            column = best - 1;
+            diagonal -= 1;
+        } else {
+            runs_add(runs, 'I', 1);
+            column = best;
+            diagonal += 1;
+        }
+    }
+    if (column > 0) runs_add(runs, matched, column);
+    (void)backwards;
+    for (int64_t s = 0; s < count; ++s) free(fronts[s].cols);
+    free(fronts);
+    return distance;
+}
+
+int64_t oracle_edit_cigar(const uint8_t *first, int64_t n, const uint8_t *second, int64_t m, int32_t right,
+                          int32_t eqx, char *cigar, int64_t capacity) {
+    cigar_runs runs;
+    if (!runs_init(&runs, 2 * (n + m) + 4)) return -2;
+    int64_t distance;
+    int64_t written;
+    if (right) {
+        distance = dt_cigar(first, n, second, m, 0, eqx, &runs);
+        written = runs_text(&runs, 1, cigar, capacity);
+    } else {
+        uint8_t *a = reversed_copy(first, n), *b = reversed_copy(second, m);
+        distance = dt_cigar(a, n, b, m, 1, eqx, &runs);
+        written = runs_text(&runs, 0, cigar, capacity);
+        free(a);
+        free(b);
+    }
+    runs_free(&runs);
+    return written < 0 ? -2 : distance;
+}
+
+/* The gap-affine wavefront of gap_affine.mojo (one gap piece): each cost's alignment front (its
+ * furthest column a diagonal, after sliding over matches), its two gap layers' fronts and the flag of
+ * which source won each (gap_affine.mojo:858-1010 with `record`), over the costs divided by their common
+ * factor (Penalties.scale). A letter of the first sequence against a gap (the FIRST_GAP layer, a
+ * deletion, its own opening and extension) comes from the diagonal below and moves a column; one of the
+ * second (SECOND_GAP, an insertion) from the diagonal above, moving a row. */
+#define WF_UNREACHED ((int64_t)-(1ll << 40))
+#define WF_ALIGNED 0
+#define WF_FIRST 1
+#define WF_SECOND 2
+#define WF_OPENED_FIRST 8
+#define WF_OPENED_SECOND 16
+
+typedef struct {
+    int64_t lo, hi;
+    int64_t *aligned, *first_gap, *second_gap;
+    uint8_t *flags;
+} wf_front;
+
+static inline int64_t wf_get(const wf_front *fronts, int64_t count, int64_t s, int layer, int64_t k) {
+    if (s < 0 || s >= count) return WF_UNREACHED;
+    const wf_front *f = &fronts[s];
+    if (f->lo > f->hi || k < f->lo || k > f->hi) return WF_UNREACHED;
+    const int64_t *v = layer == WF_ALIGNED ? f->aligned : layer == WF_FIRST ? f->first_gap : f->second_gap;
+    return v[k - f->lo];
+}
+
+static inline int64_t gcd64(int64_t a, int64_t b) {
+    while (b) {
+        const int64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+/* The single search of gap_affine.mojo over one direction and its trace (trace, :2028-2124), the moves
+ * right to left into `runs`. Returns the cost (scaled back), or -4 when it passes `max_cost`. */
+static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *second, int64_t rows, int64_t x,
+                        int64_t od, int64_t ed, int64_t oi, int64_t ei, int64_t max_cost, int eqx, cigar_runs *runs) {
+    int64_t scale = gcd64(gcd64(gcd64(x, od), gcd64(ed, oi)), ei);
+    if (scale <= 0) scale = 1;
+    x /= scale;
+    od /= scale;
+    ed /= scale;
+    oi /= scale;
+    ei /= scale;
+    const int64_t ceiling = max_cost < 0 ? INT64_MAX : max_cost / scale;
+    int64_t capacity = 64, count = 0;
+    wf_front *fronts = (wf_front *)calloc((size_t)capacity, sizeof(wf_front));
+    const int64_t target = columns - rows;
+    int64_t cost = -1;
+    for (int64_t s = 0;; ++s) {
+        if (s > ceiling) break;
+        if (count == capacity) {
+            capacity *= 2;
+            fronts = (wf_front *)realloc(fronts, (size_t)capacity * sizeof(wf_front));
+        }
+        wf_front *f = &fronts[count];
+        memset(f, 0, sizeof *f);
+        if (s == 0) {
+            f->lo = f->hi = 0;
+        } else {
+            /* The diagonals any source reaches. */
+            int64_t lo = INT64_MAX, hi = INT64_MIN;
+            const int64_t from[5] = {s - x, s - od - ed, s - ed, s - oi - ei, s - ei};
+            const int64_t shift[5] = {0, 1, 1, -1, -1};
+            for (int q = 0; q < 5; ++q) {
+                if (from[q] < 0 || from[q] >= count) continue;
+                const wf_front *g = &fronts[from[q]];
+                if (g->lo > g->hi) continue;
+                if (g->lo + shift[q] < lo) lo = g->lo + shift[q];
+                if (g->hi + shift[q] > hi) hi = g->hi + shift[q];
+            }
+            if (lo < -rows) lo = -rows;
+            if (hi > columns) hi = columns;
+            f->lo = lo;
+            f->hi = hi;
+        }
+        const int64_t width = f->hi >= f->lo ? f->hi - f->lo + 1 : 0;
+        f->aligned = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
+        f->first_gap = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
+        f->second_gap = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
+        f->flags = (uint8_t *)calloc((size_t)(width > 0 ? width : 1), 1);
+        ++count;
+        for (int64_t k = f->lo; k <= f->hi; ++k) {
+            const int64_t i = k - f->lo;
+            if (s == 0) {
+                f->aligned[i] = slide(first, columns, second, rows, 0, 0);
+                f->first_gap[i] = f->second_gap[i] = WF_UNREACHED;
+                continue;
+            }
+            const int64_t same = wf_get(fronts, count, s - x, WF_ALIGNED, k);
+            const int64_t opened_below = wf_get(fronts, count, s - od - ed, WF_ALIGNED, k - 1);
+            const int64_t extended_below = wf_get(fronts, count, s - ed, WF_FIRST, k - 1);
+            const int64_t opened_above = wf_get(fronts, count, s - oi - ei, WF_ALIGNED, k + 1);
+            const int64_t extended_above = wf_get(fronts, count, s - ei, WF_SECOND, k + 1);
+            const int64_t below = opened_below > extended_below ? opened_below : extended_below;
+            const int64_t above = opened_above > extended_above ? opened_above : extended_above;
+            const int64_t first_gap = below >= 0 && below < columns ? below + 1 : WF_UNREACHED;
+            const int64_t second_gap = above >= 0 && above - k <= rows ? above : WF_UNREACHED;
+            const int64_t substituted = same >= 0 && same < columns && same - k < rows ? same + 1 : WF_UNREACHED;
+            const int64_t gapped = first_gap > second_gap ? first_gap : second_gap;
+            uint8_t flag = 0;
+            /* Ties as WFA2-lib's backtrace breaks them: a substitution, then a letter of the first
+             * sequence alone before one of the second, and an extension before an opening. */
+            if (opened_below > extended_below) flag |= WF_OPENED_FIRST;
+            if (opened_above > extended_above) flag |= WF_OPENED_SECOND;
+            if (!(substituted >= gapped)) flag |= first_gap >= second_gap ? WF_FIRST : WF_SECOND;
+            f->flags[i] = flag;
+            f->first_gap[i] = first_gap;
+            f->second_gap[i] = second_gap;
+            const int64_t start = substituted > gapped ? substituted : gapped;
+            f->aligned[i] = start >= 0 ? slide(first, columns, second, rows, start, k) : WF_UNREACHED;
+        }
+        if (target >= f->lo && target <= f->hi && f->aligned[target - f->lo] >= columns) {
+            cost = s;
+            break;
+        }
+    }
+    if (cost >= 0) {
+        /* The trace, gap_affine.mojo:2028-2124, moves right to left. */
+        const char matched = eqx ? '=' : 'M', substituted = eqx ? 'X' : 'M';
+        int64_t spent = cost, k = target, c = columns;
+        int current = WF_ALIGNED;
+        for (;;) {
+            if (current == WF_ALIGNED) {
+                const int64_t row = c - k;
+                if (c == 0) {
+                    runs_add(runs, 'I', row);
+                    break;
+                }
+                if (row == 0) {
+                    runs_add(runs, 'D', c);
+                    break;
+                }
+                if (spent == 0) {
+                    const int64_t start = k > 0 ? k : 0;
+                    runs_add(runs, matched, c - start);
+                    c = start;
+                    continue;
+                }
+                const wf_front *f = &fronts[spent];
+                const int source = f->flags[k - f->lo] & 7;
+                const int64_t entry = source == WF_ALIGNED ? wf_get(fronts, count, spent - x, WF_ALIGNED, k) + 1
+                                      : source == WF_FIRST ? f->first_gap[k - f->lo]
+                                                           : f->second_gap[k - f->lo];
+                if (entry <= c) {
+                    runs_add(runs, matched, c - entry);
+                    c = entry;
+                }
+                if (source == WF_ALIGNED) {
+                    runs_add(runs, substituted, 1);
+                    c -= 1;
+                    spent -= x;
+                } else {
+                    current = source;
+                }
+            } else {
+                const wf_front *f = &fronts[spent];
+                const int opened = (f->flags[k - f->lo] & (current == WF_FIRST ? WF_OPENED_FIRST : WF_OPENED_SECOND)) != 0;
+                if (current == WF_FIRST) {
+                    runs_add(runs, 'D', 1);
+                    c -= 1;
+                    k -= 1;
+                    if (c == 0) {
+                        runs_add(runs, 'I', -k);
+                        break;
+                    }
+                    if (opened) {
+                        spent -= od + ed;
+                        current = WF_ALIGNED;
+                    } else {
+                        spent -= ed;
+                    }
+                } else {
+                    runs_add(runs, 'I', 1);
+                    k += 1;
+                    if (c - k == 0) {
+                        runs_add(runs, 'D', c);
+                        break;
+                    }
+                    if (opened) {
+                        spent -= oi + ei;
+                        current = WF_ALIGNED;
+                    } else {
+                        spent -= ei;
+                    }
+                }
+            }
+        }
+    }
+    for (int64_t s = 0; s < count; ++s) {
+        free(fronts[s].aligned);
+        free(fronts[s].first_gap);
+        free(fronts[s].second_gap);
+        free(fronts[s].flags);
+    }
+    free(fronts);
+    return cost < 0 ? -4 : cost * scale;
+}
+
+int64_t oracle_affine_cigar(const uint8_t *first, int64_t n, const uint8_t *second, int64_t m, int64_t mismatch,
+                            int64_t deletion_opening, int64_t deletion_extension, int64_t insertion_opening,
+                            int64_t insertion_extension, int64_t max_cost, int32_t right, int32_t eqx, char *cigar,
+                            int64_t capacity) {
+    cigar_runs runs;
+    if (!runs_init(&runs, 2 * (n + m) + 4)) return -2;
+    int64_t cost;
+    int64_t written = 0;
+    if (right) {
+        cost = wf_cigar(first, n, second, m, mismatch, deletion_opening, deletion_extension, insertion_opening,
+                        insertion_extension, max_cost, eqx, &runs);
+        if (cost >= 0) written = runs_text(&runs, 1, cigar, capacity);
+    } else {
+        uint8_t *a = reversed_copy(first, n), *b = reversed_copy(second, m);
+        cost = wf_cigar(a, n, b, m, mismatch, deletion_opening, deletion_extension, insertion_opening,
+                        insertion_extension, max_cost, eqx, &runs);
+        if (cost >= 0) written = runs_text(&runs, 0, cigar, capacity);
+        free(a);
+        free(b);
+    }
+    runs_free(&runs);
+    if (cost >= 0 && written < 0) return -2;
+    if (cost < 0 && capacity > 0) cigar[0] = 0;
+    return cost;
+}

@@ -86,6 +86,27 @@ void oracle_batch_alignments(int64_t pairs, const uint8_t *tape, const int64_t *
 void oracle_batch_distances(int64_t pairs, const uint8_t *tape, const int64_t *offsets, int64_t start,
                             int32_t threads, int64_t *results);
 
+
+/*
+ * CIGARs under Costs, by the Ties rule (modes.mojo:402-426). `first` is the reference, its letters the
+ * columns; a 'D' is one of its letters alone, an 'I' one of the second's. `right` nonzero is Ties.RIGHT
+ * (one search from the start traced back from the corner, WFA2-lib's); zero is Ties.LEFT (the same over
+ * both sequences reversed, read forward). `cigar` needs 2 * (n + m) + 2 bytes; NUL-terminated.
+ */
+
+/* Unit costs with no cap (edit_distance.mojo:265-330 edit_cigar): the distance, or -2 for no room. */
+int64_t oracle_edit_cigar(const uint8_t *first, int64_t n, const uint8_t *second, int64_t m, int32_t right,
+                          int32_t eqx, char *cigar, int64_t capacity);
+
+/* One-piece gap-affine costs, or unit costs under a cap (api.mojo:622-716 least_costly -> cigar_within,
+ * the wavefront of gap_affine.mojo): a gap of k first-sequence letters costs deletion_opening +
+ * k * deletion_extension, of the second's insertion_opening + k * insertion_extension. The cost, or -4
+ * when it passes `max_cost` (negative for none), or -2 for no room. */
+int64_t oracle_affine_cigar(const uint8_t *first, int64_t n, const uint8_t *second, int64_t m, int64_t mismatch,
+                            int64_t deletion_opening, int64_t deletion_extension, int64_t insertion_opening,
+                            int64_t insertion_extension, int64_t max_cost, int32_t right, int32_t eqx, char *cigar,
+                            int64_t capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,11 @@ def lib() -> ctypes.CDLL:
         handle.oracle_batch_alignments.restype = None
         handle.oracle_batch_alignments.argtypes = [i64, u8p, i64p, i8p, i32, i32, i32, i32, i32, i32, i32p,
                                                    ctypes.c_char_p, i64, i64p]
+        handle.oracle_edit_cigar.restype = i64
+        handle.oracle_edit_cigar.argtypes = [u8p, i64, u8p, i64, i32, i32, ctypes.c_char_p, i64]
+        handle.oracle_affine_cigar.restype = i64
+        handle.oracle_affine_cigar.argtypes = [u8p, i64, u8p, i64, i64, i64, i64, i64, i64, i64, i32, i32,
+                                               ctypes.c_char_p, i64]
         handle.oracle_batch_distances.restype = None
         handle.oracle_batch_distances.argtypes = [i64, u8p, i64p, i64, i32, i64p]
         _lib = handle
@@ -150,6 +155,31 @@ def banded_round(a, b, threshold: int) -> int:
     x, px = _u8(a)
     y, py = _u8(b)
     return lib().oracle_banded_round(px, len(x), py, len(y), threshold, None)
+
+
+def edit_cigar(first, second, right=False, eqx=True) -> tuple:
+    """(distance, CIGAR) at unit costs by the Ties rule: Ties.RIGHT with `right`, else Ties.LEFT."""
+    a, pa = _u8(first)
+    b, pb = _u8(second)
+    capacity = 2 * (len(a) + len(b)) + 8
+    out = ctypes.create_string_buffer(capacity)
+    distance = lib().oracle_edit_cigar(pa, len(a), pb, len(b), 1 if right else 0, 1 if eqx else 0, out, capacity)
+    return distance, out.value.decode("ascii")
+
+
+def affine_cigar(first, second, mismatch, opening, extension, deletion_opening=None, deletion_extension=None,
+                 max_cost=-1, right=False, eqx=True) -> tuple:
+    """(cost, CIGAR) under one-piece Costs by the wavefront and the Ties rule; cost -4 past `max_cost`.
+    Deletions (letters of the first alone) cost as insertions unless their own costs are given."""
+    a, pa = _u8(first)
+    b, pb = _u8(second)
+    capacity = 2 * (len(a) + len(b)) + 8
+    out = ctypes.create_string_buffer(capacity)
+    od = opening if deletion_opening is None else deletion_opening
+    ed = extension if deletion_extension is None else deletion_extension
+    cost = lib().oracle_affine_cigar(pa, len(a), pb, len(b), mismatch, od, ed, opening, extension, max_cost,
+                                     1 if right else 0, 1 if eqx else 0, out, capacity)
+    return cost, out.value.decode("ascii")
 
 
 def score_reach_refuses(table, size, open_, extend, rows, columns, mode=GLOBAL) -> bool:
