@@ -116,12 +116,21 @@ __device__ __forceinline__ int32_t furthest_source(int32_t same, int32_t left, i
 // or (for a trace that runs right to left) as the text reversed, which the gather turns round.
 struct CigarOut {
     char *slot;
+    int64_t capacity;  // the slot's bytes; a run that would pass them sets `overflow` and is dropped
     int64_t written = 0;
     char letter = 0;
     int64_t count = 0;
     bool forward;
+    bool overflow = false;
     __device__ void flush() {
         if (count <= 0) return;
+        int digits = 1;
+        for (int64_t v = count; v >= 10; v /= 10) ++digits;
+        if (written + digits + 1 > capacity) {
+            overflow = true;
+            count = 0;
+            return;
+        }
         if (forward) {
             char digits[20];
             int d = 0;
@@ -154,7 +163,7 @@ struct CigarOut {
 
 // The trace of diagonal transition (diagonal_cigar, traceback.mojo:803-900): from the corner, each cost
 // undoes the matches its front slid over and the edit `furthest_source` names.
-__device__ void trace_edit(const WaveArgs &a, const uint8_t *arena, const CostEntry *table, int32_t distance,
+__device__ bool trace_edit(const WaveArgs &a, const uint8_t *arena, const CostEntry *table, int32_t distance,
                            int32_t columns, int32_t rows, CigarOut &out) {
     const char matched = a.eqx ? '=' : 'M', substituted = a.eqx ? 'X' : 'M';
     int32_t diagonal = columns - rows, column = columns;
@@ -163,6 +172,7 @@ __device__ void trace_edit(const WaveArgs &a, const uint8_t *arena, const CostEn
         int move;
         const int32_t best = furthest_source(front_at(arena, back, 0, diagonal), front_at(arena, back, 0, diagonal - 1),
                                              front_at(arena, back, 0, diagonal + 1), diagonal, columns, rows, move);
+        if (best < 0 || best > column) return false;
         out.add(matched, column - best);
         if (move == 0) {
             out.add(substituted, 1);
@@ -178,6 +188,7 @@ __device__ void trace_edit(const WaveArgs &a, const uint8_t *arena, const CostEn
         }
     }
     out.add(matched, column);
+    return true;
 }
 
 // Layers of a gap-affine front: the alignment front, the first sequence's gap layer, the second's, and
@@ -194,21 +205,28 @@ __device__ __forceinline__ uint8_t flag_at(const uint8_t *arena, const CostEntry
 // (a substitution from the front `x` back, or a gap layer at the same cost, entered after the matches
 // back to its column); in a gap layer a letter of its sequence, then the opening or the extension its
 // flag names, an extension on a tie. On the first row or column the rest is a gap along it.
-__device__ void trace_affine(const WaveArgs &a, const uint8_t *arena, const CostEntry *table, int32_t cost,
+__device__ bool trace_affine(const WaveArgs &a, const uint8_t *arena, const CostEntry *table, int32_t cost,
                              int32_t columns, int32_t rows, CigarOut &out) {
     const char matched = a.eqx ? '=' : 'M', substituted = a.eqx ? 'X' : 'M';
     int32_t spent = cost, k = columns - rows, c = columns;
     int current = kAligned;
-    for (;;) {
+    // Every step moves a letter or leaves the alignment layer, so a consistent trace ends well within
+    // this; the bound and the index checks keep an inconsistent one from running on or reading astray.
+    for (int64_t steps = 4 * (int64_t(columns) + rows) + int64_t(cost) + 16; steps > 0; --steps) {
+        if (spent < 0 || spent > cost || c < 0 || c - k < 0) return false;
+        {
+            const CostEntry here = table[spent];
+            if (spent > 0 && (here.lo > here.hi || k < here.lo || k > here.hi)) return false;
+        }
         if (current == kAligned) {
             const int32_t row = c - k;
             if (c == 0) {
                 out.add('I', row);
-                return;
+                return true;
             }
             if (row == 0) {
                 out.add('D', c);
-                return;
+                return true;
             }
             if (spent == 0) {
                 const int32_t start = k > 0 ? k : 0;
@@ -240,7 +258,7 @@ __device__ void trace_affine(const WaveArgs &a, const uint8_t *arena, const Cost
                 k -= 1;
                 if (c == 0) {
                     out.add('I', -k);
-                    return;
+                    return true;
                 }
                 if (opened) {
                     spent -= a.od + a.ed;
@@ -253,7 +271,7 @@ __device__ void trace_affine(const WaveArgs &a, const uint8_t *arena, const Cost
                 k += 1;
                 if (c - k == 0) {
                     out.add('D', c);
-                    return;
+                    return true;
                 }
                 if (opened) {
                     spent -= a.oi + a.ei;
@@ -264,6 +282,7 @@ __device__ void trace_affine(const WaveArgs &a, const uint8_t *arena, const Cost
             }
         }
     }
+    return false;
 }
 
 template <bool EDIT>
@@ -402,13 +421,18 @@ __global__ void __launch_bounds__(kWaveBlock) wavefront_kernel(WaveArgs a) {
                     // (Ties.LEFT) that is the CIGAR's own order.
                     CigarOut out;
                     out.slot = a.slots + a.slot_offsets[pair];
+                    out.capacity = 2 * (int64_t(columns) + rows) + 8;
                     out.forward = a.reversed;
-                    if (EDIT)
-                        trace_edit(a, arena, table, s, columns, rows, out);
-                    else
-                        trace_affine(a, arena, table, s, columns, rows, out);
+                    const bool traced = EDIT ? trace_edit(a, arena, table, s, columns, rows, out)
+                                             : trace_affine(a, arena, table, s, columns, rows, out);
                     out.flush();
                     length = out.written;
+                    if (!traced || out.overflow) {
+                        // A trace that does not reach the origin within its fronts is a failure, reported
+                        // as the pair's code rather than as a CIGAR.
+                        a.results[pair] = DINARA_DEVICE_FAILURE;
+                        length = 0;
+                    }
                 }
             }
             if (a.lengths) a.lengths[pair] = length;

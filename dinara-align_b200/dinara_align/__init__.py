@@ -101,16 +101,37 @@ class Costs:
             raise ValueError(f"second piece {opening2}, {extension2}: its extension must cost")
         return Costs(mismatch, opening, extension, opening2, extension2)
 
+    def with_deletions(self, opening: int, extension: int, opening2: int = -1, extension2: int = 0) -> "Costs":
+        """These costs with deletions (runs of reference letters alone) of their own, the others an
+        insertion's, as bwa's `-O del,ins`."""
+        if _integers(extension)[0] <= 0 or _integers(opening)[0] < 0 or (
+                _integers(opening2)[0] >= 0 and _integers(extension2)[0] <= 0):
+            raise ValueError(f"deletions {opening}, {extension}: an extension must cost")
+        return replace(self, deletion_opening=opening, deletion_extension=extension, deletion_opening2=opening2,
+                       deletion_extension2=extension2)
+
+    def symmetric(self) -> bool:
+        """Whether deletions cost what insertions do."""
+        return self.deletion_extension == 0 or (
+            self.deletion_opening, self.deletion_extension, self.deletion_opening2, self.deletion_extension2) == (
+            self.opening, self.extension, self.opening2, self.extension2)
+
     def unit_scale(self) -> int:
         """The multiple of the edit distance these costs price every pair at, or 0 if they are not unit
-        costs: a mismatch and a gap letter alike, no opening, one piece (modes.mojo unit_scale)."""
-        one_piece = self.opening2 < 0 and self.deletion_extension == 0
-        if one_piece and self.opening == 0 and self.mismatch == self.extension and self.mismatch > 0:
-            return self.mismatch
-        return 0
+        costs: a mismatch and a gap letter alike, no opening, one piece (modes.mojo:158-163)."""
+        if self.opening2 >= 0 or self.opening != 0 or self.mismatch != self.extension or not self.symmetric():
+            return 0
+        return self.mismatch if self.mismatch > 0 else 0
+
+    def _struct(self) -> native.CCosts:
+        return native.CCosts(*_integers(self.mismatch, self.opening, self.extension, self.opening2, self.extension2,
+                                        self.deletion_opening, self.deletion_extension, self.deletion_opening2,
+                                        self.deletion_extension2))
 
 
 class Anchor:
+    """Which end of both sequences an extension is fixed at (the reference's)."""
+
     START = 0
     END = 1
 
@@ -143,8 +164,19 @@ class Mode:
         return replace(self, match_score=match_score)
 
     @staticmethod
+    def extension(match_score: int, anchor: int = Anchor.START, *, zdrop: int = -1, end_bonus: int = -1) -> "Mode":
+        """A seed's extension from both starts (or `anchor` END, both ends), a match earning
+        `match_score`; the GPU path refuses it."""
+        return Mode(_EXTENSION, match_score=match_score, anchor=anchor, zdrop=zdrop, end_bonus=end_bonus)
+
+    @staticmethod
     def local(match_score: int = 0) -> "Mode":
         return Mode(_LOCAL, match_score=match_score)
+
+    @staticmethod
+    def overlap(match_score: int) -> "Mode":
+        """Every end free and a match earning `match_score` (parasail's `sg`); the GPU path refuses it."""
+        return Mode(_ENDS, UNBOUNDED, UNBOUNDED, UNBOUNDED, UNBOUNDED, match_score)
 
     def is_global(self) -> bool:
         return self.kind == _ENDS and not (self.reference_start or self.reference_end or self.query_start
@@ -254,6 +286,47 @@ class Alignment:
                 column += length
                 row += length
         return "".join(top), "".join(bottom)
+
+    def clipped_cigar(self, query_length: int, hard: bool = False) -> str:
+        """The CIGAR as a SAM record carries it: the query's letters before and after the span clipped,
+        soft ('S') or with `hard` hard ('H'); the record's POS is reference_start + 1."""
+        clip = "H" if hard else "S"
+        head = f"{self.query_start}{clip}" if self.query_start > 0 else ""
+        tail = f"{query_length - self.query_end}{clip}" if query_length > self.query_end else ""
+        return head + self.cigar + tail
+
+    def edit_distance(self, reference: Text, query: Text) -> int:
+        """SAM's NM: substitutions and gapped letters of the aligned span."""
+        top, bottom = self.gapped(reference, query)
+        return sum(a != b for a, b in zip(top, bottom))
+
+    def identity(self, reference: Text, query: Text) -> float:
+        """Matching columns over all columns of the alignment (BLAST's identity); 0 with no columns."""
+        top, bottom = self.gapped(reference, query)
+        return sum(a == b for a, b in zip(top, bottom)) / len(top) if top else 0.0
+
+    def mismatch_string(self, reference: Text, query: Text) -> str:
+        """SAM's MD tag: runs of matched reference letters, each mismatched reference letter, and '^'
+        before each run of deleted ones; inserted query letters leave no mark."""
+        top, bottom = self.gapped(reference, query)
+        pieces, matched, in_deletion = [], 0, False
+        for a, b in zip(top, bottom):
+            if b == "-":
+                if not in_deletion:
+                    pieces.append(f"{matched}^")
+                    matched, in_deletion = 0, True
+                pieces.append(a)
+                continue
+            in_deletion = False
+            if a == "-":
+                continue
+            if a == b:
+                matched += 1
+            else:
+                pieces.append(f"{matched}{a}")
+                matched = 0
+        pieces.append(str(matched))
+        return "".join(pieces)
 
 
 @dataclass(frozen=True)
@@ -386,19 +459,94 @@ def _owned_bytes(address: Optional[int], size: int) -> np.ndarray:
     return array
 
 
+def _cost_options(band: Optional[Band], max_cost: Optional[int], eqx: bool, ties: str,
+                  max_memory: Optional[int]) -> native.COptions:
+    """The options a Costs call takes on the GPU (the reference's `_options`, python/dinara_align/
+    __init__.py:415-432): no band, a cap of zero or more, '='/'X' or 'M', ties left or right."""
+    if ties not in ("left", "right"):
+        raise ValueError("ties: 'left' or 'right'")
+    if band is not None and (band.low > -UNBOUNDED or band.high < UNBOUNDED):
+        raise ValueError("on the GPU, Costs take no band")
+    cap = -1 if max_cost is None else _integers(max_cost)[0]
+    if max_memory is not None:
+        _integers(max_memory)
+    return native.COptions(-(1 << 63), (1 << 63) - 1, cap, 1 if eqx else 0, 1 if ties == "right" else 0,
+                           max_memory or 0)
+
+
+def cost_alignments_tape(tape: Tape, costs: Costs = Costs(), *, max_cost: Optional[int] = None, ties: str = "left",
+                         eqx: bool = True, trace: bool = True, placement=None):
+    """Every pair's least cost under `costs`, globally, on the GPU, and with `trace` its CIGAR by the Ties
+    rule: (costs int64 array, negative entries the pair's code; CIGAR offsets; CIGAR bytes)."""
+    handle = native.context(_placement(placement))
+    options = _cost_options(None, max_cost, eqx, ties, None)
+    costs_struct = costs._struct()
+    mode_struct = Mode.GLOBAL._struct()
+    pairs = tape.pairs
+    out = np.empty(max(pairs, 1), dtype=np.int64)
+    offsets = np.zeros(pairs + 1, dtype=np.int64)
+    buffer = ctypes.c_void_p()
+    code = native.lib().dinara_gpu_cost_alignments_tape(
+        handle, pairs, tape.letters.ctypes.data, native.pointer(tape.offsets, ctypes.c_int64),
+        ctypes.byref(costs_struct), ctypes.byref(mode_struct), ctypes.byref(options), native.pointer(out, ctypes.c_int64),
+        native.pointer(offsets, ctypes.c_int64) if trace else None, ctypes.byref(buffer) if trace else None)
+    native.check(code, handle)
+    total = int(offsets[pairs]) if (trace and pairs) else 0
+    return out[:pairs], offsets, _owned_bytes(buffer.value, total) if trace else np.zeros(0, dtype=np.uint8)
+
+
+def _check_cost_call(costs: Costs, mode: Mode) -> None:
+    if not isinstance(costs, Costs):
+        raise TypeError("costs: a Costs or a Scoring")
+    if not mode.is_global() or mode.match_score > 0 or mode.kind != _ENDS:
+        raise ValueError("on the GPU, Costs align globally")
+    if costs.opening2 >= 0 or costs.deletion_opening2 >= 0:
+        raise ValueError("on the GPU, Costs of one gap piece")
+    if costs.mismatch <= 0:
+        raise ValueError("a mismatch that costs nothing")
+
+
+def _raise_code(pair: int, code: int) -> None:
+    if code == native.UNSUPPORTED_SYMBOLS:
+        raise ValueError(f"pair {pair}: a 0xFE or 0xFF byte")
+    if code == native.OUT_OF_MEMORY:
+        raise RuntimeError(f"dinara-align: pair {pair}: its fronts pass the device memory")
+    raise ValueError(f"pair {pair}: code {code}")
+
+
 def alignments(references: Sequence[Text], queries: Sequence[Text], costs: Union[Costs, Scoring] = Costs(),
                mode: Mode = Mode.GLOBAL, *, band: Optional[Band] = None, max_cost: Optional[int] = None,
                ties: str = "left", eqx: bool = True, max_memory: Optional[int] = None, threads: int = 0,
                placement: Optional[Placement] = None) -> list:
-    """Every pair's alignment (the reference's `alignments` signature). On the GPU under a `Scoring`,
-    Gotoh's walk picks among equal alignments, as the reference's device path does (api.mojo:895-1006)."""
-    if not isinstance(costs, Scoring):
-        raise ValueError("on the GPU, alignments under a Scoring")
+    """Every pair's alignment (the reference's `alignments` signature), None past `max_cost`. Under a
+    `Costs` the CIGAR is the one `ties` names among equally good alignments (modes.mojo:402-426); under a
+    `Scoring`, Gotoh's walk picks, as the reference's device path does (api.mojo:895-1006)."""
     if ties not in ("left", "right"):
         raise ValueError("ties: 'left' or 'right'")
+    _integers(threads)
+    tape = Tape.of(references, queries)
+    if not isinstance(costs, Scoring):
+        _check_cost_call(costs, mode)
+        _cost_options(band, max_cost, eqx, ties, max_memory)
+        if max_cost is not None and max_cost < 0:
+            return [None] * tape.pairs
+        found, offsets, data = cost_alignments_tape(tape, costs, max_cost=max_cost, ties=ties, eqx=eqx,
+                                                    placement=placement)
+        out = []
+        for pair in range(tape.pairs):
+            value = int(found[pair])
+            if value == native.ABOVE_MAX:
+                out.append(None)
+                continue
+            if value < 0:
+                _raise_code(pair, value)
+            cigar = data[offsets[pair]:offsets[pair + 1]].tobytes().decode("ascii")
+            rows = int(tape.offsets[2 * pair + 1] - tape.offsets[2 * pair])
+            columns = int(tape.offsets[2 * pair + 2] - tape.offsets[2 * pair + 1])
+            out.append(Alignment(value, -value, cigar, 0, rows, 0, columns))
+        return out
     if band is not None or max_cost is not None:
         raise ValueError("a Scoring takes no band or cap")
-    tape = Tape.of(references, queries)
     found, spans, offsets, data, codes = alignments_tape(tape, costs, mode, eqx=eqx, placement=placement)
     _raise_first(codes, "Scoring's alphabet")
     out = []
@@ -435,21 +583,33 @@ def distances_tape(tape: Tape, *, policy: int = native.BAND_PLAIN, start_thresho
 def distances(references: Sequence[Text], queries: Sequence[Text], costs: Costs = Costs(), mode: Mode = Mode.GLOBAL,
               *, band: Optional[Band] = None, max_cost: Optional[int] = None, threads: int = 0,
               placement: Optional[Placement] = None) -> list:
-    """Every pair's least cost (the reference's `distances` signature): on the GPU, unit costs
-    globally with no band or cap, as the reference's GPU placement requires (api.mojo:1237-1247)."""
+    """Every pair's least cost (the reference's `distances` signature), None past `max_cost`, globally on
+    the GPU: band doubling at unit costs with no cap (api.mojo:1237-1247), the gap-affine wavefront
+    otherwise (api.mojo:622-716)."""
     if mode.match_score > 0:
         raise ValueError("a mode with a match score maximizes a score, which `align` finds")
-    scale = costs.unit_scale()
-    if scale == 0 or not mode.is_global() or (band is not None and (band.low > -UNBOUNDED or band.high < UNBOUNDED)):
-        raise ValueError("on the GPU, distances at unit costs, globally, with no band")
-    if max_cost is not None:
-        raise ValueError("on the GPU, distances with no cap")
+    _check_cost_call(costs, mode)
+    _cost_options(band, max_cost, True, "left", None)
     _integers(threads)
-    found = distances_tape(Tape.of(references, queries), placement=placement)
-    if (found < 0).any():
-        first = int(np.flatnonzero(found < 0)[0])
-        raise ValueError(f"pair {first}: a 0xFE or 0xFF byte")
-    return [int(value) * scale for value in found]
+    tape = Tape.of(references, queries)
+    scale = costs.unit_scale()
+    if scale and max_cost is None:
+        found = distances_tape(tape, placement=placement)
+        if (found < 0).any():
+            _raise_code(int(np.flatnonzero(found < 0)[0]), int(found[found < 0][0]))
+        return [int(value) * scale for value in found]
+    if max_cost is not None and max_cost < 0:
+        return [None] * tape.pairs
+    found, _offsets, _data = cost_alignments_tape(tape, costs, max_cost=max_cost, trace=False, placement=placement)
+    out = []
+    for pair, value in enumerate(found.tolist()):
+        if value == native.ABOVE_MAX:
+            out.append(None)
+        elif value < 0:
+            _raise_code(pair, value)
+        else:
+            out.append(value)
+    return out
 
 
 def distance(reference: Text, query: Text, costs: Costs = Costs(), mode: Mode = Mode.GLOBAL, *, band=None,
@@ -457,13 +617,18 @@ def distance(reference: Text, query: Text, costs: Costs = Costs(), mode: Mode = 
     return distances([reference], [query], costs, mode, band=band, max_cost=max_cost, placement=placement)[0]
 
 
-def score(reference: Text, query: Text, costs: Union[Costs, Scoring], mode: Mode = Mode.GLOBAL, *,
-          placement=None) -> int:
-    if not isinstance(costs, Scoring):
-        raise ValueError("on the GPU, scores under a Scoring")
-    return scores([reference], [query], costs, mode, placement=placement)[0]
+def score(reference: Text, query: Text, costs: Union[Costs, Scoring] = Costs(), mode: Mode = Mode.GLOBAL, *,
+          band=None, placement=None) -> int:
+    """The score `align` would give: under a `Scoring` its score, under `Costs` minus the least cost."""
+    if isinstance(costs, Scoring):
+        if band is not None:
+            raise ValueError("a Scoring takes no band")
+        return scores([reference], [query], costs, mode, placement=placement)[0]
+    return -distance(reference, query, costs, mode, band=band, placement=placement)
 
 
-def align(reference: Text, query: Text, costs: Union[Costs, Scoring], mode: Mode = Mode.GLOBAL, *, eqx=True,
-          placement=None) -> Alignment:
-    return alignments([reference], [query], costs, mode, eqx=eqx, placement=placement)[0]
+def align(reference: Text, query: Text, costs: Union[Costs, Scoring] = Costs(), mode: Mode = Mode.GLOBAL, *,
+          band=None, max_cost=None, ties: str = "left", eqx=True, max_memory=None,
+          placement=None) -> Optional[Alignment]:
+    return alignments([reference], [query], costs, mode, band=band, max_cost=max_cost, ties=ties, eqx=eqx,
+                      max_memory=max_memory, placement=placement)[0]

@@ -107,6 +107,10 @@ def lib() -> ctypes.CDLL:
         handle.dinara_gpu_alignments_tape.argtypes = [vp, i64, vp, i64p, ctypes.POINTER(CScoring),
                                                       ctypes.POINTER(CMode), i64, i32p, i64p, i64p,
                                                       ctypes.POINTER(ctypes.c_void_p), i64p]
+        handle.dinara_gpu_cost_alignments_tape.restype = i64
+        handle.dinara_gpu_cost_alignments_tape.argtypes = [vp, i64, vp, i64p, ctypes.POINTER(CCosts),
+                                                           ctypes.POINTER(CMode), ctypes.POINTER(COptions), i64p, i64p,
+                                                           ctypes.POINTER(ctypes.c_void_p)]
         handle.dinara_gpu_distances_tape.restype = i64
         handle.dinara_gpu_distances_tape.argtypes = [vp, i64, vp, i64p, ctypes.POINTER(CBandPlan), i64p,
                                                      ctypes.POINTER(CBandReport)]

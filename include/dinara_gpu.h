@@ -129,6 +129,50 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
 void dinara_free(char *cigar);
 
 /*
+ * Global alignments under Costs, with the CIGAR the reference's Ties rule picks among equally good
+ * ones (replaces the reference's CPU-only `alignments(references, queries, costs)`, api.mojo:1415-1526
+ * -> least_costly api.mojo:622-716: edit_cigar, edit_distance.mojo:265-330, at unit costs with no cap;
+ * the gap-affine wavefront and its trace, gap_affine.mojo:858-1010 and 2028-2124, otherwise).
+ * `costs` is one gap piece (null for unit costs), deletions (reference letters alone) with costs of
+ * their own when deletion_extension is above zero; `mode` null or global; `options` null, or no band,
+ * `max_cost` (zero or more) a cap, `eqx`, and `right_ties` for Ties.RIGHT (WFA2-lib's backtrace from the
+ * far corner) instead of Ties.LEFT (the same over both sequences reversed). `max_memory` is read as
+ * unlimited: no pair is split, so a pair whose kept fronts would pass the reference's limit (80 MB by
+ * default) takes the unsplit trace. results[i] is pair i's least cost or its code: -1 a 0xFE or 0xFF
+ * byte, -4 past the cap, -2 fronts past the device budget. With `cigar_bytes` non-null, pair i's CIGAR
+ * is (*cigar_bytes)[cigar_offsets[i] .. cigar_offsets[i+1]) (dinara_free the buffer); null measures
+ * costs alone. A two-piece cost, a band or another mode fails the batch with DINARA_INVALID_MODE.
+ */
+int64_t dinara_gpu_cost_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                                        const dinara_costs *costs, const dinara_mode *mode,
+                                        const dinara_options *options, int64_t *results, int64_t *cigar_offsets,
+                                        char **cigar_bytes);
+
+/*
+ * The reference's own C entry points under its names and argument lists (c/dinara.h:141-228), so a C
+ * caller of the reference relinks against this library. They run on device 0 through a context the
+ * library opens at the first call and keeps; calls from several threads take turns on it, and `threads`
+ * is read as the device's own parallelism. Unit costs with no band or cap take band doubling (distances)
+ * and the unit-cost trace (alignments); other one-piece costs the wavefront. Globally only: free ends,
+ * extensions, local modes, bands and two-piece costs fail the batch with DINARA_INVALID_MODE. An
+ * alignment's CIGAR is freed with dinara_free; its span is the whole of both sequences.
+ */
+int64_t dinara_distance(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                        const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options);
+int64_t dinara_align(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                     const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options,
+                     dinara_alignment *alignment);
+int64_t dinara_score(const char *reference, int64_t reference_length, const char *query, int64_t query_length,
+                     const dinara_costs *costs, const dinara_mode *mode, const dinara_options *options, int64_t *score);
+int64_t dinara_distances(int64_t pairs, const char *const *references, const int64_t *reference_lengths,
+                         const char *const *queries, const int64_t *query_lengths, const dinara_costs *costs,
+                         const dinara_mode *mode, const dinara_options *options, int64_t threads, int64_t *results);
+int64_t dinara_alignments(int64_t pairs, const char *const *references, const int64_t *reference_lengths,
+                          const char *const *queries, const int64_t *query_lengths, const dinara_costs *costs,
+                          const dinara_mode *mode, const dinara_options *options, int64_t threads,
+                          dinara_alignment *alignments, int64_t *statuses);
+
+/*
  * Unit-cost global edit distances (replaces api.mojo:1216-1312 `distances(placement=on_gpu)` ->
  * `gpu_distances` -> device_edit.mojo:80-173, and the reference's CPU band doubling,
  * band.mojo:526-657, which its GPU path lacks). Costs must be unit (null, or {1,0,1,-1,0,...}), the

@@ -66,6 +66,36 @@ KNOWN = [
      "source": "tests/test_python.py:67; python/dinara_align/__init__.py:7-8"},
 ]
 
+# Alignments under Costs, the CIGAR the Ties rule names. `costs` is dinara_costs' nine fields in order;
+# `cost` None means past `max_cost`.
+UNIT = [1, 0, 1, -1, 0, 0, 0, -1, 0]
+AFFINE = [4, 6, 2, -1, 0, 0, 0, -1, 0]
+DEAR_DELETIONS = [4, 6, 2, -1, 0, 20, 5, -1, 0]
+KNOWN += [
+    {"kind": "costs", "reference": "ACGTACGTTTGCA", "query": "ACGTCGTTTTGCA", "costs": UNIT, "ties": "left",
+     "eqx": True, "cost": 2, "cigar": "4=1D2=1I6=", "source": "tests/test_python.py:71-72"},
+    {"kind": "costs", "reference": "ACGTACGTTTGCA", "query": "ACGTCGTTTTGCA", "costs": UNIT, "ties": "left",
+     "eqx": False, "cost": 2, "cigar": "4M1D2M1I6M", "source": "tests/test_python.py:73"},
+    {"kind": "costs", "reference": "ACGTTTTACG", "query": "ACGTTTACG", "costs": AFFINE, "ties": "left", "eqx": True,
+     "cost": 8, "cigar": "3=1D6=", "source": "tests/test_python.py:74; tests/test_alignment.mojo:2162"},
+    {"kind": "costs", "reference": "ACGTTTTACG", "query": "ACGTTTACG", "costs": AFFINE, "ties": "right",
+     "eqx": True, "cost": 8, "cigar": "6=1D3=", "source": "tests/test_python.py:75; tests/test_alignment.mojo:2163"},
+    {"kind": "costs", "reference": "ACGTTTTACG", "query": "ACGTTTACG", "costs": UNIT, "ties": "left", "eqx": True,
+     "cost": 1, "cigar": "3=1D6=", "source": "tests/test_alignment.mojo:2199"},
+    {"kind": "costs", "reference": "ACGTTTTACG", "query": "ACGTTTACG", "costs": UNIT, "ties": "right", "eqx": True,
+     "cost": 1, "cigar": "6=1D3=", "source": "tests/test_alignment.mojo:2222"},
+    {"kind": "costs", "reference": "ACGT", "query": "ACGT", "costs": UNIT, "ties": "left", "eqx": True, "cost": 0,
+     "cigar": "4=", "source": "tests/test_python.py:76"},
+    {"kind": "costs", "reference": "ACGTACGTTTGCA", "query": "ACGTCGTTTTGCA", "costs": AFFINE, "ties": "left",
+     "eqx": True, "max_cost": 11, "cost": None, "source": "tests/test_python.py:78"},
+    {"kind": "costs", "reference": "ACGTACGTTTGCA", "query": "ACGTCGTTTTGCA", "costs": AFFINE, "ties": "left",
+     "eqx": True, "max_cost": 12, "cost": 12, "cigar": "4=3X6=", "source": "tests/test_python.py:79, 81"},
+    {"kind": "costs", "reference": "ACGACGT", "query": "ACGTACGT", "costs": DEAR_DELETIONS, "ties": "left",
+     "eqx": True, "cost": 8, "source": "tests/test_python.py:85"},
+    {"kind": "costs", "reference": "ACGTACGT", "query": "ACGACGT", "costs": DEAR_DELETIONS, "ties": "left",
+     "eqx": True, "cost": 25, "source": "tests/test_python.py:86"},
+]
+
 
 def mutated(text: str, rate: float, rng: random.Random) -> str:
     """About `rate` of the letters substituted, deleted or followed by an inserted letter, a third each

@@ -49,3 +49,20 @@ def test_python_package_imports_without_gpu():
     assert dinara_align.Tape.of(["AC"], ["G"]).pairs == 1
     assert dinara_align.Costs.edit().unit_scale() == 1
     assert dinara_align.Costs.affine(4, 6, 2).unit_scale() == 0
+
+
+def test_sam_fields():
+    """An alignment's SAM fields from its CIGAR and span, with the reference's own answers
+    (tests/test_python.py:89-91): the clipped CIGAR, MD and NM."""
+    import dinara_align as da
+
+    core = da.Alignment(0, 14, "4=1X3=", 4, 12, 4, 12)
+    assert core.clipped_cigar(14) == "4S4=1X3=2S"
+    assert core.clipped_cigar(14, hard=True) == "4H4=1X3=2H"
+    assert core.mismatch_string("GGGGACGTACGTGGGG", "CCCCACGTTCGTCC") == "4A3"
+    assert core.edit_distance("GGGGACGTACGTGGGG", "CCCCACGTTCGTCC") == 1
+    gapped = da.Alignment(2, -2, "2=2D2=1I1=", 0, 7, 0, 6)
+    assert gapped.gapped("ACGTTGA", "ACTGCA") == ("ACGTTG-A", "AC--TGCA")
+    assert gapped.mismatch_string("ACGTTGA", "ACTGCA") == "2^GT3"
+    assert gapped.edit_distance("ACGTTGA", "ACTGCA") == 3
+    assert da.Costs.affine(4, 6, 2).with_deletions(20, 5).unit_scale() == 0 and da.Costs.linear(3, 3).unit_scale() == 3

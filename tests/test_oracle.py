@@ -19,6 +19,19 @@ def _scoring(entry):
     return table, len(entry["alphabet"]), entry["opening"] + entry["extension"], entry["extension"]
 
 
+def costs_cigar(oracle, a, b, entry):
+    """(cost, CIGAR) of a known answer under Costs: the unit-cost trace for unit costs with no cap (the
+    reference's edit_cigar), else the wavefront's."""
+    x, o, e, _o2, _e2, do, de, _do2, _de2 = entry["costs"]
+    right = entry["ties"] == "right"
+    cap = entry.get("max_cost", -1)
+    if o == 0 and x == e and de == 0 and cap < 0:
+        distance, cigar = oracle.edit_cigar(a, b, right=right, eqx=entry["eqx"])
+        return distance * x, cigar
+    return oracle.affine_cigar(a, b, x, o, e, do if de else None, de if de else None, max_cost=cap, right=right,
+                               eqx=entry["eqx"])
+
+
 def test_known_answers(oracle):
     """Every known answer the reference's tests give for this path (tests/golden/known_answers.json)."""
     known = json.load(open(os.path.join(GOLDEN, "known_answers.json")))
@@ -29,6 +42,12 @@ def test_known_answers(oracle):
             assert oracle.edit_distance_dp(a, b) == entry["distance"], entry
             assert oracle.myers_distance(a, b) == entry["distance"], entry
             assert oracle.band_doubling(a, b, 0)[0] == entry["distance"], entry
+            continue
+        if entry["kind"] == "costs":
+            cost, cigar = costs_cigar(oracle, a, b, entry)
+            assert cost == (-4 if entry["cost"] is None else entry["cost"]), entry
+            if "cigar" in entry:
+                assert cigar == entry["cigar"], entry
             continue
         table, size, op, ex = _scoring(entry["scoring"])
         mode = oracle.LOCAL if entry["mode"] == "local" else oracle.GLOBAL
@@ -233,3 +252,102 @@ def test_mlp_oracle_kmer_features():
     g = mlp_oracle.features(b"ACGTTGCAAC", b"ACGTAGCAAC")
     h = mlp_oracle.features(b"ACGTAGCAAC", b"ACGTTGCAAC")
     assert np.array_equal(g, h) and abs(g[:256].sum() - 32.0 * 8 / 10) < 1e-12
+
+
+def _runs(cigar):
+    out, length = [], 0
+    for letter in cigar:
+        if letter.isdigit():
+            length = length * 10 + int(letter)
+        else:
+            out.append((length, letter))
+            length = 0
+    return out
+
+
+def priced(cigar, reference, query, x, od, ed, oi, ei):
+    """What a CIGAR costs over the pair it spells, checking that it spells it: substitutions x, a run of k
+    reference letters alone od + k ed, of query letters oi + k ei (the reference's tests/test_python.py:
+    26-46 `rows_cost`)."""
+    total, i, j = 0, 0, 0
+    for length, op in _runs(cigar):
+        if op in "=XM":
+            for _ in range(length):
+                if op == "=":
+                    assert reference[i] == query[j]
+                if op == "X":
+                    assert reference[i] != query[j]
+                total += x if reference[i] != query[j] else 0
+                i, j = i + 1, j + 1
+        elif op == "D":
+            total += od + length * ed
+            i += length
+        else:
+            total += oi + length * ei
+            j += length
+    assert (i, j) == (len(reference), len(query))
+    return total
+
+
+def least_cost(a, b, x, od, ed, oi, ei):
+    """The least gap-affine cost by the plain three-layer dynamic program."""
+    big = 1 << 40
+    n, m = len(a), len(b)
+    H = [[big] * (m + 1) for _ in range(n + 1)]
+    D = [[big] * (m + 1) for _ in range(n + 1)]
+    I = [[big] * (m + 1) for _ in range(n + 1)]
+    H[0][0] = 0
+    for i in range(n + 1):
+        for j in range(m + 1):
+            if i > 0:
+                D[i][j] = min(H[i - 1][j] + od + ed, D[i - 1][j] + ed)
+            if j > 0:
+                I[i][j] = min(H[i][j - 1] + oi + ei, I[i][j - 1] + ei)
+            if i > 0 and j > 0:
+                H[i][j] = H[i - 1][j - 1] + (0 if a[i - 1] == b[j - 1] else x)
+            H[i][j] = min(H[i][j], D[i][j], I[i][j])
+    return H[n][m]
+
+
+def repeats(rng):
+    """A pair rich in ties: runs of a short unit between random letters, and a mutated copy (the shape of
+    the reference's tests/test_alignment.mojo:2023-2040 tie tests)."""
+    unit = "".join(rng.choice("ACGT") for _ in range(rng.randint(1, 4)))
+    core = "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 30)))
+    for _ in range(rng.randint(0, 5)):
+        core += unit * rng.randint(1, 3) + "".join(rng.choice("ACGT") for _ in range(rng.randint(0, 10)))
+    rate = rng.choice([0.03, 0.1, 0.25])
+    out = []
+    for letter in core:
+        roll = rng.random()
+        if roll < rate / 3:
+            out.append(rng.choice("ACGT"))
+        elif roll < 2 * rate / 3:
+            continue
+        elif roll < rate:
+            out.append(letter + rng.choice("ACGT"))
+        else:
+            out.append(letter)
+    return core, "".join(out)
+
+
+@pytest.mark.parametrize("costs", [(1, 0, 1, 0, 1), (4, 6, 2, 6, 2), (3, 1, 4, 1, 4), (4, 6, 2, 20, 5), (2, 2, 3, 0, 1)])
+def test_costs_cigars_are_optimal_and_follow_the_rule(oracle, costs):
+    """Under Costs the CIGAR prices at the least cost (a plain DP's) and spells the pair; Ties.LEFT is
+    Ties.RIGHT over both sequences reversed, read backwards (tests/test_alignment.mojo:2023-2200)."""
+    x, od, ed, oi, ei = costs
+    rng = random.Random(17 + sum(costs))
+    unit = costs == (1, 0, 1, 0, 1)
+    for _ in range(150):
+        reference, query = repeats(rng)
+        expected = least_cost(reference, query, x, od, ed, oi, ei)
+        for right in (False, True):
+            cost, cigar = oracle.affine_cigar(reference, query, x, oi, ei, od, ed, right=right)
+            assert cost == expected
+            assert priced(cigar, reference, query, x, od, ed, oi, ei) == expected
+            mirrored = oracle.affine_cigar(reference[::-1], query[::-1], x, oi, ei, od, ed, right=not right)[1]
+            assert "".join(f"{n}{op}" for n, op in reversed(_runs(mirrored))) == cigar
+            if unit:
+                # The unit-cost trace (edit_cigar) and the wavefront's agree, as the reference asserts for
+                # a capped search against an uncapped one (tests/test_alignment.mojo:2212-2218).
+                assert oracle.edit_cigar(reference, query, right=right) == (cost, cigar)
