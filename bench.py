@@ -2,8 +2,8 @@
 
 Headline workload (default `uneven`, the metric's own comparison): 200,000 synthetic pairs, lengths
 log-uniform 100 bp-20 kbp, per-pair error rate uniform 0.5-15% (substitutions/insertions/deletions
-50/25/25), global unit-cost edit distances by band doubling. The learned band (a 257-64-64-1 network over
-4-mer count differences, trained first on the GPU on 1,000,000 pairs of the same distribution, whose exact
+50/25/25), global unit-cost edit distances by band doubling. The learned band (a 258-64-64-1 network over
+4-mer count differences and a 6-mer sketch, trained first on the GPU on 1,000,000 pairs of the same distribution, whose exact
 distances plain band doubling measures) sets each pair's first threshold; plain band doubling from the
 default band is run beside it as the judge, and both must give the same distance on every pair.
 
@@ -319,12 +319,20 @@ def coded(tape):
 # The CPU legs: the oracle (a C restatement of the reference's CPU algorithms) on the host's cores.
 
 
-def cpu_measure(workload: str, threads: int, runs: int) -> dict:
-    """The oracle timed on `threads` host threads over a bounded sample of the workload: pairs/s."""
+def cpu_measure(workload: str, threads: int, runs: int, gotoh: bool = False) -> dict:
+    """The oracle timed on `threads` host threads over a bounded sample of the workload: pairs/s. For the
+    global affine workload the reference's host path for a uniform Scoring is the gap-affine wavefront
+    (scoring.mojo:414-440), restated in the oracle; `gotoh` times the full-matrix Gotoh walk instead."""
     oracle = oracle_module()
     tape = make_workload(workload, CPU_SAMPLE[workload], seed=1000)
     letters = tape.letters[: tape.offsets[-1]]
-    if workload == "affine":
+    if workload == "affine" and not gotoh:
+        what = ("the gap-affine wavefront's costs and CIGARs under Costs.affine(4,6,2), one search from the start "
+                "traced back (gap_affine.mojo:858-1010, 2028-2124), the reference's host path for a uniform Scoring")
+
+        def run():
+            oracle.batch_wavefront(letters, tape.offsets, 4, 6, 2, threads=threads)
+    elif workload == "affine":
         table, (op, ex) = oracle.dna_table(0, -4), oracle.kernel_gaps(-6, -2)
         what = "full-matrix Gotoh scores and the walk's CIGARs (gotoh.mojo:285-510)"
 
@@ -684,6 +692,8 @@ def run_workload(ctx, workload: str, pairs: int, steps: int, warmup: int, cpu: b
                       "parallelism": f"pairs sharded, {ctx['ranks'].world} independent ranks"}
     if cpu and ctx["ranks"].rank == 0:
         line["cpu_baseline"] = cpu_measure(workload, os.cpu_count() or 1, 1 if workload != "unit250" else 3)
+        if workload == "affine":
+            line["cpu_baseline_gotoh"] = cpu_measure(workload, os.cpu_count() or 1, 1, gotoh=True)
     return line
 
 

@@ -1,8 +1,9 @@
-// The learned band: a small network that reads a pair's 4-mer sketch and predicts its edit distance, so
+// The learned band: a small network that reads a pair's k-mer sketch and predicts its edit distance, so
 // band doubling starts near the answer instead of at the default threshold (band.mojo:521 starts an
-// untrusted band 256 past what it knows). The network is 257 -> 64 -> 64 -> 1, fp32, ReLU: its input the
-// 256 counts of each 4-mer in the reference less those in the query, over the pair's mean length, and
-// the length ratio; its output the distance over the mean length. Nothing about the answer depends on
+// untrusted band 256 past what it knows). The network is 258 -> 64 -> 64 -> 1, fp32, ReLU: its input the
+// 256 counts of each 4-mer in the reference less those in the query (squared, over the pair's mean
+// length), the length ratio, and the 6-mer count differences' squares summed over the mean length; its
+// output the distance over the mean length. Nothing about the answer depends on
 // it: a low guess costs extra doublings, a high one a wider band, and the doubling that follows is the
 // reference's.
 //
@@ -128,101 +129,235 @@ __device__ __forceinline__ uint32_t reversed_kmer(uint32_t k) {
     return ((k & 3u) << 6) | (((k >> 2) & 3u) << 4) | (((k >> 4) & 3u) << 2) | ((k >> 6) & 3u);
 }
 
-// A warp's 4-mer counts of one sequence into `counts` (shared, 256 ints, indexed with the first letter in
-// the lowest bits), `sign` +1 or -1; a 4-mer holding another letter is skipped.
-__device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, int *counts) {
-    // The warp reads the sequence 512 letters at a time, lane i the 4-mers starting at the 16 letters from
-    // 16i, through six aligned words that hold those letters and the three after them (a word may reach
-    // three bytes past the sequence's end: device letter buffers keep 16 bytes of room there).
-    const int lane = threadIdx.x & 31;
+// A warp's 6-mer counts of one sequence into `sixes` (shared, 4096 ints, a 6-mer's letters' 2-bit codes
+// with the first letter in the lowest bits), `sign` +1 or -1; a 6-mer holding another letter is skipped.
+// The 4-mer counts follow from them (a 4-mer is the first four letters of the 6-mer starting with it),
+// save where a 4-mer starts no valid 6-mer (the sequence's last two 4-mers, or one whose fifth or sixth
+// letter is another letter): those go into `fours` (256 ints, the same order) directly.
+// Adds `sign` to 6-mer bin `bin`.
+template <bool WIDE>
+__device__ __forceinline__ void add_six(unsigned *sixes, uint32_t bin, int sign) {
+    if (WIDE) {
+        atomicAdd(&sixes[bin], unsigned(sign));
+        return;
+    }
+    // Two 16-bit bins a word, each held as 32,768 plus its count difference. Neither sequence has more
+    // than kNarrowLimit letters, so in whatever order they are added no half passes 65,535 or falls below
+    // zero, and no add reaches the other half.
+    atomicAdd(&sixes[bin >> 1], unsigned(sign) << (16 * (bin & 1u)));
+}
+
+template <bool WIDE>
+__device__ __forceinline__ int six_at(const unsigned *sixes, uint32_t bin) {
+    if (WIDE) return int(sixes[bin]);
+    return int((sixes[bin >> 1] >> (16 * (bin & 1u))) & 0xFFFFu) - 32768;
+}
+
+template <bool WIDE>
+__device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, unsigned *sixes, int *fours,
+                            int64_t slot) {
+    // One slot of 16 letters: the 6-mers starting at letters 16 slot .. 16 slot + 15, read through seven
+    // aligned words that hold those letters and the five after them (a word may reach three bytes past
+    // the sequence's end: device letter buffers keep 16 bytes of room there).
     const uintptr_t origin = reinterpret_cast<uintptr_t>(sequence);
     const uintptr_t end = origin + uintptr_t(length);
-    for (int64_t chunk = 0; chunk < length; chunk += 512) {
-        const int64_t first = chunk + 16 * lane;
-        if (first >= length) continue;
+    {
+        const int64_t first = 16 * slot;
         const uintptr_t address = origin + uintptr_t(first);
         const uintptr_t aligned = address & ~uintptr_t(3);
         const uint32_t *words = reinterpret_cast<const uint32_t *>(aligned);
-        uint32_t w[6];
+        uint32_t w[7];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) w[i] = aligned + 4 * uintptr_t(i) < end ? __ldg(words + i) : 0u;
+        for (int i = 0; i < 7; ++i) w[i] = aligned + 4 * uintptr_t(i) < end ? __ldg(words + i) : 0u;
         const uint32_t shift = uint32_t(address & 3u) * 8u;
-        uint32_t a[5];
+        uint32_t a[6];
 #pragma unroll
-        for (int i = 0; i < 5; ++i) a[i] = __funnelshift_r(w[i], w[i + 1], shift);
-        if (first + 19 <= length) {
-            // The lane's 19 letters, four a word at once: each byte's 2-bit code, the letters rebuilt from
+        for (int i = 0; i < 6; ++i) a[i] = __funnelshift_r(w[i], w[i + 1], shift);
+        if (first + 21 <= length) {
+            // The lane's 21 letters, four a word at once: each byte's 2-bit code, the letters rebuilt from
             // the codes (A, C, G, T by a byte permute) to check that every byte was one of the four, and
             // the codes packed two bits a letter, the first letter lowest.
             bool valid = true;
             uint64_t packed = 0;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
+            for (int q = 0; q < 6; ++q) {
                 const uint32_t c = ((a[q] >> 1) & 0x03030303u) ^ ((a[q] >> 2) & 0x01010101u);
                 const uint32_t t = c | (c >> 4);
                 const uint32_t rebuilt = __byte_perm(0x54474341u, 0u, (t & 0xFFu) | ((t >> 8) & 0xFF00u));
-                const uint32_t used = q < 4 ? 0xFFFFFFFFu : 0x00FFFFFFu;  // 16 + 3 letters
+                const uint32_t used = q < 5 ? 0xFFFFFFFFu : 0x000000FFu;  // 16 + 5 letters
                 valid = valid && ((rebuilt ^ a[q]) & used) == 0u;
                 const uint32_t x = c | (c >> 6);
                 packed |= uint64_t((x & 0xFu) | ((x >> 12) & 0xF0u)) << (8 * q);
             }
             if (valid) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) atomicAdd(&counts[uint32_t(packed >> (2 * j)) & 0xFFu], sign);
-                continue;
+                for (int j = 0; j < 16; ++j) add_six<WIDE>(sixes, uint32_t(packed >> (2 * j)) & 0xFFFu, sign);
+                return;
             }
         }
-        // Near the sequence's end or another letter in reach: letter by letter.
+        // Near the sequence's end or another letter in reach: letter by letter. `run` counts the valid
+        // letters ending at j; the 6-mer (or, failing it, the 4-mer) starting at j - 5 (j - 3) is counted
+        // once its letters are all in hand.
         uint32_t kmer = 0;
         int run = 0;
 #pragma unroll
-        for (int j = 0; j < 19; ++j) {
+        for (int j = 0; j < 21; ++j) {
             const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
-            kmer = (kmer >> 2) | (uint32_t(c & 3) << 6);
+            kmer = (kmer >> 2) | (uint32_t(c & 3) << 10);
             run = c < 0 ? 0 : run + 1;
-            if (j >= 3 && run >= 4) atomicAdd(&counts[kmer], sign);
+            if (j >= 5 && j - 5 < 16 && run >= 6) add_six<WIDE>(sixes, kmer, sign);
+        }
+        // 4-mers starting at the lane's 16 places with no valid 6-mer from the same place.
+        run = 0;
+        int valid_from[21];
+#pragma unroll
+        for (int j = 20; j >= 0; --j) {
+            const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
+            run = c < 0 ? 0 : run + 1;
+            valid_from[j] = run;  // valid letters from j on
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (valid_from[j] >= 4 && valid_from[j] < 6) {
+                uint32_t four = 0;
+#pragma unroll
+                for (int q = 3; q >= 0; --q)
+                    four = (four << 2) | uint32_t(code_of((a[(j + q) >> 2] >> (8 * ((j + q) & 3))) & 0xFFu) & 3);
+                atomicAdd(&fours[four], sign);
+            }
         }
     }
 }
 
-// Writes a pair's 257 features, scaled as the network reads them: each count difference squared, times
-// 32 over the mean length, since an error moves a handful of 4-mers between bins and the squares of the
-// differences then sum to about eight times the errors whether a bin holds one move or many of either
-// sign, so their sum over the length tracks the error rate; and the length ratio.
-__device__ void features_of(const int *counts, int64_t reference, int64_t query, float *out, int stride) {
+// Writes a pair's 258 features, scaled as the network reads them. The first 256: each 4-mer count
+// difference squared, times 32 over the mean length, since an error moves a handful of 4-mers between
+// bins and the squares of the differences then sum to about eight times the errors whether a bin holds
+// one move or many of either sign, so their sum over the length tracks the error rate. Then the length
+// ratio. Then the 6-mer count differences' squares summed over their 4,096 bins, over the mean length:
+// the same measure with sixteen times the bins, whose noise from moves sharing a bin is a quarter of
+// the 4-mers' (about 3.6% against 11% of a 4 kbp pair's distance).
+template <bool WIDE>
+__device__ void features_of(const unsigned *sixes, const int *fours, int64_t reference, int64_t query, float *out,
+                            int stride) {
     const int lane = threadIdx.x & 31;
     const float mean = 0.5f * float(reference + query);
     const float scale = 32.0f / (mean > 1.0f ? mean : 1.0f);
     for (int k = lane; k < 256; k += 32) {
-        const float difference = float(counts[reversed_kmer(uint32_t(k))]);
+        // Feature k's 4-mer has its first letter in the highest bits; the counts, in the lowest.
+        const uint32_t four = reversed_kmer(uint32_t(k));
+        int count = fours[four];
+#pragma unroll
+        for (int y = 0; y < 16; ++y) count += six_at<WIDE>(sixes, four | (uint32_t(y) << 8));
+        const float difference = float(count);
         out[int64_t(k) * stride] = difference * difference * scale;
     }
+    long long squares = 0;
+    for (int b = lane; b < 4096; b += 32) {
+        const long long v = six_at<WIDE>(sixes, uint32_t(b));
+        squares += v * v;
+    }
+#pragma unroll
+    for (int span = 16; span > 0; span >>= 1) squares += __shfl_xor_sync(0xffffffffu, squares, span);
     if (lane == 0) {
         const int64_t low = min(reference, query), high = max(reference, query);
         out[int64_t(256) * stride] = high > 0 ? float(low) / float(high) : 1.0f;
+        out[int64_t(257) * stride] = float(double(squares) / double(mean > 1.0f ? mean : 1.0f));
     }
 }
 
-// A warp a pair: the features into a matrix, feature f of pair p at f * pairs + p (feature-major, as
-// training reads them) or at p * kIn + f (pair-major, as prediction does).
-__global__ void features_kernel(const uint8_t *letters, const int64_t *offsets, int64_t pairs, float *features,
-                                bool pair_major) {
-    __shared__ int counts[8][256];
-    const int warp_in_block = threadIdx.x >> 5;
-    const int64_t pair = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp_in_block;
+// The sketch kernel's warps each take one pair at a time from a queue, its counts in the warp's own
+// shared memory: 4,096 6-mer bins (two 16-bit bins a word, or a word each for pairs with a side past
+// kNarrowLimit letters) and 256 4-mer ints. No warp waits for another, so a long pair holds up nothing.
+constexpr int kSketchWarps = 4;
+constexpr int kSketchNarrowWords = 2048 + 256;
+constexpr int kSketchWideWords = 4096 + 256;
+constexpr int64_t kNarrowLimit = 32000;
+
+template <bool WIDE>
+constexpr size_t sketch_shared_bytes() {
+    return size_t(kSketchWarps) * size_t(WIDE ? kSketchWideWords : kSketchNarrowWords) * sizeof(unsigned);
+}
+
+// Persistent warps, each taking its next pair from a queue: pair `order[item]` (or pair item itself with
+// no order). The features into a matrix, feature f of pair p at f * pairs + p (feature-major, as training
+// reads them) or at p * kIn + f (pair-major, as prediction does). The narrow form skips pairs with a side
+// past kNarrowLimit letters, which the wide form takes.
+template <bool WIDE>
+__global__ void __launch_bounds__(32 * kSketchWarps) features_kernel(const uint8_t *letters, const int64_t *offsets,
+                                                                      int64_t pairs, const uint32_t *order,
+                                                                      int64_t count, unsigned *queue, float *features,
+                                                                      bool pair_major) {
+    extern __shared__ unsigned sketch_counts[];
+    constexpr int kWords = WIDE ? kSketchWideWords : kSketchNarrowWords;
     const int lane = threadIdx.x & 31;
-    int *mine = counts[warp_in_block];
-    for (int k = lane; k < 256; k += 32) mine[k] = 0;
-    __syncwarp();
-    if (pair < pairs) {
+    unsigned *sixes = sketch_counts + (threadIdx.x >> 5) * kWords;
+    int *fours = reinterpret_cast<int *>(sixes + (WIDE ? 4096 : 2048));
+    for (;;) {
+        unsigned item = 0;
+        if (lane == 0) item = atomicAdd(queue, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= count) return;
+        const int64_t pair = order ? int64_t(order[item]) : int64_t(item);
         const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
-        count_kmers(letters + r0, q0 - r0, 1, mine);
-        count_kmers(letters + q0, q1 - q0, -1, mine);
+        const int64_t reference = q0 - r0, query = q1 - q0;
+        if (!WIDE && (reference > kNarrowLimit || query > kNarrowLimit)) continue;  // the wide form's
+        for (int k = lane; k < kWords; k += 32) sixes[k] = (WIDE || k >= 2048) ? 0u : 0x80008000u;
+        __syncwarp();
+        // Both sequences' 16-letter slots in one run, the reference's (+1) then the query's (-1).
+        const int64_t reference_slots = (reference + 15) / 16, slots = reference_slots + (query + 15) / 16;
+        for (int64_t slot = lane; slot < slots; slot += 32) {
+            if (slot < reference_slots)
+                count_kmers<WIDE>(letters + r0, reference, 1, sixes, fours, slot);
+            else
+                count_kmers<WIDE>(letters + q0, query, -1, sixes, fours, slot - reference_slots);
+        }
+        __syncwarp();
+        features_of<WIDE>(sixes, fours, reference, query, pair_major ? features + pair * kIn : features + pair,
+                          pair_major ? 1 : int(pairs));
+        __syncwarp();
     }
-    __syncwarp();
-    if (pair < pairs)
-        features_of(mine, offsets[2 * pair + 1] - offsets[2 * pair], offsets[2 * pair + 2] - offsets[2 * pair + 1],
-                    pair_major ? features + pair * kIn : features + pair, pair_major ? 1 : int(pairs));
+}
+
+// The pairs with a side past kNarrowLimit letters, for the wide form.
+__global__ void wide_pairs_kernel(const int64_t *offsets, int64_t pairs, uint32_t *wide, unsigned *count) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= pairs) return;
+    if (offsets[2 * p + 1] - offsets[2 * p] > kNarrowLimit || offsets[2 * p + 2] - offsets[2 * p + 1] > kNarrowLimit)
+        wide[atomicAdd(count, 1u)] = uint32_t(p);
+}
+
+void launch_features(dinara_gpu *gpu, const uint8_t *letters, const int64_t *offsets, int64_t pairs, float *features,
+                     bool pair_major) {
+    cudaStream_t stream = gpu->stream;
+    unsigned *counts = reinterpret_cast<unsigned *>(gpu->counters.ensure<unsigned int>(64) + 56);  // [0] wide, [1..2] queues
+    DINARA_CUDA(cudaMemsetAsync(counts, 0, 3 * sizeof(unsigned), stream));
+    int per_sm = 0;
+    DINARA_CUDA(cudaFuncSetAttribute(features_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(sketch_shared_bytes<false>())));
+    DINARA_CUDA(cudaFuncSetAttribute(features_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(sketch_shared_bytes<true>())));
+    DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, features_kernel<false>, 32 * kSketchWarps,
+                                                              sketch_shared_bytes<false>()));
+    int64_t blocks = std::min<int64_t>(int64_t(std::max(per_sm, 1)) * gpu->multiprocessors,
+                                       (pairs + kSketchWarps - 1) / kSketchWarps);
+    features_kernel<false><<<unsigned(std::max<int64_t>(blocks, 1)), 32 * kSketchWarps, sketch_shared_bytes<false>(),
+                             stream>>>(letters, offsets, pairs, nullptr, pairs, counts + 1, features, pair_major);
+    DINARA_CUDA(cudaGetLastError());
+    // The few pairs past the narrow bins' reach, again with a word a bin.
+    uint32_t *wide = gpu->keys.ensure<uint32_t>(size_t(pairs) + 1);
+    wide_pairs_kernel<<<unsigned((pairs + 255) / 256), 256, 0, stream>>>(offsets, pairs, wide, counts);
+    DINARA_CUDA(cudaGetLastError());
+    unsigned wide_count = 0;
+    read_back(gpu, &wide_count, counts, sizeof wide_count);
+    if (wide_count > 0) {
+        DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, features_kernel<true>, 32 * kSketchWarps,
+                                                                  sketch_shared_bytes<true>()));
+        blocks = std::min<int64_t>(int64_t(std::max(per_sm, 1)) * gpu->multiprocessors,
+                                   (int64_t(wide_count) + kSketchWarps - 1) / kSketchWarps);
+        features_kernel<true><<<unsigned(std::max<int64_t>(blocks, 1)), 32 * kSketchWarps, sketch_shared_bytes<true>(),
+                                stream>>>(letters, offsets, pairs, wide, wide_count, counts + 2, features, pair_major);
+        DINARA_CUDA(cudaGetLastError());
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -480,10 +615,8 @@ size_t work_floats(int batch) { return size_t(batch) * (4 * kH + 2) + 64; }
 
 void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
                         float *features) {
-    const int threads = 256;
-    features_kernel<<<unsigned((pairs + 7) / 8), threads, 0, gpu->stream>>>(letters, offsets, pairs, features, false);
-    gpu->launches += 1;
-    DINARA_CUDA(cudaGetLastError());
+    launch_features(gpu, letters, offsets, pairs, features, false);
+    gpu->launches += 2;
 }
 
 void predictor_gradients(dinara_gpu *gpu, int batch, const float *features, const float *targets, float *grads,
@@ -498,12 +631,8 @@ const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t 
     if (!gpu->predictor_ready) throw Failure(DINARA_INVALID_MODE, "no trained band predictor on this context");
     int64_t *thresholds = gpu->predictions.ensure<int64_t>(size_t(pairs));
     float *predicted = gpu->targets.ensure<float>(size_t(pairs));
-    static bool configured = false;
     const size_t shared = predict_shared_bytes();
-    if (!configured) {
-        DINARA_CUDA(cudaFuncSetAttribute(predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared)));
-        configured = true;
-    }
+    DINARA_CUDA(cudaFuncSetAttribute(predict_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared)));
     int per_sm = 0;
     DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, predict_kernel, 256, shared));
     int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
@@ -513,9 +642,8 @@ const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t 
     // The sketches first, a warp a pair at full occupancy (reading the letters is the slow part), then the
     // network from them with its weights in shared memory.
     float *sketches = gpu->sketches.ensure<float>(size_t(pairs) * kIn);
-    features_kernel<<<unsigned((pairs + 7) / 8), 256, 0, gpu->stream>>>(letters, offsets, pairs, sketches, true);
-    DINARA_CUDA(cudaGetLastError());
-    gpu->launches += 1;
+    launch_features(gpu, letters, offsets, pairs, sketches, true);
+    gpu->launches += 2;
     predict_kernel<<<unsigned(std::max<int64_t>(blocks, 1)), 256, shared, gpu->stream>>>(
         sketches, offsets, pairs, gpu->weights.as<float>(), margins, float(gpu->predictor_slack), thresholds, predicted);
     DINARA_CUDA(cudaGetLastError());

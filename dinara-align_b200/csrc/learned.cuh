@@ -5,9 +5,10 @@
 
 namespace dinara {
 
-constexpr int kPredictorInputs = 257;  // 256 4-mer count differences and the length ratio
+// 256 4-mer count differences, the length ratio and the 6-mer squared count differences' sum.
+constexpr int kPredictorInputs = 258;
 constexpr int kPredictorHidden = 64;
-// w1 [257][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3 [1], flat in that order.
+// w1 [258][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3 [1], flat in that order.
 constexpr int kPredictorParameters =
     kPredictorInputs * kPredictorHidden + kPredictorHidden + kPredictorHidden * kPredictorHidden + kPredictorHidden +
     kPredictorHidden + 1;
@@ -16,7 +17,7 @@ constexpr int kPredictorParameters =
 void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets, float *features);
 
 // One batch's gradients of the summed squared error over the mean, for the context's parameters: the
-// features feature-major ([257][batch]), targets, gradients and the squared error's sum on the device.
+// features feature-major ([258][batch]), targets, gradients and the squared error's sum on the device.
 void predictor_gradients(dinara_gpu *gpu, int batch, const float *features, const float *targets, float *grads,
                          float *loss);
 

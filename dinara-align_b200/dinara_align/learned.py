@@ -12,8 +12,9 @@ import numpy as np
 from . import Placement, Tape, _placement
 from . import _native as native
 
-PARAMETERS = 20737
-VERSION = 2
+PARAMETERS = 20801
+INPUTS = 258
+VERSION = 3
 
 
 class TrainOptions(ctypes.Structure):
@@ -98,7 +99,7 @@ class Predictor:
         """A versioned blob: the parameters, the margins and slack, and the training seed."""
         flat, margin, slack = self.parameters()
         meta = json.dumps({"version": VERSION, "seed": self.seed, "margin": margin, "margins": self.margins(),
-                           "slack": slack, "features": "squared 4-mer count differences x 32 / mean length"})
+                           "slack": slack, "features": "squared 4-mer count differences x 32 / mean length, length ratio, summed squared 6-mer count differences / mean length"})
         np.savez(path, parameters=flat, meta=np.frombuffer(meta.encode(), dtype=np.uint8))
 
     def load(self, path: str) -> None:
@@ -111,7 +112,7 @@ class Predictor:
         self.seed = meta.get("seed")
 
     def features(self, tape: Tape) -> np.ndarray:
-        out = np.zeros((max(tape.pairs, 1), 257), dtype=np.float32)
+        out = np.zeros((max(tape.pairs, 1), INPUTS), dtype=np.float32)
         native.check(self.lib.dinara_gpu_predictor_features(self.handle, tape.pairs, tape.letters.ctypes.data,
                                                             native.pointer(tape.offsets, ctypes.c_int64),
                                                             native.pointer(out, ctypes.c_float)), self.handle)

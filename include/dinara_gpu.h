@@ -216,13 +216,14 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
                                   const dinara_band_plan *plan, int64_t *results, dinara_band_report *report);
 
 /*
- * The learned band predictor (no reference counterpart): a 257 -> 64 -> 64 -> 1 fp32 network over a
- * pair's 4-mer count differences and length ratio, predicting its distance over its mean length; band
+ * The learned band predictor (no reference counterpart): a 258 -> 64 -> 64 -> 1 fp32 network over a
+ * pair's 4-mer count differences, its length ratio and the sum of its squared 6-mer count differences,
+ * predicting its distance over its mean length; band
  * doubling with DINARA_BAND_LEARNED starts each pair at the prediction times the margin plus the slack,
  * never below the length difference. Parameters are one flat vector of DINARA_PREDICTOR_PARAMETERS
- * floats: w1 [257][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3.
+ * floats: w1 [258][64], b1 [64], w2 [64][64], b2 [64], w3 [64], b3.
  */
-#define DINARA_PREDICTOR_PARAMETERS 20737
+#define DINARA_PREDICTOR_PARAMETERS 20801
 
 typedef struct {
     uint64_t seed;          /* the training pairs' generator seed */
@@ -259,10 +260,12 @@ int64_t dinara_gpu_predictor_get(dinara_gpu *gpu, float *parameters, double *mar
  * pairs; dinara_gpu_predictor_set sets all four to its one margin. */
 int64_t dinara_gpu_predictor_margins(dinara_gpu *gpu, int64_t set, double *margins);
 
-/* The 257 features of each pair of a tape, pair-major into `features` (pairs x 257 floats). */
+/* The 258 features of each pair of a tape, pair-major into `features` (pairs x 258 floats): the 256 4-mer
+ * count differences squared times 32 over the mean length, the length ratio, and the 6-mer count
+ * differences' squares summed over the mean length. */
 int64_t dinara_gpu_predictor_features(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
                                       float *features);
-/* One batch's gradients for the installed parameters: features pair-major (batch x 257), targets
+/* One batch's gradients for the installed parameters: features pair-major (batch x 258), targets
  * (distance over mean length); the gradient of the mean squared error into `gradients`, and the mean
  * squared error into *loss. For checking the training kernels against another implementation. */
 int64_t dinara_gpu_predictor_gradients(dinara_gpu *gpu, int64_t batch, const float *features, const float *targets,

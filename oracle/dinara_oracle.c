@@ -484,156 +484,6 @@ int32_t oracle_score_reach_refuses(const int8_t *table, int32_t size, int32_t op
 }
 
 /* ---------------------------------------------------------------------------------------------- */
-/* Batches on host threads, longest pair first                                                     */
-/* ---------------------------------------------------------------------------------------------- */
-
-typedef struct {
-    int64_t pairs;
-    const uint8_t *tape;
-    const int64_t *offsets;
-    const int8_t *table;
-    int32_t size, open, extend, mode, eqx;
-    int64_t start;
-    int kind; /* 0 scores, 1 alignments, 2 distances */
-    int32_t *scores;
-    char *cigars;
-    int64_t cigar_stride;
-    int64_t *cigar_lengths;
-    int64_t *distances;
-    const int64_t *order;
-    atomic_llong next;
-} batch_job;
-
-static void run_pair(batch_job *job, int64_t p) {
-    const uint8_t *first = job->tape + job->offsets[2 * p];
-    const uint8_t *second = job->tape + job->offsets[2 * p + 1];
-    int64_t rows = job->offsets[2 * p + 1] - job->offsets[2 * p];
-    int64_t columns = job->offsets[2 * p + 2] - job->offsets[2 * p + 1];
-    if (job->kind == 0) {
-        job->scores[p] = oracle_gotoh_score(first, rows, second, columns, job->table, job->size, job->open,
-                                            job->extend, job->mode, NULL, NULL);
-    } else if (job->kind == 1) {
-        uint8_t *top = (uint8_t *)malloc((size_t)(rows + columns + 1));
-        uint8_t *bottom = (uint8_t *)malloc((size_t)(rows + columns + 1));
-        int64_t length = 0;
-        job->scores[p] = oracle_gotoh_align(first, rows, second, columns, job->table, job->size, job->open,
-                                            job->extend, job->mode, top, bottom, &length);
-        char *cigar = (char *)malloc((size_t)(2 * length + 2));
-        int64_t written = oracle_cigar(top, bottom, length, job->eqx, cigar);
-        char *slot = job->cigars + p * job->cigar_stride;
-        if (written < job->cigar_stride) {
-            memcpy(slot, cigar, (size_t)written + 1);
-            job->cigar_lengths[p] = written;
-        } else {
-            memcpy(slot, cigar, (size_t)job->cigar_stride - 1);
-            slot[job->cigar_stride - 1] = 0;
-            job->cigar_lengths[p] = -1;
-        }
-        free(cigar);
-        free(top);
-        free(bottom);
-    } else {
-        job->distances[p] = job->start < 0 ? oracle_myers_distance(first, rows, second, columns)
-                                           : oracle_band_doubling(first, rows, second, columns, job->start, NULL,
-                                                                  NULL);
-    }
-}
-
-static void *batch_worker(void *argument) {
-    batch_job *job = (batch_job *)argument;
-    for (;;) {
-        long long k = atomic_fetch_add(&job->next, 1);
-        if (k >= job->pairs) break;
-        run_pair(job, job->order[k]);
-    }
-    return NULL;
-}
-
-static const int64_t *batch_offsets_for_sort;
-static int by_cells_descending(const void *x, const void *y) {
-    int64_t a = *(const int64_t *)x, b = *(const int64_t *)y;
-    const int64_t *o = batch_offsets_for_sort;
-    int64_t ca = (o[2 * a + 1] - o[2 * a] + 1) * (o[2 * a + 2] - o[2 * a + 1] + 1);
-    int64_t cb = (o[2 * b + 1] - o[2 * b] + 1) * (o[2 * b + 2] - o[2 * b + 1] + 1);
-    if (ca != cb) return ca > cb ? -1 : 1;
-    return a < b ? -1 : (a > b);
-}
-
-static pthread_mutex_t sort_lock = PTHREAD_MUTEX_INITIALIZER;
-
-static void run_batch(batch_job *job, int32_t threads) {
-    int64_t *order = (int64_t *)malloc((size_t)(job->pairs > 0 ? job->pairs : 1) * sizeof(int64_t));
-    for (int64_t p = 0; p < job->pairs; ++p) order[p] = p;
-    pthread_mutex_lock(&sort_lock);
-    batch_offsets_for_sort = job->offsets;
-    qsort(order, (size_t)job->pairs, sizeof(int64_t), by_cells_descending);
-    pthread_mutex_unlock(&sort_lock);
-    job->order = order;
-    atomic_init(&job->next, 0);
-    if (threads <= 1) {
-        batch_worker(job);
-    } else {
-        pthread_t *pool = (pthread_t *)malloc((size_t)threads * sizeof(pthread_t));
-        for (int32_t k = 0; k < threads; ++k) pthread_create(&pool[k], NULL, batch_worker, job);
-        for (int32_t k = 0; k < threads; ++k) pthread_join(pool[k], NULL);
-        free(pool);
-    }
-    free(order);
-}
-
-void oracle_batch_scores(int64_t pairs, const uint8_t *tape, const int64_t *offsets, const int8_t *table,
-                         int32_t size, int32_t open, int32_t extend, int32_t mode, int32_t threads, int32_t *results) {
-    batch_job job;
-    memset(&job, 0, sizeof job);
-    job.pairs = pairs;
-    job.tape = tape;
-    job.offsets = offsets;
-    job.table = table;
-    job.size = size;
-    job.open = open;
-    job.extend = extend;
-    job.mode = mode;
-    job.kind = 0;
-    job.scores = results;
-    run_batch(&job, threads);
-}
-
-void oracle_batch_alignments(int64_t pairs, const uint8_t *tape, const int64_t *offsets, const int8_t *table,
-                             int32_t size, int32_t open, int32_t extend, int32_t mode, int32_t eqx, int32_t threads,
-                             int32_t *results, char *cigars, int64_t cigar_stride, int64_t *cigar_lengths) {
-    batch_job job;
-    memset(&job, 0, sizeof job);
-    job.pairs = pairs;
-    job.tape = tape;
-    job.offsets = offsets;
-    job.table = table;
-    job.size = size;
-    job.open = open;
-    job.extend = extend;
-    job.mode = mode;
-    job.eqx = eqx;
-    job.kind = 1;
-    job.scores = results;
-    job.cigars = cigars;
-    job.cigar_stride = cigar_stride;
-    job.cigar_lengths = cigar_lengths;
-    run_batch(&job, threads);
-}
-
-void oracle_batch_distances(int64_t pairs, const uint8_t *tape, const int64_t *offsets, int64_t start,
-                            int32_t threads, int64_t *results) {
-    batch_job job;
-    memset(&job, 0, sizeof job);
-    job.pairs = pairs;
-    job.tape = tape;
-    job.offsets = offsets;
-    job.start = start;
-    job.kind = 2;
-    job.distances = results;
-    run_batch(&job, threads);
-}
-
-/* ---------------------------------------------------------------------------------------------- */
 /* CIGARs under Costs, by the Ties rule                                                             */
 /* ---------------------------------------------------------------------------------------------- */
 
@@ -840,16 +690,38 @@ int64_t oracle_edit_cigar(const uint8_t *first, int64_t n, const uint8_t *second
 
 typedef struct {
     int64_t lo, hi;
-    int64_t *aligned, *first_gap, *second_gap;
-    uint8_t *flags;
+    int64_t at; /* the front's first entry in the pools: aligned, first_gap, second_gap at 3 * at; flags at at */
 } wf_front;
 
-static inline int64_t wf_get(const wf_front *fronts, int64_t count, int64_t s, int layer, int64_t k) {
+/* Every cost's fronts of one search, in pools that grow and are kept from pair to pair on a thread. */
+typedef struct {
+    wf_front *fronts;
+    int64_t fronts_capacity;
+    int64_t *values; /* three layers a diagonal */
+    uint8_t *flags;
+    int64_t used, capacity;
+} wf_pool;
+
+static _Thread_local wf_pool thread_pool;
+
+static int64_t wf_reserve(wf_pool *pool, int64_t width) {
+    if (pool->used + width > pool->capacity) {
+        int64_t grown = pool->capacity ? 2 * pool->capacity : 1 << 16;
+        while (grown < pool->used + width) grown *= 2;
+        pool->values = (int64_t *)realloc(pool->values, (size_t)grown * 3 * sizeof(int64_t));
+        pool->flags = (uint8_t *)realloc(pool->flags, (size_t)grown);
+        pool->capacity = grown;
+    }
+    const int64_t at = pool->used;
+    pool->used += width;
+    return at;
+}
+
+static inline int64_t wf_get(const wf_pool *pool, int64_t count, int64_t s, int layer, int64_t k) {
     if (s < 0 || s >= count) return WF_UNREACHED;
-    const wf_front *f = &fronts[s];
+    const wf_front *f = &pool->fronts[s];
     if (f->lo > f->hi || k < f->lo || k > f->hi) return WF_UNREACHED;
-    const int64_t *v = layer == WF_ALIGNED ? f->aligned : layer == WF_FIRST ? f->first_gap : f->second_gap;
-    return v[k - f->lo];
+    return pool->values[3 * (f->at + (k - f->lo)) + layer];
 }
 
 static inline int64_t gcd64(int64_t a, int64_t b) {
@@ -864,7 +736,8 @@ static inline int64_t gcd64(int64_t a, int64_t b) {
 /* The single search of gap_affine.mojo over one direction and its trace (trace, :2028-2124), the moves
  * right to left into `runs`. Returns the cost (scaled back), or -4 when it passes `max_cost`. */
 static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *second, int64_t rows, int64_t x,
-                        int64_t od, int64_t ed, int64_t oi, int64_t ei, int64_t max_cost, int eqx, cigar_runs *runs) {
+                        int64_t od, int64_t ed, int64_t oi, int64_t ei, int64_t max_cost, int eqx, int trace,
+                        cigar_runs *runs) {
     int64_t scale = gcd64(gcd64(gcd64(x, od), gcd64(ed, oi)), ei);
     if (scale <= 0) scale = 1;
     x /= scale;
@@ -873,18 +746,18 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
     oi /= scale;
     ei /= scale;
     const int64_t ceiling = max_cost < 0 ? INT64_MAX : max_cost / scale;
-    int64_t capacity = 64, count = 0;
-    wf_front *fronts = (wf_front *)calloc((size_t)capacity, sizeof(wf_front));
+    wf_pool *pool = &thread_pool;
+    pool->used = 0;
+    int64_t count = 0;
     const int64_t target = columns - rows;
     int64_t cost = -1;
     for (int64_t s = 0;; ++s) {
         if (s > ceiling) break;
-        if (count == capacity) {
-            capacity *= 2;
-            fronts = (wf_front *)realloc(fronts, (size_t)capacity * sizeof(wf_front));
+        if (count == pool->fronts_capacity) {
+            pool->fronts_capacity = pool->fronts_capacity ? 2 * pool->fronts_capacity : 256;
+            pool->fronts = (wf_front *)realloc(pool->fronts, (size_t)pool->fronts_capacity * sizeof(wf_front));
         }
-        wf_front *f = &fronts[count];
-        memset(f, 0, sizeof *f);
+        wf_front *f = &pool->fronts[count];
         if (s == 0) {
             f->lo = f->hi = 0;
         } else {
@@ -894,7 +767,7 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
             const int64_t shift[5] = {0, 1, 1, -1, -1};
             for (int q = 0; q < 5; ++q) {
                 if (from[q] < 0 || from[q] >= count) continue;
-                const wf_front *g = &fronts[from[q]];
+                const wf_front *g = &pool->fronts[from[q]];
                 if (g->lo > g->hi) continue;
                 if (g->lo + shift[q] < lo) lo = g->lo + shift[q];
                 if (g->hi + shift[q] > hi) hi = g->hi + shift[q];
@@ -905,23 +778,22 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
             f->hi = hi;
         }
         const int64_t width = f->hi >= f->lo ? f->hi - f->lo + 1 : 0;
-        f->aligned = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
-        f->first_gap = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
-        f->second_gap = (int64_t *)malloc((size_t)(width > 0 ? width : 1) * sizeof(int64_t));
-        f->flags = (uint8_t *)calloc((size_t)(width > 0 ? width : 1), 1);
+        f->at = wf_reserve(pool, width);
         ++count;
         for (int64_t k = f->lo; k <= f->hi; ++k) {
-            const int64_t i = k - f->lo;
+            int64_t *v = &pool->values[3 * (f->at + (k - f->lo))];
+            uint8_t *flag_out = &pool->flags[f->at + (k - f->lo)];
             if (s == 0) {
-                f->aligned[i] = slide(first, columns, second, rows, 0, 0);
-                f->first_gap[i] = f->second_gap[i] = WF_UNREACHED;
+                v[WF_ALIGNED] = slide(first, columns, second, rows, 0, 0);
+                v[WF_FIRST] = v[WF_SECOND] = WF_UNREACHED;
+                *flag_out = 0;
                 continue;
             }
-            const int64_t same = wf_get(fronts, count, s - x, WF_ALIGNED, k);
-            const int64_t opened_below = wf_get(fronts, count, s - od - ed, WF_ALIGNED, k - 1);
-            const int64_t extended_below = wf_get(fronts, count, s - ed, WF_FIRST, k - 1);
-            const int64_t opened_above = wf_get(fronts, count, s - oi - ei, WF_ALIGNED, k + 1);
-            const int64_t extended_above = wf_get(fronts, count, s - ei, WF_SECOND, k + 1);
+            const int64_t same = wf_get(pool, count, s - x, WF_ALIGNED, k);
+            const int64_t opened_below = wf_get(pool, count, s - od - ed, WF_ALIGNED, k - 1);
+            const int64_t extended_below = wf_get(pool, count, s - ed, WF_FIRST, k - 1);
+            const int64_t opened_above = wf_get(pool, count, s - oi - ei, WF_ALIGNED, k + 1);
+            const int64_t extended_above = wf_get(pool, count, s - ei, WF_SECOND, k + 1);
             const int64_t below = opened_below > extended_below ? opened_below : extended_below;
             const int64_t above = opened_above > extended_above ? opened_above : extended_above;
             const int64_t first_gap = below >= 0 && below < columns ? below + 1 : WF_UNREACHED;
@@ -934,18 +806,18 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
             if (opened_below > extended_below) flag |= WF_OPENED_FIRST;
             if (opened_above > extended_above) flag |= WF_OPENED_SECOND;
             if (!(substituted >= gapped)) flag |= first_gap >= second_gap ? WF_FIRST : WF_SECOND;
-            f->flags[i] = flag;
-            f->first_gap[i] = first_gap;
-            f->second_gap[i] = second_gap;
+            *flag_out = flag;
+            v[WF_FIRST] = first_gap;
+            v[WF_SECOND] = second_gap;
             const int64_t start = substituted > gapped ? substituted : gapped;
-            f->aligned[i] = start >= 0 ? slide(first, columns, second, rows, start, k) : WF_UNREACHED;
+            v[WF_ALIGNED] = start >= 0 ? slide(first, columns, second, rows, start, k) : WF_UNREACHED;
         }
-        if (target >= f->lo && target <= f->hi && f->aligned[target - f->lo] >= columns) {
+        if (target >= f->lo && target <= f->hi && pool->values[3 * (f->at + (target - f->lo)) + WF_ALIGNED] >= columns) {
             cost = s;
             break;
         }
     }
-    if (cost >= 0) {
+    if (cost >= 0 && trace) {
         /* The trace, gap_affine.mojo:2028-2124, moves right to left. */
         const char matched = eqx ? '=' : 'M', substituted = eqx ? 'X' : 'M';
         int64_t spent = cost, k = target, c = columns;
@@ -967,11 +839,10 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
                     c = start;
                     continue;
                 }
-                const wf_front *f = &fronts[spent];
-                const int source = f->flags[k - f->lo] & 7;
-                const int64_t entry = source == WF_ALIGNED ? wf_get(fronts, count, spent - x, WF_ALIGNED, k) + 1
-                                      : source == WF_FIRST ? f->first_gap[k - f->lo]
-                                                           : f->second_gap[k - f->lo];
+                const wf_front *f = &pool->fronts[spent];
+                const int source = pool->flags[f->at + (k - f->lo)] & 7;
+                const int64_t entry = source == WF_ALIGNED ? wf_get(pool, count, spent - x, WF_ALIGNED, k) + 1
+                                                           : wf_get(pool, count, spent, source, k);
                 if (entry <= c) {
                     runs_add(runs, matched, c - entry);
                     c = entry;
@@ -984,8 +855,9 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
                     current = source;
                 }
             } else {
-                const wf_front *f = &fronts[spent];
-                const int opened = (f->flags[k - f->lo] & (current == WF_FIRST ? WF_OPENED_FIRST : WF_OPENED_SECOND)) != 0;
+                const wf_front *f = &pool->fronts[spent];
+                const int opened =
+                    (pool->flags[f->at + (k - f->lo)] & (current == WF_FIRST ? WF_OPENED_FIRST : WF_OPENED_SECOND)) != 0;
                 if (current == WF_FIRST) {
                     runs_add(runs, 'D', 1);
                     c -= 1;
@@ -1017,13 +889,6 @@ static int64_t wf_cigar(const uint8_t *first, int64_t columns, const uint8_t *se
             }
         }
     }
-    for (int64_t s = 0; s < count; ++s) {
-        free(fronts[s].aligned);
-        free(fronts[s].first_gap);
-        free(fronts[s].second_gap);
-        free(fronts[s].flags);
-    }
-    free(fronts);
     return cost < 0 ? -4 : cost * scale;
 }
 
@@ -1037,12 +902,12 @@ int64_t oracle_affine_cigar(const uint8_t *first, int64_t n, const uint8_t *seco
     int64_t written = 0;
     if (right) {
         cost = wf_cigar(first, n, second, m, mismatch, deletion_opening, deletion_extension, insertion_opening,
-                        insertion_extension, max_cost, eqx, &runs);
+                        insertion_extension, max_cost, eqx, 1, &runs);
         if (cost >= 0) written = runs_text(&runs, 1, cigar, capacity);
     } else {
         uint8_t *a = reversed_copy(first, n), *b = reversed_copy(second, m);
         cost = wf_cigar(a, n, b, m, mismatch, deletion_opening, deletion_extension, insertion_opening,
-                        insertion_extension, max_cost, eqx, &runs);
+                        insertion_extension, max_cost, eqx, 1, &runs);
         if (cost >= 0) written = runs_text(&runs, 0, cigar, capacity);
         free(a);
         free(b);
@@ -1051,4 +916,192 @@ int64_t oracle_affine_cigar(const uint8_t *first, int64_t n, const uint8_t *seco
     if (cost >= 0 && written < 0) return -2;
     if (cost < 0 && capacity > 0) cigar[0] = 0;
     return cost;
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* Batches on host threads, longest pair first                                                     */
+/* ---------------------------------------------------------------------------------------------- */
+
+typedef struct {
+    int64_t pairs;
+    const uint8_t *tape;
+    const int64_t *offsets;
+    const int8_t *table;
+    int32_t size, open, extend, mode, eqx;
+    int64_t start;
+    int kind; /* 0 scores, 1 alignments, 2 distances, 3 wavefront costs (and CIGARs) */
+    int64_t costs[5]; /* kind 3: mismatch, deletion opening and extension, insertion opening and extension */
+    int32_t *scores;
+    char *cigars;
+    int64_t cigar_stride;
+    int64_t *cigar_lengths;
+    int64_t *distances;
+    const int64_t *order;
+    atomic_llong next;
+} batch_job;
+
+static void run_pair(batch_job *job, int64_t p) {
+    const uint8_t *first = job->tape + job->offsets[2 * p];
+    const uint8_t *second = job->tape + job->offsets[2 * p + 1];
+    int64_t rows = job->offsets[2 * p + 1] - job->offsets[2 * p];
+    int64_t columns = job->offsets[2 * p + 2] - job->offsets[2 * p + 1];
+    if (job->kind == 0) {
+        job->scores[p] = oracle_gotoh_score(first, rows, second, columns, job->table, job->size, job->open,
+                                            job->extend, job->mode, NULL, NULL);
+    } else if (job->kind == 1) {
+        uint8_t *top = (uint8_t *)malloc((size_t)(rows + columns + 1));
+        uint8_t *bottom = (uint8_t *)malloc((size_t)(rows + columns + 1));
+        int64_t length = 0;
+        job->scores[p] = oracle_gotoh_align(first, rows, second, columns, job->table, job->size, job->open,
+                                            job->extend, job->mode, top, bottom, &length);
+        char *cigar = (char *)malloc((size_t)(2 * length + 2));
+        int64_t written = oracle_cigar(top, bottom, length, job->eqx, cigar);
+        char *slot = job->cigars + p * job->cigar_stride;
+        if (written < job->cigar_stride) {
+            memcpy(slot, cigar, (size_t)written + 1);
+            job->cigar_lengths[p] = written;
+        } else {
+            memcpy(slot, cigar, (size_t)job->cigar_stride - 1);
+            slot[job->cigar_stride - 1] = 0;
+            job->cigar_lengths[p] = -1;
+        }
+        free(cigar);
+        free(top);
+        free(bottom);
+    } else if (job->kind == 3) {
+        /* The wavefront runs over the pair with the reference as its first sequence, its columns. */
+        cigar_runs runs;
+        runs_init(&runs, 64);
+        const int trace = job->cigars != NULL;
+        job->distances[p] = wf_cigar(first, rows, second, columns, job->costs[0], job->costs[1], job->costs[2],
+                                     job->costs[3], job->costs[4], -1, job->eqx, trace, &runs);
+        if (trace) {
+            char *slot = job->cigars + p * job->cigar_stride;
+            const int64_t written = runs_text(&runs, 1, slot, job->cigar_stride);
+            job->cigar_lengths[p] = written;
+        }
+        runs_free(&runs);
+    } else {
+        job->distances[p] = job->start < 0 ? oracle_myers_distance(first, rows, second, columns)
+                                           : oracle_band_doubling(first, rows, second, columns, job->start, NULL,
+                                                                  NULL);
+    }
+}
+
+static void *batch_worker(void *argument) {
+    batch_job *job = (batch_job *)argument;
+    for (;;) {
+        long long k = atomic_fetch_add(&job->next, 1);
+        if (k >= job->pairs) break;
+        run_pair(job, job->order[k]);
+    }
+    return NULL;
+}
+
+static const int64_t *batch_offsets_for_sort;
+static int by_cells_descending(const void *x, const void *y) {
+    int64_t a = *(const int64_t *)x, b = *(const int64_t *)y;
+    const int64_t *o = batch_offsets_for_sort;
+    int64_t ca = (o[2 * a + 1] - o[2 * a] + 1) * (o[2 * a + 2] - o[2 * a + 1] + 1);
+    int64_t cb = (o[2 * b + 1] - o[2 * b] + 1) * (o[2 * b + 2] - o[2 * b + 1] + 1);
+    if (ca != cb) return ca > cb ? -1 : 1;
+    return a < b ? -1 : (a > b);
+}
+
+static pthread_mutex_t sort_lock = PTHREAD_MUTEX_INITIALIZER;
+
+static void run_batch(batch_job *job, int32_t threads) {
+    int64_t *order = (int64_t *)malloc((size_t)(job->pairs > 0 ? job->pairs : 1) * sizeof(int64_t));
+    for (int64_t p = 0; p < job->pairs; ++p) order[p] = p;
+    pthread_mutex_lock(&sort_lock);
+    batch_offsets_for_sort = job->offsets;
+    qsort(order, (size_t)job->pairs, sizeof(int64_t), by_cells_descending);
+    pthread_mutex_unlock(&sort_lock);
+    job->order = order;
+    atomic_init(&job->next, 0);
+    if (threads <= 1) {
+        batch_worker(job);
+    } else {
+        pthread_t *pool = (pthread_t *)malloc((size_t)threads * sizeof(pthread_t));
+        for (int32_t k = 0; k < threads; ++k) pthread_create(&pool[k], NULL, batch_worker, job);
+        for (int32_t k = 0; k < threads; ++k) pthread_join(pool[k], NULL);
+        free(pool);
+    }
+    free(order);
+}
+
+void oracle_batch_scores(int64_t pairs, const uint8_t *tape, const int64_t *offsets, const int8_t *table,
+                         int32_t size, int32_t open, int32_t extend, int32_t mode, int32_t threads, int32_t *results) {
+    batch_job job;
+    memset(&job, 0, sizeof job);
+    job.pairs = pairs;
+    job.tape = tape;
+    job.offsets = offsets;
+    job.table = table;
+    job.size = size;
+    job.open = open;
+    job.extend = extend;
+    job.mode = mode;
+    job.kind = 0;
+    job.scores = results;
+    run_batch(&job, threads);
+}
+
+void oracle_batch_alignments(int64_t pairs, const uint8_t *tape, const int64_t *offsets, const int8_t *table,
+                             int32_t size, int32_t open, int32_t extend, int32_t mode, int32_t eqx, int32_t threads,
+                             int32_t *results, char *cigars, int64_t cigar_stride, int64_t *cigar_lengths) {
+    batch_job job;
+    memset(&job, 0, sizeof job);
+    job.pairs = pairs;
+    job.tape = tape;
+    job.offsets = offsets;
+    job.table = table;
+    job.size = size;
+    job.open = open;
+    job.extend = extend;
+    job.mode = mode;
+    job.eqx = eqx;
+    job.kind = 1;
+    job.scores = results;
+    job.cigars = cigars;
+    job.cigar_stride = cigar_stride;
+    job.cigar_lengths = cigar_lengths;
+    run_batch(&job, threads);
+}
+
+void oracle_batch_distances(int64_t pairs, const uint8_t *tape, const int64_t *offsets, int64_t start,
+                            int32_t threads, int64_t *results) {
+    batch_job job;
+    memset(&job, 0, sizeof job);
+    job.pairs = pairs;
+    job.tape = tape;
+    job.offsets = offsets;
+    job.start = start;
+    job.kind = 2;
+    job.distances = results;
+    run_batch(&job, threads);
+}
+
+
+void oracle_batch_wavefront(int64_t pairs, const uint8_t *tape, const int64_t *offsets, int64_t mismatch,
+                            int64_t deletion_opening, int64_t deletion_extension, int64_t insertion_opening,
+                            int64_t insertion_extension, int32_t eqx, int32_t threads, int64_t *costs, char *cigars,
+                            int64_t cigar_stride, int64_t *cigar_lengths) {
+    batch_job job;
+    memset(&job, 0, sizeof job);
+    job.pairs = pairs;
+    job.tape = tape;
+    job.offsets = offsets;
+    job.kind = 3;
+    job.eqx = eqx;
+    job.costs[0] = mismatch;
+    job.costs[1] = deletion_opening;
+    job.costs[2] = deletion_extension;
+    job.costs[3] = insertion_opening;
+    job.costs[4] = insertion_extension;
+    job.distances = costs;
+    job.cigars = cigars;
+    job.cigar_stride = cigar_stride;
+    job.cigar_lengths = cigar_lengths;
+    run_batch(&job, threads);
 }

@@ -107,6 +107,15 @@ int64_t oracle_affine_cigar(const uint8_t *first, int64_t n, const uint8_t *seco
                             int64_t insertion_extension, int64_t max_cost, int32_t right, int32_t eqx, char *cigar,
                             int64_t capacity);
 
+/* Batch costs under one-piece gap-affine Costs by the wavefront, the reference's host path for a global
+ * alignment under a uniform Scoring (scoring.mojo:414-440 global_on_host -> gap_affine.mojo's wavefront),
+ * threaded as the batches above. Each pair's cost into costs[p] and, with `cigars` non-null, its Ties.RIGHT
+ * CIGAR into cigars + p * cigar_stride (its length into cigar_lengths[p], -1 when it did not fit). */
+void oracle_batch_wavefront(int64_t pairs, const uint8_t *tape, const int64_t *offsets, int64_t mismatch,
+                            int64_t deletion_opening, int64_t deletion_extension, int64_t insertion_opening,
+                            int64_t insertion_extension, int32_t eqx, int32_t threads, int64_t *costs, char *cigars,
+                            int64_t cigar_stride, int64_t *cigar_lengths);
+
 #ifdef __cplusplus
 }
 #endif

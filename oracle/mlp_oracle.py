@@ -2,7 +2,7 @@
 float64 numpy.
 
 TEST INFRASTRUCTURE ONLY: the tests check the GPU's features and training gradients against these; nothing
-in the product imports it. The layout follows the library's flat parameter vector: w1 [257][64], b1 [64],
+in the product imports it. The layout follows the library's flat parameter vector: w1 [258][64], b1 [64],
 w2 [64][64], b2 [64], w3 [64], b3.
 """
 
@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import numpy as np
 
-INPUTS, HIDDEN = 257, 64
+INPUTS, HIDDEN = 258, 64
 SIZES = [("w1", (INPUTS, HIDDEN)), ("b1", (HIDDEN,)), ("w2", (HIDDEN, HIDDEN)), ("b2", (HIDDEN,)), ("w3", (HIDDEN,)),
          ("b3", (1,))]
 PARAMETERS = sum(int(np.prod(shape)) for _, shape in SIZES)
@@ -30,13 +30,13 @@ def pack(parts: dict) -> np.ndarray:
     return np.concatenate([np.asarray(parts[name], dtype=np.float64).ravel() for name, _ in SIZES])
 
 
-def kmer_counts(sequence: bytes) -> np.ndarray:
-    """Counts of each 4-mer (A=0, C=1, G=2, T=3, first letter most significant); a 4-mer holding another
+def kmer_counts(sequence: bytes, k: int = 4) -> np.ndarray:
+    """Counts of each k-mer (A=0, C=1, G=2, T=3, first letter most significant); a k-mer holding another
     letter is skipped."""
-    counts = np.zeros(256, dtype=np.int64)
-    for start in range(len(sequence) - 3):
+    counts = np.zeros(4 ** k, dtype=np.int64)
+    for start in range(len(sequence) - k + 1):
         code = 0
-        for letter in sequence[start:start + 4]:
+        for letter in sequence[start:start + k]:
             value = CODES.get(letter)
             if value is None:
                 code = -1
@@ -48,19 +48,21 @@ def kmer_counts(sequence: bytes) -> np.ndarray:
 
 
 def features(reference: bytes, query: bytes) -> np.ndarray:
-    """The 257 inputs: each 4-mer count difference squared, times 32 over the mean length, then the length
-    ratio."""
+    """The 258 inputs: each 4-mer count difference squared, times 32 over the mean length; the length
+    ratio; and the 6-mer count differences' squares summed, over the mean length."""
     out = np.zeros(INPUTS, dtype=np.float64)
     mean = 0.5 * (len(reference) + len(query))
     difference = (kmer_counts(reference) - kmer_counts(query)).astype(np.float64)
     out[:256] = 32.0 * difference ** 2 / max(mean, 1.0)
     low, high = min(len(reference), len(query)), max(len(reference), len(query))
     out[256] = low / high if high > 0 else 1.0
+    sixes = (kmer_counts(reference, 6) - kmer_counts(query, 6)).astype(np.float64)
+    out[257] = float((sixes ** 2).sum()) / max(mean, 1.0)
     return out
 
 
 def forward(parts: dict, x: np.ndarray) -> tuple:
-    """x: [batch, 257]; returns (y [batch], cache)."""
+    """x: [batch, 258]; returns (y [batch], cache)."""
     z1 = x @ parts["w1"] + parts["b1"]
     h1 = np.maximum(z1, 0.0)
     z2 = h1 @ parts["w2"] + parts["b2"]

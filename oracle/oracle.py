@@ -69,6 +69,9 @@ def lib() -> ctypes.CDLL:
         handle.oracle_affine_cigar.restype = i64
         handle.oracle_affine_cigar.argtypes = [u8p, i64, u8p, i64, i64, i64, i64, i64, i64, i64, i32, i32,
                                                ctypes.c_char_p, i64]
+        handle.oracle_batch_wavefront.restype = None
+        handle.oracle_batch_wavefront.argtypes = [i64, u8p, i64p, i64, i64, i64, i64, i64, i32, i32, i64p,
+                                                  ctypes.c_char_p, i64, i64p]
         handle.oracle_batch_distances.restype = None
         handle.oracle_batch_distances.argtypes = [i64, u8p, i64p, i64, i32, i64p]
         _lib = handle
@@ -254,3 +257,24 @@ def dna_table(match: int, mismatch: int) -> np.ndarray:
 def kernel_gaps(opening: int, extension: int) -> tuple:
     """A Scoring's (opening, extension) in the kernels' terms (scoring.mojo:202-215 gap_scores)."""
     return opening + extension, extension
+
+
+def batch_wavefront(tape, offsets, mismatch, opening, extension, cigars=True, eqx=True, threads=1) -> tuple:
+    """(costs, CIGARs or None) of every pair under Costs.affine(mismatch, opening, extension) by the
+    wavefront, threaded: the reference's host path for a global alignment under a uniform Scoring."""
+    pairs = (len(offsets) - 1) // 2
+    t, pt = _u8(tape)
+    o = np.ascontiguousarray(offsets, dtype=np.int64)
+    costs = np.zeros(max(pairs, 1), dtype=np.int64)
+    lengths = o[2::2][:pairs] - o[0::2][:pairs] if pairs else np.zeros(0, dtype=np.int64)
+    stride = int(2 * (lengths.max() if pairs else 0) + 8)
+    buffer = ctypes.create_string_buffer(max(pairs, 1) * stride) if cigars else None
+    cigar_lengths = np.zeros(max(pairs, 1), dtype=np.int64)
+    lib().oracle_batch_wavefront(pairs, pt, o.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), mismatch, opening,
+                                 extension, opening, extension, 1 if eqx else 0, threads,
+                                 costs.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), buffer, stride,
+                                 cigar_lengths.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    if not cigars:
+        return costs[:pairs], None
+    raw = buffer.raw
+    return costs[:pairs], [raw[p * stride: p * stride + int(cigar_lengths[p])].decode("ascii") for p in range(pairs)]

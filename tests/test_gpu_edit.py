@@ -76,8 +76,10 @@ def test_bytes_and_refusals(da, oracle):
     assert list(got[:3]) == [3, 4, 3]
     assert got[3] == -1
     assert got[4] == oracle.edit_distance_dp(refs[4], queries[4])
+    # Gap-affine costs take the wavefront (tests/test_gpu_costs.py); two gap pieces are not served.
+    assert da.distances(["ACGTAC"], ["ACGAC"], da.Costs.affine(4, 6, 2)) == [8]
     with pytest.raises(ValueError):
-        da.distances(["ACGT"], ["ACGT"], da.Costs.affine(4, 6, 2))
+        da.distances(["ACGT"], ["ACGT"], da.Costs.two_piece(4, 6, 2, 24, 1))
     with pytest.raises(ValueError):
         da.distances(["ACGT"], ["ACGT"], mode=da.Mode.INFIX)
     with pytest.raises(ValueError):

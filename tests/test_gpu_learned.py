@@ -39,7 +39,7 @@ def test_gradients_match_oracle(learned):
 
     rng = np.random.default_rng(4)
     flat = rng.normal(0, 0.1, size=learned.PARAMETERS).astype(np.float32)
-    x = rng.normal(0, 0.5, size=(300, 257)).astype(np.float32)
+    x = rng.normal(0, 0.5, size=(300, 258)).astype(np.float32)
     t = rng.uniform(0, 0.2, size=300).astype(np.float32)
     predictor = learned.Predictor()
     predictor.install(flat, 1.0, 0.0)

@@ -229,7 +229,7 @@ def test_mlp_oracle_gradients_by_finite_differences():
 
     rng = np.random.default_rng(2)
     flat = rng.normal(0, 0.2, size=mlp_oracle.PARAMETERS)
-    x = rng.normal(0, 1, size=(7, 257))
+    x = rng.normal(0, 1, size=(7, 258))
     t = rng.uniform(0, 1, size=7)
     grads, _ = mlp_oracle.gradients(flat, x, t)
     for index in list(rng.integers(0, mlp_oracle.PARAMETERS, size=40)) + [mlp_oracle.PARAMETERS - 1]:
@@ -351,3 +351,16 @@ def test_costs_cigars_are_optimal_and_follow_the_rule(oracle, costs):
                 # The unit-cost trace (edit_cigar) and the wavefront's agree, as the reference asserts for
                 # a capped search against an uncapped one (tests/test_alignment.mojo:2212-2218).
                 assert oracle.edit_cigar(reference, query, right=right) == (cost, cigar)
+
+
+def test_batch_wavefront_matches_single_pairs(oracle):
+    """The threaded wavefront batch (the reference's host path for a uniform Scoring, timed as a CPU
+    baseline) gives every pair the single-pair search's cost and Ties.RIGHT CIGAR, and the plain DP's cost."""
+    rng = random.Random(23)
+    refs, queries = zip(*[repeats(rng) for _ in range(300)])
+    tape, offsets = oracle.tape_of([np.frombuffer(r.encode(), np.uint8) for r in refs],
+                                   [np.frombuffer(q.encode(), np.uint8) for q in queries])
+    costs, cigars = oracle.batch_wavefront(tape, offsets, 4, 6, 2, threads=4)
+    for k, (a, b) in enumerate(zip(refs, queries)):
+        assert (costs[k], cigars[k]) == oracle.affine_cigar(a, b, 4, 6, 2, right=True)
+        assert costs[k] == least_cost(a, b, 4, 6, 2, 6, 2)
