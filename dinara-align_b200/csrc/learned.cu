@@ -153,22 +153,25 @@ __device__ __forceinline__ int six_at(const unsigned *sixes, uint32_t bin) {
     return int((sixes[bin >> 1] >> (16 * (bin & 1u))) & 0xFFFFu) - 32768;
 }
 
-template <bool WIDE>
-__device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, unsigned *sixes, int *fours,
-                            int64_t slot) {
-    // One slot of 16 letters: the 6-mers starting at letters 16 slot .. 16 slot + 15, read through seven
-    // aligned words that hold those letters and the five after them (a word may reach three bytes past
-    // the sequence's end: device letter buffers keep 16 bytes of room there).
+// The seven aligned words holding a slot's 16 letters and the five after them (a word may reach three
+// bytes past the sequence's end: device letter buffers keep 16 bytes of room there); loaded apart from
+// their use so that a lane keeps two slots' loads in flight.
+__device__ __forceinline__ void load_slot(const uint8_t *sequence, int64_t length, int64_t slot, uint32_t w[7]) {
     const uintptr_t origin = reinterpret_cast<uintptr_t>(sequence);
     const uintptr_t end = origin + uintptr_t(length);
+    const uintptr_t aligned = (origin + uintptr_t(16 * slot)) & ~uintptr_t(3);
+    const uint32_t *words = reinterpret_cast<const uint32_t *>(aligned);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) w[i] = aligned + 4 * uintptr_t(i) < end ? __ldg(words + i) : 0u;
+}
+
+// One slot of 16 letters: the 6-mers starting at letters 16 slot .. 16 slot + 15, from its loaded words.
+template <bool WIDE>
+__device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, unsigned *sixes, int *fours,
+                            int64_t slot, const uint32_t w[7]) {
     {
         const int64_t first = 16 * slot;
-        const uintptr_t address = origin + uintptr_t(first);
-        const uintptr_t aligned = address & ~uintptr_t(3);
-        const uint32_t *words = reinterpret_cast<const uint32_t *>(aligned);
-        uint32_t w[7];
-#pragma unroll
-        for (int i = 0; i < 7; ++i) w[i] = aligned + 4 * uintptr_t(i) < end ? __ldg(words + i) : 0u;
+        const uintptr_t address = reinterpret_cast<uintptr_t>(sequence) + uintptr_t(first);
         const uint32_t shift = uint32_t(address & 3u) * 8u;
         uint32_t a[6];
 #pragma unroll
@@ -195,36 +198,26 @@ __device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, u
                 return;
             }
         }
-        // Near the sequence's end or another letter in reach: letter by letter. `run` counts the valid
-        // letters ending at j; the 6-mer (or, failing it, the 4-mer) starting at j - 5 (j - 3) is counted
-        // once its letters are all in hand.
-        uint32_t kmer = 0;
-        int run = 0;
-#pragma unroll
-        for (int j = 0; j < 21; ++j) {
-            const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
-            kmer = (kmer >> 2) | (uint32_t(c & 3) << 10);
-            run = c < 0 ? 0 : run + 1;
-            if (j >= 5 && j - 5 < 16 && run >= 6) add_six<WIDE>(sixes, kmer, sign);
-        }
-        // 4-mers starting at the lane's 16 places with no valid 6-mer from the same place.
-        run = 0;
-        int valid_from[21];
-#pragma unroll
-        for (int j = 20; j >= 0; --j) {
-            const int c = first + j < length ? code_of((a[j >> 2] >> (8 * (j & 3))) & 0xFFu) : -1;
-            run = c < 0 ? 0 : run + 1;
-            valid_from[j] = run;  // valid letters from j on
-        }
-#pragma unroll
+        // Near the sequence's end or another letter in reach (rare): start by start, letter by letter, in a
+        // loop kept rolled so the kernel's body stays in the instruction cache. The 6-mer starting at each
+        // of the slot's places, or failing it the 4-mer.
+#pragma unroll 1
         for (int j = 0; j < 16; ++j) {
-            if (valid_from[j] >= 4 && valid_from[j] < 6) {
-                uint32_t four = 0;
-#pragma unroll
-                for (int q = 3; q >= 0; --q)
-                    four = (four << 2) | uint32_t(code_of((a[(j + q) >> 2] >> (8 * ((j + q) & 3))) & 0xFFu) & 3);
-                atomicAdd(&fours[four], sign);
+            const int64_t place = first + j;
+            if (place + 4 > length) break;
+            uint32_t kmer = 0;
+            int valid = 0;
+#pragma unroll 1
+            for (int q = 0; q < 6 && place + q < length; ++q) {
+                const int c = code_of(__ldg(sequence + place + q));
+                if (c < 0) break;
+                kmer |= uint32_t(c) << (2 * q);
+                ++valid;
             }
+            if (valid == 6)
+                add_six<WIDE>(sixes, kmer, sign);
+            else if (valid >= 4)
+                atomicAdd(&fours[kmer & 0xFFu], sign);
         }
     }
 }
@@ -303,13 +296,23 @@ __global__ void __launch_bounds__(32 * kSketchWarps) features_kernel(const uint8
         if (!WIDE && (reference > kNarrowLimit || query > kNarrowLimit)) continue;  // the wide form's
         for (int k = lane; k < kWords; k += 32) sixes[k] = (WIDE || k >= 2048) ? 0u : 0x80008000u;
         __syncwarp();
-        // Both sequences' 16-letter slots in one run, the reference's (+1) then the query's (-1).
+        // Both sequences' 16-letter slots in one run, the reference's (+1) then the query's (-1), two slots
+        // a lane at a time: both slots' words are loaded before either is counted.
         const int64_t reference_slots = (reference + 15) / 16, slots = reference_slots + (query + 15) / 16;
-        for (int64_t slot = lane; slot < slots; slot += 32) {
-            if (slot < reference_slots)
-                count_kmers<WIDE>(letters + r0, reference, 1, sixes, fours, slot);
-            else
-                count_kmers<WIDE>(letters + q0, query, -1, sixes, fours, slot - reference_slots);
+        for (int64_t slot = lane; slot < slots; slot += 64) {
+            const int64_t other = slot + 32;
+            const bool first_ref = slot < reference_slots, other_ref = other < reference_slots;
+            uint32_t w0[7], w1[7];
+            load_slot(first_ref ? letters + r0 : letters + q0, first_ref ? reference : query,
+                      first_ref ? slot : slot - reference_slots, w0);
+            if (other < slots)
+                load_slot(other_ref ? letters + r0 : letters + q0, other_ref ? reference : query,
+                          other_ref ? other : other - reference_slots, w1);
+            count_kmers<WIDE>(first_ref ? letters + r0 : letters + q0, first_ref ? reference : query, first_ref ? 1 : -1,
+                              sixes, fours, first_ref ? slot : slot - reference_slots, w0);
+            if (other < slots)
+                count_kmers<WIDE>(other_ref ? letters + r0 : letters + q0, other_ref ? reference : query,
+                                  other_ref ? 1 : -1, sixes, fours, other_ref ? other : other - reference_slots, w1);
         }
         __syncwarp();
         features_of<WIDE>(sixes, fours, reference, query, pair_major ? features + pair * kIn : features + pair,
