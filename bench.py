@@ -64,6 +64,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-parity", action="store_true")
     parser.add_argument("--no-sections", action="store_true", help="only the headline workload")
+    parser.add_argument("--predictor", default="",
+                        help="band predictor blob: loaded when the file exists, else trained and saved there")
     parser.add_argument("--selftest-ranks", action="store_true",
                         help="check the rank launch and the max-over-ranks timing on the CPU (gloo), no GPU work")
     return parser.parse_args()
@@ -389,11 +391,21 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
     the GPU first."""
     da, native, lib, handle, ranks, peaks = ctx["da"], ctx["native"], ctx["lib"], ctx["handle"], ctx["ranks"], \
         ctx["peaks"]
-    from dinara_align import learned
+    from dinara_align import learned, tuning
 
     placement = da.Placement.on_gpu(ranks.local_rank)
+    # The band autotuner first: both arms then sweep with the shapes it measured, and the predictor's
+    # margins are calibrated against the windows those shapes give.
+    tuned = tuning.autotune(placement)
     predictor = learned.Predictor(placement)
-    training = predictor.train(pairs=1_000_000, epochs=4, batch=4096, seed=2024)
+    blob = ctx.get("predictor", "")
+    if blob and os.path.exists(blob):
+        predictor.load(blob)
+        training = {"loaded": blob}
+    else:
+        training = predictor.train(pairs=1_000_000, epochs=4, batch=1024, seed=2024)
+        if blob:
+            predictor.save(blob)
     native.check(lib.dinara_gpu_resident_load(handle, tape.pairs, tape.letters.ctypes.data,
                                               tape.offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), None),
                  handle)
@@ -431,7 +443,9 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
             "speedup_learned_over_plain": out["learned"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
             "identical_distances": bool((found["learned"] == found["plain"]).all()),
             "gcups": out["learned"]["gcups_full_matrix"], "plain_gcups": out["plain"]["gcups_full_matrix"],
-            "learned": out["learned"], "plain": out["plain"], "training": training}
+            "learned": out["learned"], "plain": out["plain"], "training": training,
+            "autotune": {"chain_words": tuned["chain_words"], "chain_ms": tuned["chain_ms"],
+                         "seconds": tuned["seconds"], "words_per_ms": tuned["words_per_ms"]}}
     # The dominant kernel: every round's band kernels. A Myers/Hyyro word step is about 20 u64 operations
     # (bit_parallel.mojo:10-11), 40 in int32 terms, over the words the rounds swept.
     kernels = []
@@ -722,7 +736,7 @@ def main() -> None:
     handle = native.context(ranks.local_rank)
     peaks = int32_peaks(handle, lib)
     ctx = {"da": da, "native": native, "lib": lib, "handle": handle, "ranks": ranks, "peaks": peaks,
-           "e2e": not args.no_e2e, "parity": not args.no_parity}
+           "e2e": not args.no_e2e, "parity": not args.no_parity, "predictor": args.predictor}
     head = run_workload(ctx, args.workload, args.pairs, args.steps, args.warmup, not args.no_cpu)
     begin, end = head.pop("timed_region")
     sections = {}

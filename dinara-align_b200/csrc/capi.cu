@@ -1466,6 +1466,30 @@ dinara_gpu *default_gpu() {
 
 }  // namespace
 
+int64_t dinara_gpu_band_autotune(dinara_gpu *gpu, const dinara_band_tune_options *options,
+                                 dinara_band_tune_report *report) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+        DINARA_CUDA(cudaSetDevice(gpu->device));
+        dinara_band_tune_options given;
+        std::memset(&given, 0, sizeof given);
+        if (options) given = *options;
+        dinara_band_tune_report local;
+        band_autotune(gpu, given, local);
+        DINARA_CUDA(cudaStreamSynchronize(gpu->stream));
+        if (report) *report = local;
+        return 0;
+    });
+}
+
+int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, float *word_costs) {
+    return guard(gpu, [&]() -> int64_t {
+        if (!gpu || !chain_words || !word_costs) throw Failure(DINARA_INVALID_MODE, "no context or tuning arrays");
+        band_tuning_access(gpu, set != 0, chain_words, word_costs);
+        return 0;
+    });
+}
+
 int64_t dinara_gpu_predictor_train(dinara_gpu *gpu, const dinara_train_options *options, dinara_train_report *report) {
     return guard(gpu, [&]() -> int64_t {
         if (!gpu || !options) throw Failure(DINARA_INVALID_MODE, "no context or options");

@@ -122,6 +122,23 @@ inline uint64_t packed_words_total(int64_t letters, int64_t sequences, int bits)
 
 }  // namespace dinara
 
+namespace dinara {
+
+// How a unit-cost band round picks a pair's window shape among those that hold its band (band_shape_for,
+// edit.cuh). `word_cost` is each shape's time a 64-cell word step, relative (lower is faster), and
+// `chain_words` bounds a pair's chain of dependent word steps (text letters x words a lane), so that a
+// long pair, which holds its lanes for the whole of that chain, takes more lanes and fewer words each.
+// The band autotuner (dinara_gpu_band_autotune) measures both on the device; until then they come from
+// default_band_tuning (edit.cuh).
+struct BandTuning {
+    static constexpr int kShapes = 40;
+    int64_t chain_words;
+    float word_cost[kShapes];
+    int32_t tuned;  // 1 once the autotuner has set them on this context
+};
+
+}  // namespace dinara
+
 // The context behind the C ABI's opaque handle.
 struct dinara_gpu {
     int device = 0;
@@ -132,7 +149,7 @@ struct dinara_gpu {
     cudaStream_t upload = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
     // Side streams that let a round's launches of different shapes run at once, joined by events.
-    static constexpr int kSideStreams = 23;  // one for each band window shape
+    static constexpr int kSideStreams = 39;  // one for each band window shape
     cudaStream_t side[kSideStreams] = {nullptr};
     cudaEvent_t fork = nullptr, joins[kSideStreams] = {nullptr};
     std::string error;
@@ -153,6 +170,7 @@ struct dinara_gpu {
     dinara::DeviceBuffer features, weights, gradients, optimizer, predictions, targets, activations, sketches;
     // Alignments under Costs: each warp's arena of kept fronts (ties.cu).
     dinara::DeviceBuffer wavefront;
+    dinara::BandTuning band_tuning{};
     bool predictor_ready = false;
     double predictor_margin = 1.25;    // the largest of the classes' margins (reported)
     double predictor_margins[4] = {1.25, 1.25, 1.25, 1.25};  // by mean length: < 300, < 1000, < 4096, more

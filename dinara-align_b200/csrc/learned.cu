@@ -229,25 +229,46 @@ __device__ void count_kmers(const uint8_t *sequence, int64_t length, int sign, u
 // ratio. Then the 6-mer count differences' squares summed over their 4,096 bins, over the mean length:
 // the same measure with sixteen times the bins, whose noise from moves sharing a bin is a quarter of
 // the 4-mers' (about 3.6% against 11% of a 4 kbp pair's distance).
+//
+// One pass over the counts does it all, and leaves them cleared for the warp's next pair: a lane reads
+// the words lane, lane + 32, ... of the 6-mer bins, whose 4-mers (a bin's low eight bits) are eight fixed
+// ones per lane, so the 4-mer counts build up in eight registers while the squares are summed.
 template <bool WIDE>
-__device__ void features_of(const unsigned *sixes, const int *fours, int64_t reference, int64_t query, float *out,
-                            int stride) {
+__device__ void features_of(unsigned *sixes, int *fours, int64_t reference, int64_t query, float *out, int stride) {
     const int lane = threadIdx.x & 31;
     const float mean = 0.5f * float(reference + query);
     const float scale = 32.0f / (mean > 1.0f ? mean : 1.0f);
-    for (int k = lane; k < 256; k += 32) {
-        // Feature k's 4-mer has its first letter in the highest bits; the counts, in the lowest.
-        const uint32_t four = reversed_kmer(uint32_t(k));
-        int count = fours[four];
-#pragma unroll
-        for (int y = 0; y < 16; ++y) count += six_at<WIDE>(sixes, four | (uint32_t(y) << 8));
-        const float difference = float(count);
-        out[int64_t(k) * stride] = difference * difference * scale;
-    }
+    int sums[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long squares = 0;
-    for (int b = lane; b < 4096; b += 32) {
-        const long long v = six_at<WIDE>(sixes, uint32_t(b));
-        squares += v * v;
+    if (WIDE) {
+        // Word w is bin w; bin lane + 32 i has 4-mer lane + 32 (i mod 8).
+#pragma unroll 8
+        for (int i = 0; i < 128; ++i) {
+            const int v = int(sixes[lane + 32 * i]);
+            sixes[lane + 32 * i] = 0u;
+            squares += (long long)v * v;
+            sums[i & 7] += v;
+        }
+    } else {
+        // Word w holds bins 2w and 2w + 1; for w = lane + 32 i their 4-mers are 2 lane + 64 (i mod 4) and
+        // one more.
+#pragma unroll 4
+        for (int i = 0; i < 64; ++i) {
+            const unsigned word = sixes[lane + 32 * i];
+            sixes[lane + 32 * i] = 0x80008000u;
+            const int low = int(word & 0xFFFFu) - 32768, high = int(word >> 16) - 32768;
+            squares += (long long)low * low + (long long)high * high;
+            sums[2 * (i & 3)] += low;
+            sums[2 * (i & 3) + 1] += high;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const uint32_t four = WIDE ? uint32_t(lane + 32 * s) : uint32_t(2 * lane + (s & 1) + 64 * (s >> 1));
+        const float difference = float(sums[s] + fours[four]);
+        fours[four] = 0;
+        // Feature k's 4-mer has its first letter in the highest bits; the counts, in the lowest.
+        out[int64_t(reversed_kmer(four)) * stride] = difference * difference * scale;
     }
 #pragma unroll
     for (int span = 16; span > 0; span >>= 1) squares += __shfl_xor_sync(0xffffffffu, squares, span);
@@ -285,6 +306,9 @@ __global__ void __launch_bounds__(32 * kSketchWarps) features_kernel(const uint8
     const int lane = threadIdx.x & 31;
     unsigned *sixes = sketch_counts + (threadIdx.x >> 5) * kWords;
     int *fours = reinterpret_cast<int *>(sixes + (WIDE ? 4096 : 2048));
+    // Cleared once here; each pair's features clear what its counts used.
+    for (int k = lane; k < kWords; k += 32) sixes[k] = (WIDE || k >= 2048) ? 0u : 0x80008000u;
+    __syncwarp();
     for (;;) {
         unsigned item = 0;
         if (lane == 0) item = atomicAdd(queue, 1u);
@@ -294,8 +318,6 @@ __global__ void __launch_bounds__(32 * kSketchWarps) features_kernel(const uint8
         const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
         const int64_t reference = q0 - r0, query = q1 - q0;
         if (!WIDE && (reference > kNarrowLimit || query > kNarrowLimit)) continue;  // the wide form's
-        for (int k = lane; k < kWords; k += 32) sixes[k] = (WIDE || k >= 2048) ? 0u : 0x80008000u;
-        __syncwarp();
         // Both sequences' 16-letter slots in one run, the reference's (+1) then the query's (-1), two slots
         // a lane at a time: both slots' words are loaded before either is counted.
         const int64_t reference_slots = (reference + 15) / 16, slots = reference_slots + (query + 15) / 16;
@@ -654,31 +676,40 @@ const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t 
     return thresholds;
 }
 
+GeneratedPairs generate_pairs(dinara_gpu *gpu, uint64_t seed, int64_t pairs, double length_low, double length_high,
+                              double rate_low, double rate_high) {
+    cudaStream_t stream = gpu->stream;
+    // Lengths first (each pair's letters' fates decide the query's), then offsets, then the letters.
+    int64_t *lengths = gpu->thresholds.ensure<int64_t>(size_t(2 * pairs + 1));
+    const int threads = 256;
+    const unsigned pair_blocks = unsigned((pairs + threads - 1) / threads);
+    generate_lengths_kernel<<<pair_blocks, threads, 0, stream>>>(seed, pairs, length_low, length_high, rate_low,
+                                                                 rate_high, lengths);
+    DINARA_CUDA(cudaGetLastError());
+    GeneratedPairs out;
+    out.offsets = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
+    DINARA_CUDA(cudaMemsetAsync(lengths + 2 * pairs, 0, sizeof(int64_t), stream));
+    size_t scratch = 0;
+    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, lengths, out.offsets, int(2 * pairs + 1), stream));
+    void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
+    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, lengths, out.offsets, int(2 * pairs + 1), stream));
+    read_back(gpu, &out.letters_total, out.offsets + 2 * pairs, sizeof(int64_t));
+    out.letters = gpu->letters.ensure<uint8_t>(size_t(out.letters_total) + 16);
+    generate_letters_kernel<<<pair_blocks, threads, 0, stream>>>(seed, pairs, length_low, length_high, rate_low,
+                                                                 rate_high, out.offsets, out.letters);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 2;
+    return out;
+}
+
 void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinara_train_report &report) {
     cudaStream_t stream = gpu->stream;
     const int64_t pairs = options.pairs;
     // The training pairs: lengths, offsets, letters, all on the device.
-    int64_t *lengths = gpu->thresholds.ensure<int64_t>(size_t(2 * pairs + 1));
-    const int threads = 256;
-    const unsigned pair_blocks = unsigned((pairs + threads - 1) / threads);
-    generate_lengths_kernel<<<pair_blocks, threads, 0, stream>>>(options.seed, pairs, options.length_low,
-                                                                 options.length_high, options.rate_low,
-                                                                 options.rate_high, lengths);
-    DINARA_CUDA(cudaGetLastError());
-    int64_t *offsets = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
-    DINARA_CUDA(cudaMemsetAsync(lengths + 2 * pairs, 0, sizeof(int64_t), stream));
-    size_t scratch = 0;
-    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, lengths, offsets, int(2 * pairs + 1), stream));
-    void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
-    DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, lengths, offsets, int(2 * pairs + 1), stream));
-    int64_t total = 0;
-    DINARA_CUDA(cudaMemcpyAsync(&total, offsets + 2 * pairs, sizeof total, cudaMemcpyDeviceToHost, stream));
-    DINARA_CUDA(cudaStreamSynchronize(stream));
-    uint8_t *letters = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
-    generate_letters_kernel<<<pair_blocks, threads, 0, stream>>>(options.seed, pairs, options.length_low,
-                                                                 options.length_high, options.rate_low,
-                                                                 options.rate_high, offsets, letters);
-    DINARA_CUDA(cudaGetLastError());
+    const GeneratedPairs generated = generate_pairs(gpu, options.seed, pairs, options.length_low, options.length_high,
+                                                    options.rate_low, options.rate_high);
+    int64_t *offsets = generated.offsets;
+    uint8_t *letters = generated.letters;
     // Their exact distances: the method's own, plain band doubling.
     int64_t *distances = gpu->features.ensure<int64_t>(size_t(pairs));
     band_doubling(gpu, pairs, letters, offsets, nullptr, 0, distances, nullptr);
@@ -764,30 +795,72 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
     DINARA_CUDA(cudaMemcpyAsync(guesses.data(), gpu->targets.as<float>(), size_t(held) * sizeof(float),
                                 cudaMemcpyDeviceToHost, stream));
     DINARA_CUDA(cudaStreamSynchronize(stream));
-    // Each held-out pair's ratio of distance (less the slack) to guess, by length class; a class's margin
-    // reaches a share of its pairs. A pair that undershoots sweeps again, and the round it adds lasts as
+    // A class's margin is the least that settles a share of its held-out pairs in their first round: a
+    // pair settles when its distance lies within the band its first window sweeps (band_reach: a window
+    // holds a wider band than the threshold needs, for nothing), with the window the first round would
+    // give it under the context's tuning. A pair that misses sweeps again, and the round it adds lasts as
     // long as its longest pair's sweep, so the longer classes are held to a higher share: the asked
     // coverage for pairs under 1,000 letters, a third of the misses past it under 4,096, a tenth longer.
-    std::vector<double> ratios[4];
+    struct HeldPair {
+        int64_t n, m, d;
+        double guess;
+    };
+    std::vector<HeldPair> classes[4];
     double squared = 0.0;
     for (int64_t k = 0; k < held; ++k) {
         const int64_t p = trained + k;
+        const int64_t reference = host_offsets[size_t(2 * p + 1)] - host_offsets[size_t(2 * p)];
+        const int64_t query = host_offsets[size_t(2 * p + 2)] - host_offsets[size_t(2 * p + 1)];
         const double d = double(host_distances[size_t(p)]);
         const double g = double(guesses[size_t(k)]);
-        const double mean = 0.5 * double(host_offsets[size_t(2 * p + 2)] - host_offsets[size_t(2 * p)]);
-        ratios[length_class(mean)].push_back((d - options.slack) / std::max(g, 1.0));
+        const double mean = 0.5 * double(reference + query);
+        classes[length_class(mean)].push_back({std::min(reference, query), std::max(reference, query),
+                                               host_distances[size_t(p)], g});
         const double e = (mean > 0 ? d / mean : 0.0) - (mean > 0 ? g / mean : 0.0);
         squared += e * e;
     }
+    if (gpu->band_tuning.chain_words == 0) gpu->band_tuning = default_band_tuning();
+    const BandTuning tuning = gpu->band_tuning;
+    const double slack = options.slack;
+    // Whether a pair settles in its first round at margin `margin` (predict_kernel's threshold).
+    auto settles = [&](const HeldPair &h, double margin) {
+        const int64_t delta = h.m - h.n;
+        int64_t t = int64_t(std::ceil(h.guess * margin + slack));
+        t = std::max<int64_t>(std::max<int64_t>(t, delta), 1);
+        const int64_t window = band_capacity(band_shape_for(h.n, h.m, t, false, tuning));
+        const int64_t words = (h.n + 63) / 64;
+        if (window >= words) return true;
+        if (window < band_words_needed(h.n, h.m, t)) return false;
+        const int64_t half = (t - delta) / 2, reach = band_reach(h.n, h.m, window);
+        return h.d <= delta + 2 * std::max(half, reach) + 1;
+    };
     const double coverage = std::min(std::max(options.coverage, 0.5), 0.999);
     const double misses[4] = {1.0, 1.0, 1.0 / 3.0, 0.1};
-    double widest = 1.0;
+    double widest = 0.0;
     for (int c = 0; c < 4; ++c) {
         double margin = 1.0;
-        if (!ratios[c].empty()) {
-            std::sort(ratios[c].begin(), ratios[c].end());
+        if (!classes[c].empty()) {
             const double share = 1.0 - (1.0 - coverage) * misses[c];
-            margin = std::max(1.0, ratios[c][size_t(double(ratios[c].size() - 1) * share)]);
+            const int64_t wanted = int64_t(std::ceil(share * double(classes[c].size())));
+            auto enough = [&](double mu) {
+                int64_t settled = 0;
+                for (const HeldPair &h : classes[c]) settled += settles(h, mu) ? 1 : 0;
+                return settled >= wanted;
+            };
+            // The least margin in [0.5, 4] reaching the share, to 1/1000 (settling grows with the margin).
+            double low = 0.5, high = 4.0;
+            if (enough(low)) {
+                high = low;
+            } else {
+                while (high - low > 1e-3) {
+                    const double mid = 0.5 * (low + high);
+                    if (enough(mid))
+                        high = mid;
+                    else
+                        low = mid;
+                }
+            }
+            margin = high;
         }
         gpu->predictor_margins[c] = margin;
         widest = std::max(widest, margin);

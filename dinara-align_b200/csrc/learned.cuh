@@ -21,6 +21,17 @@ void predictor_features(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, 
 void predictor_gradients(dinara_gpu *gpu, int batch, const float *features, const float *targets, float *grads,
                          float *loss);
 
+// Pairs drawn on the device from the uneven distribution (reference lengths log-uniform in [length_low,
+// length_high], an error rate uniform in [rate_low, rate_high] split 50/25/25), into the context's letters
+// and offsets buffers (valid until their next use).
+struct GeneratedPairs {
+    int64_t *offsets;
+    uint8_t *letters;
+    int64_t letters_total;
+};
+GeneratedPairs generate_pairs(dinara_gpu *gpu, uint64_t seed, int64_t pairs, double length_low, double length_high,
+                              double rate_low, double rate_high);
+
 // Trains the context's predictor on device-generated pairs and sets its margin.
 void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinara_train_report &report);
 

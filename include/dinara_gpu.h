@@ -216,6 +216,45 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
                                   const dinara_band_plan *plan, int64_t *results, dinara_band_report *report);
 
 /*
+ * The band autotuner (no reference counterpart; the reference's band doubling runs on the host with one
+ * code path). A unit-cost round sweeps each pair's band with a window of G lanes x K 64-bit words, one of
+ * DINARA_BAND_SHAPES shapes; which shape a band takes is set by two figures the autotuner measures on the
+ * context's own device: each shape's sweep rate (words a millisecond, as a relative word cost) and the
+ * bound on a pair's chain of word steps (text letters x K) that gives the fastest band doubling over pairs
+ * drawn from the given distribution. Shapes only decide how a band is swept, so distances never depend
+ * on the tuning. A context starts from fixed defaults until this runs.
+ */
+#define DINARA_BAND_SHAPES 39
+
+typedef struct {
+    uint64_t seed;           /* the probe pairs' generator seed (0: 77) */
+    int64_t pairs;           /* pairs drawn for the chain search (0: 50,000) */
+    double length_low;       /* their reference lengths, log-uniform (0: 100 to 20,000) */
+    double length_high;
+    double rate_low;         /* their error rates, uniform, 50/25/25 (0: 0.5% to 15%) */
+    double rate_high;
+    int64_t probe_length;    /* letters of the pairs each shape is timed on (0: 4,096) */
+    int64_t measure_shapes;  /* nonzero: time every shape first; zero: search the chain bound alone */
+} dinara_band_tune_options;
+
+typedef struct {
+    int64_t shapes;                  /* shapes timed (0 when measure_shapes was zero) */
+    double words_per_ms[40];         /* each shape's sweep rate, shape 6 log2(G) + K - 1 for K <= 6 */
+    int64_t chain_tried;             /* chain bounds tried */
+    int64_t chain_words_tried[8];
+    double chain_ms[8];              /* the band rounds' device time under each */
+    int64_t chain_words;             /* the bound chosen */
+    double seconds;                  /* wall time of the whole tuning */
+} dinara_band_tune_report;
+
+/* Measures and installs the context's band tuning; `options` may be null for the defaults. */
+int64_t dinara_gpu_band_autotune(dinara_gpu *gpu, const dinara_band_tune_options *options,
+                                 dinara_band_tune_report *report);
+/* Reads the context's tuning (`set` 0) or installs one (`set` 1, as a previous run reported it):
+ * the chain bound and DINARA_BAND_SHAPES word costs. */
+int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, float *word_costs);
+
+/*
  * The learned band predictor (no reference counterpart): a 258 -> 64 -> 64 -> 1 fp32 network over a
  * pair's 4-mer count differences, its length ratio and the sum of its squared 6-mer count differences,
  * predicting its distance over its mean length; band

@@ -123,3 +123,26 @@ def test_a_large_batch(da, oracle):
     assert (got[refused] == -1).all()
     keep = np.setdiff1d(np.arange(tape.pairs), refused)
     np.testing.assert_array_equal(got[keep], expected[keep])
+
+
+def test_autotuned_shapes_change_no_distance(da, oracle):
+    """The band autotuner measures every window shape and a chain bound, installs them, and distances
+    under the tuned shapes (and under a tuning that sends every band to its slowest shape) still equal
+    the oracle's; a tuning read back installs again."""
+    from dinara_align import tuning, workloads
+
+    report = tuning.autotune(pairs=3000, length=(100, 6000), probe_length=2048)
+    assert len(report["words_per_ms"]) == tuning.SHAPES
+    assert all(rate > 0 for rate in report["words_per_ms"].values())
+    assert report["chain_words"] in report["chain_ms"]
+    tape = workloads.uneven_unit_cost(600, high=8000, seed=31)
+    expected = _oracle_distances(oracle, tape)
+    np.testing.assert_array_equal(da.distances_tape(tape), expected)
+    kept = tuning.tuning()
+    assert kept["chain_words"] == report["chain_words"]
+    # Inverted costs: the chooser now prefers what the device measured slowest, and chains of one step.
+    inverted = {"chain_words": 1, "word_costs": [1.0 / cost for cost in kept["word_costs"]]}
+    tuning.install(inverted)
+    np.testing.assert_array_equal(da.distances_tape(tape), expected)
+    tuning.install(kept)
+    assert tuning.tuning() == kept

@@ -66,3 +66,14 @@ def test_sam_fields():
     assert gapped.mismatch_string("ACGTTGA", "ACTGCA") == "2^GT3"
     assert gapped.edit_distance("ACGTTGA", "ACTGCA") == 3
     assert da.Costs.affine(4, 6, 2).with_deletions(20, 5).unit_scale() == 0 and da.Costs.linear(3, 3).unit_scale() == 3
+
+
+def test_band_tuning_needs_a_context():
+    """The autotuner's entry points refuse a missing context with a code."""
+    handle = ctypes.CDLL(LIBRARY)
+    handle.dinara_gpu_band_tuning.restype = ctypes.c_int64
+    chain = ctypes.c_int64(0)
+    costs = (ctypes.c_float * 39)()
+    assert handle.dinara_gpu_band_tuning(None, 0, ctypes.byref(chain), costs) == -6
+    handle.dinara_gpu_band_autotune.restype = ctypes.c_int64
+    assert handle.dinara_gpu_band_autotune(None, None, None) == -6
