@@ -340,19 +340,23 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                 const uint32_t c = (codes[1][j >> 4] >> (2 * (j & 15))) & 3u;
                 window[j] = (17u * a + 128u) | ((17u * c + 196u) << 8);
             }
+            // The window's rows' reference letters, read before the rows are swept so no global load waits
+            // inside a row (rows past a pair's end read letter 0, which no real cell uses).
+            uint32_t row_codes[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t run[2];
+                run_of_letters(b.tape, sh[h].first_word, live[h] ? rows[h] : 0, r0 - 1, run);
+                row_codes[h] = run[0];
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int row = r0 + u;
                 if (row <= warp_rows) {
                     const uint32_t nextH = __shfl_down_sync(kFull, H[0], 1, G);
                     const uint32_t nextD = __shfl_down_sync(kFull, D[0], 1, G);
-                    uint32_t x_letter[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h)
-                        x_letter[h] = (live[h] && row <= rows[h])
-                                          ? letter_at<2>(b.tape, sh[h].first_word, uint32_t(row - 1))
-                                          : 0u;
-                    const uint32_t trA = rows8[x_letter[0]], trB = rows8[x_letter[1]];
+                    const uint32_t trA = rows8[(row_codes[0] >> (2 * u)) & 3u];
+                    const uint32_t trB = rows8[(row_codes[1] >> (2 * u)) & 3u];
                     uint32_t X[C];
                     uint32_t S = unreached2;  // running max of X + opening along this lane's places
                     // Decision planes, each a bit a place for both pairs (see gather_flag).
