@@ -416,6 +416,122 @@ struct PhaseTimer {
     }
 };
 
+// A widening band round's routing. A pair swept over its band of `swept[k]` diagonals keeps its score
+// when the band proves it (band_proves_width), or when the band could not hold both ends (the sweep was
+// then whole). Otherwise the band's score, a real alignment's, says how wide a band would prove a score
+// that good: g gap letters outside it must cost more than the score, g > (4 (open - extend) + best (rows +
+// columns) - 2 score) / (best - 2 extend). The pair goes round again at that width (at least twice the
+// last, rounded up to 1,024 diagonals) unless this is the `last` round or that band's strips would sweep
+// three fifths of its rows or more: then to the whole-matrix list. With `swept` null, every pair is
+// routed to `first_width`.
+__global__ void wide_route_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ pending,
+                                  const int32_t *__restrict__ swept, int64_t count, int32_t first_width, bool last,
+                                  const int32_t *__restrict__ scores, int32_t best, int32_t open, int32_t extend,
+                                  uint32_t *__restrict__ next, int32_t *__restrict__ next_width,
+                                  unsigned int *__restrict__ next_count, uint32_t *__restrict__ whole,
+                                  unsigned int *__restrict__ whole_count) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t pair = pending[k];
+    const PairShape sh = shapes[pair];
+    const int64_t rows = sh.rows, columns = sh.columns;
+    int64_t width = first_width;
+    if (swept) {
+        const int64_t done = swept[k];
+        const int32_t low = band_low_for_width(rows, columns, done);
+        if (low == INT32_MIN) return;
+        const int64_t score = scores[pair];
+        if (band_proves_width(score, rows, columns, low, done, best, open, extend)) return;
+        const int64_t per_letter = int64_t(best) - 2 * int64_t(extend);
+        if (per_letter <= 0) {  // no band proves anything narrower than the matrix
+            whole[atomicAdd(whole_count, 1u)] = pair;
+            return;
+        }
+        const int64_t g = (4 * (int64_t(open) - extend) + int64_t(best) * (rows + columns) - 2 * score) / per_letter + 2;
+        const int64_t delta = columns > rows ? columns - rows : rows - columns;
+        width = max(2 * done, g + delta + 2);
+        width = (width + 1023) / 1024 * 1024;
+    }
+    const bool banded = !last && width < (int64_t(1) << 30) && band_low_for_width(rows, columns, width) != INT32_MIN &&
+                        10 * (int64_t(sweep::kBlock) * 16 + width) < 6 * rows;
+    if (banded) {
+        const unsigned at = atomicAdd(next_count, 1u);
+        next[at] = pair;
+        next_width[at] = int32_t(width);
+    } else {
+        whole[atomicAdd(whole_count, 1u)] = pair;
+    }
+}
+
+// Scores of long global pairs (the block-a-pair class) by a widening band: a first round sweeps each pair
+// over 2,048 diagonals; a pair its band does not prove goes round once more at the width its band score
+// says would prove it, or is swept whole when that band would cover most of its matrix (or its second
+// band proves nothing either). Every score is the whole matrix's.
+void widening_band(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const uint32_t *order,
+                   int64_t count, KernelArgs args) {
+    if (count <= 0) return;
+    const TableArgs targs = table_args(table, false);
+    int32_t best = -128;
+    for (int r = 0; r < table.size; ++r)
+        for (int c = 0; c < table.size; ++c) best = std::max(best, table.entries[r * 32 + c]);
+    uint32_t *lists = gpu->wide_pending.ensure<uint32_t>(5 * size_t(count));
+    uint32_t *whole = lists + 2 * count;
+    int32_t *widths = reinterpret_cast<int32_t *>(lists + 3 * count);
+    unsigned int *counts = gpu->class_counts.ensure<unsigned int>(16) + 9;  // [0] next, [1] whole
+    DINARA_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned int), gpu->stream));
+    constexpr int32_t kFirstWidth = 2048;
+    constexpr int kBandRounds = 2;
+    const uint32_t *pending = order;
+    const int32_t *swept = nullptr;
+    int64_t left = count;
+    for (int round = 0; round <= kBandRounds && left > 0; ++round) {
+        uint32_t *next = lists + (round & 1) * count;
+        int32_t *next_widths = widths + (round & 1) * count;
+        DINARA_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned int), gpu->stream));
+        wide_route_kernel<<<unsigned((left + 255) / 256), 256, 0, gpu->stream>>>(
+            batch.shapes, pending, swept, left, kFirstWidth, round == kBandRounds, args.scores, best, table.open,
+            table.extend, next, next_widths, counts, whole, counts + 1);
+        DINARA_CUDA(cudaGetLastError());
+        gpu->launches += 1;
+        unsigned int routed = 0;
+        read_back(gpu, &routed, counts, sizeof routed);
+        left = routed;
+        if (left == 0) break;
+        int64_t blocks = persistent_blocks(gpu, &affine_wide_kernel<false, true>);
+        blocks = std::max<int64_t>(1, std::min(blocks, left));
+        args.carry_stride = int64_t(batch.max_rows) + 1;
+        args.carry = gpu->carry.ensure<int2>(size_t(blocks * args.carry_stride));
+        args.order = next;
+        args.band_widths = next_widths;
+        args.begin = 0;
+        args.end = uint32_t(left);
+        ClockSpan clock(gpu, kClassWhole, gpu->stream);
+        affine_wide_kernel<false, true><<<unsigned(blocks), kBlock, 0, gpu->stream>>>(args, targs, nullptr);
+        DINARA_CUDA(cudaGetLastError());
+        clock.stop();
+        gpu->launches += 1;
+        pending = next;
+        swept = next_widths;
+    }
+    unsigned int swept_whole = 0;
+    read_back(gpu, &swept_whole, counts + 1, sizeof swept_whole);
+    if (swept_whole > 0) {
+        int64_t blocks = persistent_blocks(gpu, &affine_wide_kernel<false, false>);
+        blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, swept_whole));
+        args.carry_stride = int64_t(batch.max_rows) + 1;
+        args.carry = gpu->carry.ensure<int2>(size_t(blocks * args.carry_stride));
+        args.order = whole;
+        args.band_widths = nullptr;
+        args.begin = 0;
+        args.end = swept_whole;
+        ClockSpan clock(gpu, kClassWhole, gpu->stream);
+        affine_wide_kernel<false, false><<<unsigned(blocks), kBlock, 0, gpu->stream>>>(args, targs, nullptr);
+        DINARA_CUDA(cudaGetLastError());
+        clock.stop();
+        gpu->launches += 1;
+    }
+}
+
 void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const Schedule &schedule,
                        bool record, KernelArgs args) {
     const bool smem = !table.packed16 || batch.bits == 8;
@@ -430,7 +546,12 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
         const bool wide = bucket == kWideClass;
         const bool pairs16 = !wide && bucket >= kWholePairsClass;
         const int cls = pairs16 ? bucket - kWholePairsClass : wide ? 4 : bucket;
-        KernelFn fn = wide      ? (batch.local ? &affine_wide_kernel<true> : &affine_wide_kernel<false>)
+        if (wide && !batch.local && !record && band_serves(batch, table)) {
+            // Long global pairs take the widening band first.
+            widening_band(gpu, batch, table, schedule.order + b.begin[bucket], b.end[bucket] - b.begin[bucket], args);
+            continue;
+        }
+        KernelFn fn = wide      ? (batch.local ? &affine_wide_kernel<true, false> : &affine_wide_kernel<false, false>)
                       : pairs16 ? pick_pairs_kernel(cls, batch.local)
                                 : pick_kernel(cls, batch.local, record, batch.bits, smem);
         const int G = wide ? kBlock : smem && !pairs16 ? 32 : affine_lanes(cls);

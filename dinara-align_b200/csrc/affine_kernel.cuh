@@ -50,7 +50,21 @@ struct KernelArgs {
     const int64_t *decision_offsets;
     int64_t *ends;  // local: (row << 32) | column of the best cell
     int64_t first_pair;
+    // The widening band (affine_wide_kernel<false, true>): the pair at order[item] is swept over
+    // band_widths[item] diagonals from band_low_for_width; the pairs whose band proves nothing are redone
+    // wider or whole.
+    const int32_t *band_widths;
 };
+
+// The lowest diagonal (column less row) of a band of `width` diagonals holding a pair's main and end
+// diagonals, the slack shared either side; INT32_MIN when the band cannot hold both.
+__host__ __device__ inline int32_t band_low_for_width(int64_t rows, int64_t columns, int64_t width) {
+    const int64_t delta = columns - rows;
+    const int64_t span = delta < 0 ? -delta : delta;
+    if (span + 1 > width) return INT32_MIN;
+    const int64_t slack = (width - 1 - span) / 2;
+    return int32_t((delta < 0 ? delta : 0) - slack);
+}
 
 struct TableArgs {
     uint2 rows16[4];       // packed 16-bit entries, letter x at bytes 2x..2x+1
@@ -510,11 +524,19 @@ __global__ void __launch_bounds__(kBlock) affine_pairs_kernel(KernelArgs p, Tabl
 // with that barrier, so no warp waits on another in any other way.
 // ------------------------------------------------------------------------------------------------
 
-template <bool LOCAL>
+// One long pair a block of kBlock lanes, strips of kBlock x 16 columns; see the file's notes. With BANDED
+// (global only) a strip sweeps only the rows its columns share with the pair's band of band_widths[item]
+// diagonals [low, high]: rows from its first column less high to its last column less low. The cells it
+// sweeps outside the band are real cells, and every cell around the swept rows is unreached, so the
+// score is the best over paths within the swept rows: at least the band's best, and the whole matrix's
+// when the band proves it (band_proves_width).
+template <bool LOCAL, bool BANDED>
 __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__) {
     constexpr int C = 16;
     constexpr int W = kBlock * C;
     constexpr int kWarps = kBlock / 32;
+    constexpr int32_t kOut = -(1 << 28);  // unreached: below every score ScoreReach lets a pair hold
+    static_assert(!(LOCAL && BANDED), "the band proof is for global alignments");
     __shared__ uint2 rows16[4];
     __shared__ int2 handoff[2][kWarps];
     __shared__ int32_t block_best[kWarps];
@@ -535,29 +557,52 @@ __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, Table
         const int rows = int(sh.rows), cols = int(sh.columns);
         const int strips = (cols + W - 1) / W;
         int32_t best = 0;
+        // The band's diagonals; a pair whose band cannot hold both ends is swept whole.
+        int low = -rows, high = cols;
+        if (BANDED) {
+            const int32_t width = p.band_widths[item];
+            const int32_t from = band_low_for_width(rows, cols, width);
+            if (from != INT32_MIN) {
+                low = from;
+                high = from + width - 1;
+            }
+        }
+        int previous_last = rows;  // the previous strip's last swept row
 
         for (int s = 0; s < strips; ++s) {
             const int first_col = s * W + member * C;
             const int owned = min(max(cols - first_col, 0), C);
+            // The strip's rows: those its columns share with the band (all of them when not banded).
+            const int first_row = BANDED ? max(1, s * W - high) : 1;
+            const int last_row = BANDED ? min(rows, s * W + W - 1 - low) : rows;
             uint32_t sel[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {
                 const int col = first_col + k;
                 sel[k] = col < cols ? selector_of(letter_at<2>(p.tape, sh.second_word, uint32_t(col))) : kPadSelector;
             }
-            const int32_t top = LOCAL ? 0 : opening;
+            // The row above the strip's first: the matrix's top border, or (a strip starting lower, whose
+            // cells above lie outside the band) unreached.
+            const bool from_top = first_row == 1;
+            const int32_t top = from_top ? (LOCAL ? 0 : opening) : kOut;
             int32_t H[C], D[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {
                 H[k] = top;
-                D[k] = top + first_gap;
+                D[k] = from_top ? top + first_gap : kOut;
             }
-            int32_t edgeH = top, edgeI = top + first_gap;
+            int32_t edgeH = top, edgeI = from_top ? top + first_gap : kOut;
             int32_t above_left = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
-            const int steps = rows + kBlock;
+            if (BANDED && !from_top) {
+                // The cell above and left of the first row: the previous strip's last column (in the band)
+                // for lane 0, else outside the band.
+                above_left = kOut;
+                if (member == 0 && s > 0) above_left = p.carry[slot * p.carry_stride + (first_row - 1)].x;
+            }
+            const int steps = last_row - first_row + 1 + kBlock;
 
             for (int step = 1; step <= steps; ++step) {
-                const int row = step - member;
+                const int row = first_row - 1 + step - member;
                 int32_t leftH = __shfl_up_sync(kFull, edgeH, 1);
                 int32_t leftI = __shfl_up_sync(kFull, edgeI, 1);
                 if (lane == 0) {
@@ -565,6 +610,9 @@ __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, Table
                         if (s == 0) {
                             leftH = LOCAL ? 0 : opening;
                             leftI = leftH + first_gap;
+                        } else if (BANDED && row > previous_last) {
+                            leftH = kOut;  // left of the previous strip's swept rows: outside the band
+                            leftI = kOut;
                         } else {
                             const int r = min(max(row, 0), rows);
                             const int2 c = p.carry[slot * p.carry_stride + r];
@@ -579,7 +627,7 @@ __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, Table
                 }
                 int32_t diag = above_left;
                 above_left = leftH;
-                if (row >= 1 && row <= rows) {
+                if (row >= first_row && row <= last_row) {
                     const uint32_t rl = letter_at<2>(p.tape, sh.first_word, uint32_t(row - 1));
                     const uint2 tr = rows16[rl];
                     int32_t I = 0, Xprev = 0;
@@ -623,6 +671,7 @@ __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, Table
                 if (lane == 31) handoff[step & 1][warp] = make_int2(edgeH, edgeI);
                 __syncthreads();
             }
+            previous_last = last_row;
         }
         if (LOCAL) {
             const int32_t mine = warp_max(best);

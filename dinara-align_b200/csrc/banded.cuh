@@ -50,6 +50,20 @@ __host__ __device__ inline bool band_proves(int64_t score, int64_t rows, int64_t
     return true;
 }
 
+// band_proves for a band of `width` diagonals from `low`: the same bound, the nearest diagonals outside
+// being low - 1 and low + width.
+__host__ __device__ inline bool band_proves_width(int64_t score, int64_t rows, int64_t columns, int64_t low,
+                                                  int64_t width, int64_t best, int64_t open, int64_t extend) {
+    if (2 * extend - best > 0) return false;
+    const int64_t delta = columns - rows;
+    const int64_t high = low + width - 1;
+    const int64_t twice = 2 * score;
+    auto bound = [&](int64_t g) { return best * (rows + columns) + g * (2 * extend - best) + 4 * (open - extend); };
+    if (high + 1 <= columns && !(twice > bound(2 * (high + 1) - delta))) return false;
+    if (low - 1 >= -rows && !(twice > bound(delta - 2 * (low - 1)))) return false;
+    return true;
+}
+
 // The 16-bit pair sweep (banded_pairs_kernel) holds every value a pair's band takes as a 16-bit half of a
 // register: real cells plus kPairBias, cells no path reaches from kPairUnreached up. With K the largest
 // step a cell takes from its neighbour (the largest shifted table entry, or a gap's opening), a real
