@@ -64,6 +64,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-parity", action="store_true")
     parser.add_argument("--no-sections", action="store_true", help="only the headline workload")
+    parser.add_argument("--tuning", default="",
+                        help="band tuning file: loaded when the file exists, else measured and saved there")
     parser.add_argument("--predictor", default="",
                         help="band predictor blob: loaded when the file exists, else trained and saved there")
     parser.add_argument("--selftest-ranks", action="store_true",
@@ -396,7 +398,15 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
     placement = da.Placement.on_gpu(ranks.local_rank)
     # The band autotuner first: both arms then sweep with the shapes it measured, and the predictor's
     # margins are calibrated against the windows those shapes give.
-    tuned = tuning.autotune(placement)
+    tuning_file = ctx.get("tuning", "")
+    if tuning_file and os.path.exists(tuning_file):
+        tuning.load(tuning_file, placement)
+        tuned = {"chain_words": tuning.tuning(placement)["chain_words"], "chain_ms": {}, "seconds": 0.0,
+                 "words_per_ms": {}, "loaded": tuning_file}
+    else:
+        tuned = tuning.autotune(placement)
+        if tuning_file:
+            tuning.save(tuning_file, placement)
     predictor = learned.Predictor(placement)
     blob = ctx.get("predictor", "")
     if blob and os.path.exists(blob):
@@ -736,7 +746,8 @@ def main() -> None:
     handle = native.context(ranks.local_rank)
     peaks = int32_peaks(handle, lib)
     ctx = {"da": da, "native": native, "lib": lib, "handle": handle, "ranks": ranks, "peaks": peaks,
-           "e2e": not args.no_e2e, "parity": not args.no_parity, "predictor": args.predictor}
+           "e2e": not args.no_e2e, "parity": not args.no_parity, "predictor": args.predictor,
+           "tuning": args.tuning}
     head = run_workload(ctx, args.workload, args.pairs, args.steps, args.warmup, not args.no_cpu)
     begin, end = head.pop("timed_region")
     sections = {}

@@ -257,6 +257,15 @@ __device__ __forceinline__ uint32_t gather_flag(uint32_t acc, uint32_t v, int k)
     return k == 15 ? acc + flags : __umulhi(flags, 1u << (17 + k)) + acc;
 }
 
+// b - a + c (the halves' sums in [0, 0x10000), so none crosses into the other) by two multiply-adds,
+// which the multiply-add pipe takes, leaving the ALU pipe, the recording sweep's bound, to the cells.
+__device__ __forceinline__ uint32_t difference_mad(uint32_t b, uint32_t a, uint32_t c) {
+    uint32_t biased, out;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(biased) : "r"(b), "r"(1u), "r"(c));
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(out) : "r"(a), "r"(0xFFFFFFFFu), "r"(biased));
+    return out;
+}
+
 template <bool RECORD>
 __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) {
     constexpr int G = kBandLanes, C = kBandColumns;
@@ -374,8 +383,8 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                             X[k] = max2(xd, dn);
                             // gotoh.mojo:173-186 decide: the source leaves the diagonal only where the
                             // deletion beats it; a deletion run extends only where extending beats opening.
-                            deleting = gather_flag(deleting, xd - dn + at_least, k);               // dn > xd
-                            deletion_runs = gather_flag(deletion_runs, Hup - Dup + at_least_open, k);  // Dup > Hup + opening
+                            deleting = gather_flag(deleting, difference_mad(xd, dn, at_least), k);               // dn > xd
+                            deletion_runs = gather_flag(deletion_runs, difference_mad(Hup, Dup, at_least_open), k);  // Dup > Hup + opening
                             S = __viaddmax_s16x2(X[k], opening2, S);
                         } else {
                             const uint32_t x = __viaddmax_s16x2(H[k], sub, dn);
@@ -406,9 +415,9 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                             const uint32_t I = S2;
                             S2 = __viaddmax_s16x2(X[k], opening2, S2);
                             H[k] = max2(X[k], I);
-                            inserting = gather_flag(inserting, X[k] - I + at_least, k);  // I > X
+                            inserting = gather_flag(inserting, difference_mad(X[k], I, at_least), k);  // I > X
                             // The left cell's insertion beats its score plus an opening: the run extends.
-                            if (k > 0) insertion_runs = gather_flag(insertion_runs, prevH - prevI + at_least_open, k);
+                            if (k > 0) insertion_runs = gather_flag(insertion_runs, difference_mad(prevH, prevI, at_least_open), k);
                             prevH = H[k];
                             prevI = I;
                         }
