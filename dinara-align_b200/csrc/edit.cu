@@ -650,8 +650,9 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
             BandFn fn = pick_band(shape);
             int per_sm = 0;
             DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
-            const double share =
-                total_work > 0 ? double(host->shape_work[shape]) * tuning.word_cost[shape] / total_work : 1.0;
+            const double share = tuning.full_grids || total_work <= 0
+                                     ? 1.0
+                                     : double(host->shape_work[shape]) * tuning.word_cost[shape] / total_work;
             int64_t grid = int64_t(std::ceil(share * std::max(per_sm, 1) * gpu->multiprocessors));
             const int64_t needed = (n_shape + groups_per_block - 1) / groups_per_block;
             grid = std::max<int64_t>(1, std::min(grid, needed));

@@ -117,6 +117,7 @@ inline BandTuning default_band_tuning() {
     for (int s = 0; s < BandTuning::kShapes; ++s)
         t.word_cost[s] = s < kBandShapes ? 40.f + 18.f / float(band_words_per_lane(s)) : 1e30f;
     t.tuned = 0;
+    t.full_grids = 0;
     return t;
 }
 
@@ -138,9 +139,10 @@ double band_shape_rate(dinara_gpu *gpu, int shape, int64_t pairs, const uint8_t 
 int band_shape_blocks(dinara_gpu *gpu, int shape);
 
 // The band autotuner (tune.cu): each shape's sweep rate and the chain bound, measured on the device and
-// set on the context; and the tuning read back or installed (`set`), DINARA_BAND_SHAPES word costs.
+// set on the context; and the tuning read back or installed (`set`): the chain bound, the grids' scheme and
+// DINARA_BAND_SHAPES word costs.
 void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, dinara_band_tune_report &report);
-void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, float *word_costs);
+void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, int64_t *full_grids, float *word_costs);
 
 // Runs band doubling over a batch whose ASCII letters and offsets are on the device already; writes
 // every pair's distance (or its code) to `results` (device) and fills `report`. `letters` starts on a

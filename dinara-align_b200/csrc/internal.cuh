@@ -135,6 +135,10 @@ struct BandTuning {
     int64_t chain_words;
     float word_cost[kShapes];
     int32_t tuned;  // 1 once the autotuner has set them on this context
+    // How a round's launches (one a shape, all at once on side streams) share the GPU: 0 each takes the
+    // share of its lanes that its share of the round's time asks for; 1 each may fill the GPU, later
+    // launches' blocks starting as earlier ones' finish.
+    int32_t full_grids;
 };
 
 }  // namespace dinara

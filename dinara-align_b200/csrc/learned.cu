@@ -799,8 +799,9 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
     // pair settles when its distance lies within the band its first window sweeps (band_reach: a window
     // holds a wider band than the threshold needs, for nothing), with the window the first round would
     // give it under the context's tuning. A pair that misses sweeps again, and the round it adds lasts as
-    // long as its longest pair's sweep, so the longer classes are held to a higher share: the asked
-    // coverage for pairs under 1,000 letters, a third of the misses past it under 4,096, a tenth longer.
+    // long as its longest pair's chain of word steps, so the longer classes are held to a higher share: of
+    // the asked coverage's misses, all for pairs under 300 letters, half under 1,000, 3% under 4,096 and
+    // 0.3% longer (97%, 98.5%, 99.91% and 99.991% at the default 97%).
     struct HeldPair {
         int64_t n, m, d;
         double guess;
@@ -835,7 +836,7 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
         return h.d <= delta + 2 * std::max(half, reach) + 1;
     };
     const double coverage = std::min(std::max(options.coverage, 0.5), 0.999);
-    const double misses[4] = {1.0, 1.0, 1.0 / 3.0, 0.1};
+    const double misses[4] = {1.0, 0.5, 0.03, 0.003};
     double widest = 0.0;
     for (int c = 0; c < 4; ++c) {
         double margin = 1.0;

@@ -14,8 +14,9 @@
 namespace dinara {
 namespace {
 
-constexpr int64_t kChainCandidates[] = {12000, 24000, 48000, 96000, 192000};
+constexpr int64_t kChainCandidates[] = {12000, 24000, 48000, 96000};
 constexpr int kChainCount = int(sizeof(kChainCandidates) / sizeof(kChainCandidates[0]));
+static_assert(2 * kChainCount <= 8, "the report holds every candidate");
 
 // Each shape's words a millisecond, timed on pairs at least `length` letters long and at least eight words
 // taller than the shape's window (so every lane sweeps words inside the pattern), at least two full waves
@@ -87,14 +88,17 @@ void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, din
         }
         out.shapes = kBandShapes;
     }
-    // 2. The chain bound: plain band doubling over pairs of the distribution, twice a candidate.
+    // 2. The chain bound and the launches' grids: plain band doubling over pairs of the distribution, twice
+    // a candidate.
     const GeneratedPairs generated =
         generate_pairs(gpu, o.seed + 1, o.pairs, o.length_low, o.length_high, o.rate_low, o.rate_high);
     int64_t *results = gpu->features.ensure<int64_t>(size_t(o.pairs));
     double best_ms = 0.0;
     int64_t best_chain = tuning.chain_words;
-    for (int c = 0; c < kChainCount; ++c) {
-        tuning.chain_words = kChainCandidates[c];
+    int32_t best_grids = tuning.full_grids;
+    for (int c = 0; c < 2 * kChainCount; ++c) {
+        tuning.chain_words = kChainCandidates[c % kChainCount];
+        tuning.full_grids = c / kChainCount;
         gpu->band_tuning = tuning;
         double fastest_run = 0.0;
         for (int repeat = 0; repeat < 2; ++repeat) {
@@ -103,22 +107,25 @@ void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, din
             band_doubling(gpu, o.pairs, generated.letters, generated.offsets, nullptr, 0, results, &band);
             if (repeat == 0 || band.kernel_ms < fastest_run) fastest_run = band.kernel_ms;
         }
-        out.chain_words_tried[c] = kChainCandidates[c];
+        out.chain_words_tried[c] = tuning.full_grids ? -tuning.chain_words : tuning.chain_words;
         out.chain_ms[c] = fastest_run;
         if (c == 0 || fastest_run < best_ms) {
             best_ms = fastest_run;
-            best_chain = kChainCandidates[c];
+            best_chain = tuning.chain_words;
+            best_grids = tuning.full_grids;
         }
     }
-    out.chain_tried = kChainCount;
+    out.chain_tried = 2 * kChainCount;
+    out.full_grids = best_grids;
     tuning.chain_words = best_chain;
+    tuning.full_grids = best_grids;
     tuning.tuned = 1;
     gpu->band_tuning = tuning;
     out.chain_words = best_chain;
     out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - began).count();
 }
 
-void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, float *word_costs) {
+void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, int64_t *full_grids, float *word_costs) {
     if (gpu->band_tuning.chain_words == 0) gpu->band_tuning = default_band_tuning();
     if (set) {
         if (*chain_words < 1) throw Failure(DINARA_INVALID_LENGTH, "a chain bound below one word step");
@@ -126,11 +133,13 @@ void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, float *
             if (!(word_costs[s] > 0.f) || !std::isfinite(word_costs[s]))
                 throw Failure(DINARA_INVALID_LENGTH, "a word cost that is not a positive number");
         gpu->band_tuning.chain_words = *chain_words;
+        gpu->band_tuning.full_grids = *full_grids ? 1 : 0;
         for (int s = 0; s < kBandShapes; ++s) gpu->band_tuning.word_cost[s] = word_costs[s];
         gpu->band_tuning.tuned = 1;
         return;
     }
     *chain_words = gpu->band_tuning.chain_words;
+    *full_grids = gpu->band_tuning.full_grids;
     for (int s = 0; s < kBandShapes; ++s) word_costs[s] = gpu->band_tuning.word_cost[s];
 }
 

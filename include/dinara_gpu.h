@@ -240,10 +240,11 @@ typedef struct {
 typedef struct {
     int64_t shapes;                  /* shapes timed (0 when measure_shapes was zero) */
     double words_per_ms[40];         /* each shape's sweep rate, shape 6 log2(G) + K - 1 for K <= 6 */
-    int64_t chain_tried;             /* chain bounds tried */
-    int64_t chain_words_tried[8];
+    int64_t chain_tried;             /* candidates tried (the first 8 reported) */
+    int64_t chain_words_tried[8];    /* each one's chain bound, negative where its launches fill the GPU */
     double chain_ms[8];              /* the band rounds' device time under each */
     int64_t chain_words;             /* the bound chosen */
+    int64_t full_grids;              /* 1 when the chosen launches each fill the GPU, 0 when they share it */
     double seconds;                  /* wall time of the whole tuning */
 } dinara_band_tune_report;
 
@@ -251,8 +252,10 @@ typedef struct {
 int64_t dinara_gpu_band_autotune(dinara_gpu *gpu, const dinara_band_tune_options *options,
                                  dinara_band_tune_report *report);
 /* Reads the context's tuning (`set` 0) or installs one (`set` 1, as a previous run reported it):
- * the chain bound and DINARA_BAND_SHAPES word costs. */
-int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, float *word_costs);
+ * the chain bound, whether a round's launches each fill the GPU (1) or share it (0), and
+ * DINARA_BAND_SHAPES word costs. */
+int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, int64_t *full_grids,
+                               float *word_costs);
 
 /*
  * The learned band predictor (no reference counterpart): a 258 -> 64 -> 64 -> 1 fp32 network over a
