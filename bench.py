@@ -64,6 +64,8 @@ def parse() -> argparse.Namespace:
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-parity", action="store_true")
     parser.add_argument("--no-sections", action="store_true", help="only the headline workload")
+    parser.add_argument("--arms", choices=["both", "learned", "plain"], default="both",
+                        help="the uneven workload's arms to run (profiling one at a time)")
     parser.add_argument("--tuning", default="",
                         help="band tuning file: loaded when the file exists, else measured and saved there")
     parser.add_argument("--predictor", default="",
@@ -401,10 +403,11 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
     tuning_file = ctx.get("tuning", "")
     if tuning_file and os.path.exists(tuning_file):
         tuning.load(tuning_file, placement)
-        tuned = {"chain_words": tuning.tuning(placement)["chain_words"], "chain_ms": {}, "seconds": 0.0,
-                 "words_per_ms": {}, "loaded": tuning_file}
+        kept = tuning.tuning(placement)
+        tuned = {"chain_words": kept["chain_words"], "chain_share": kept["chain_share"], "chain_ms": {},
+                 "seconds": 0.0, "words_per_ms": {}, "loaded": tuning_file}
     else:
-        tuned = tuning.autotune(placement)
+        tuned = tuning.autotune(placement, pairs=tape.pairs)
         if tuning_file:
             tuning.save(tuning_file, placement)
     predictor = learned.Predictor(placement)
@@ -433,7 +436,9 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
 
     found = {}
     out = {}
-    for name, policy in (("learned", native.BAND_LEARNED), ("plain", native.BAND_PLAIN)):
+    arms = [(name, policy) for name, policy in (("learned", native.BAND_LEARNED), ("plain", native.BAND_PLAIN))
+            if ctx.get("arms", "both") in ("both", name)]
+    for name, policy in arms:
         timings, begin, end = timed_steps(stepper(policy, name), steps, warmup, ranks)
         device_ms = ranks.max(sum(t.total_ms for t in timings))
         result = np.zeros(tape.pairs, dtype=np.int64)
@@ -446,6 +451,12 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
                      "band_ms_per_step": sum(t.class_ms[CLASS_UNIT_BAND] for t in timings) / steps,
                      "predict_ms_per_step": sum(t.class_ms[CLASS_PREDICT] for t in timings) / steps,
                      "report": reports[name], "timed_region": [begin, end]}
+    if len(out) == 1:
+        # One arm alone (a profiling run): its own figures, no comparison.
+        (name, only), = out.items()
+        return {"value": only["pairs_per_s"], "ms_per_step": only["ms_per_step"],
+                "gpu_launches": int(only["launches_per_step"] * steps), "timed_region": only["timed_region"],
+                "arm": name, name: only, "training": training}
     line = {"value": out["learned"]["pairs_per_s"], "ms_per_step": out["learned"]["ms_per_step"],
             "gpu_launches": int(out["learned"]["launches_per_step"] * steps),
             "timed_region": out["learned"]["timed_region"],
@@ -454,7 +465,8 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
             "identical_distances": bool((found["learned"] == found["plain"]).all()),
             "gcups": out["learned"]["gcups_full_matrix"], "plain_gcups": out["plain"]["gcups_full_matrix"],
             "learned": out["learned"], "plain": out["plain"], "training": training,
-            "autotune": {"chain_words": tuned["chain_words"], "chain_ms": tuned["chain_ms"],
+            "autotune": {"chain_words": tuned["chain_words"], "chain_share": tuned["chain_share"],
+                         "chain_ms": tuned["chain_ms"],
                          "seconds": tuned["seconds"], "words_per_ms": tuned["words_per_ms"]}}
     # The dominant kernel: every round's band kernels. A Myers/Hyyro word step is about 20 u64 operations
     # (bit_parallel.mojo:10-11), 40 in int32 terms, over the words the rounds swept.
@@ -747,7 +759,7 @@ def main() -> None:
     peaks = int32_peaks(handle, lib)
     ctx = {"da": da, "native": native, "lib": lib, "handle": handle, "ranks": ranks, "peaks": peaks,
            "e2e": not args.no_e2e, "parity": not args.no_parity, "predictor": args.predictor,
-           "tuning": args.tuning}
+           "tuning": args.tuning, "arms": args.arms}
     head = run_workload(ctx, args.workload, args.pairs, args.steps, args.warmup, not args.no_cpu)
     begin, end = head.pop("timed_region")
     sections = {}

@@ -1482,12 +1482,10 @@ int64_t dinara_gpu_band_autotune(dinara_gpu *gpu, const dinara_band_tune_options
     });
 }
 
-int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, int64_t *full_grids,
-                               float *word_costs) {
+int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, dinara_band_tuning *tuning) {
     return guard(gpu, [&]() -> int64_t {
-        if (!gpu || !chain_words || !full_grids || !word_costs)
-            throw Failure(DINARA_INVALID_MODE, "no context or tuning arrays");
-        band_tuning_access(gpu, set != 0, chain_words, full_grids, word_costs);
+        if (!gpu || !tuning) throw Failure(DINARA_INVALID_MODE, "no context or tuning");
+        band_tuning_access(gpu, set != 0, tuning);
         return 0;
     });
 }

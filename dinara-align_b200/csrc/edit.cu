@@ -351,6 +351,7 @@ struct BandCounters {
     unsigned queues[kBandShapes + 1];                // each shape's launch's next item
     unsigned long long swept;
     unsigned long long tallies[4];
+    unsigned long long round_work;
 };
 constexpr size_t kCountsBytes = offsetof(BandCounters, queues);
 static_assert(kCountsBytes <= kReadbackBytes, "a round's counts fit the readback words");
@@ -387,6 +388,30 @@ __global__ void band_keys_kernel(const EditPair *__restrict__ pairs, const uint3
             atomicAdd(&counters->shape_work[s], block_work[s]);
         }
     }
+}
+
+// A round's work in its smallest windows: every pending pair's text letters times the words of the
+// smallest shape holding its band (at most its pattern's), summed in the block first.
+__global__ void round_work_kernel(const EditPair *__restrict__ pairs, const uint32_t *__restrict__ pending,
+                                  const unsigned int *__restrict__ pending_count, const int64_t *__restrict__ thresholds,
+                                  unsigned long long *__restrict__ work) {
+    __shared__ unsigned long long block_work;
+    if (threadIdx.x == 0) block_work = 0;
+    __syncthreads();
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < *pending_count) {
+        const EditPair e = pairs[pending[k]];
+        const int64_t needed = band_words_needed(e.n, e.m, thresholds[pending[k]]);
+        int64_t smallest = INT64_MAX;
+        for (int s = 0; s < kBandShapes; ++s) {
+            const int64_t c = band_capacity(s);
+            if (c >= needed && c < smallest) smallest = c;
+        }
+        if (smallest > e.words) smallest = e.words;
+        atomicAdd(&block_work, (unsigned long long)(int64_t(e.m) * smallest));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && block_work) atomicAdd(work, block_work);
 }
 
 // After a round: a result within the band the pair's window swept (band_reach), or from a window as tall
@@ -586,7 +611,7 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
     uint32_t *keys_sorted = gpu->keys_sorted.ensure<uint32_t>(size_t(pairs));
     uint32_t *order_sorted = gpu->order_sorted.ensure<uint32_t>(size_t(pairs));
     if (gpu->band_tuning.chain_words == 0) gpu->band_tuning = default_band_tuning();
-    const BandTuning tuning = gpu->band_tuning;
+    const BandTuning tuned = gpu->band_tuning;
     alignas(8) unsigned char host_bytes[kCountsBytes];
     const BandCounters *host = reinterpret_cast<const BandCounters *>(host_bytes);
     read_back(gpu, host_bytes, counters, sizeof(unsigned int));
@@ -606,6 +631,19 @@ void band_doubling(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const
         // A round of few pairs takes the one-word-a-lane windows: lanes to spare, and the sweep's time is
         // its longest pair's chain of steps.
         const bool latency = count <= int64_t(gpu->multiprocessors) * 32;
+        // The round's chain bound from its work over the GPU's lanes (1,024 an SM).
+        BandTuning tuning = tuned;
+        if (tuned.chain_share > 0.f && !latency) {
+            DINARA_CUDA(cudaMemsetAsync(&counters->round_work, 0, sizeof(unsigned long long), stream));
+            round_work_kernel<<<blocks, threads, 0, stream>>>(info, pending, &counters->pending, thresholds,
+                                                              &counters->round_work);
+            gpu->launches += 1;
+            DINARA_CUDA(cudaGetLastError());
+            unsigned long long work = 0;
+            read_back(gpu, &work, &counters->round_work, sizeof work);
+            const double per_lane = double(work) / (double(gpu->multiprocessors) * 1024.0);
+            tuning.chain_words = std::max<int64_t>(tuned.chain_words, int64_t(tuned.chain_share * per_lane));
+        }
         band_keys_kernel<<<blocks, threads, 0, stream>>>(info, pending, &counters->pending, thresholds, latency,
                                                          tuning, keys, counters);
         gpu->launches += 1;

@@ -56,9 +56,11 @@ __host__ __device__ inline int64_t band_reach(int64_t n, int64_t m, int64_t wind
 
 // The shape for a pair's band of threshold t. Among shapes holding the band, within a quarter of the
 // smallest that does: the cheapest a column (its words times its word cost) whose chain of word steps,
-// m x K, stays within the tuning's chain_words; failing that, the shortest chain. For a round of few pairs
-// (`latency`: the GPU has lanes to spare and the round lasts as long as its longest chain), the fewest
-// words a lane within twice the smallest window. A band past the widest shape takes the widest.
+// m x K, stays within the tuning's chain_words; failing that, the same within the tuning's reach (up to
+// twice the smallest: a long pair takes a wider window of fewer words a lane rather than hold its lanes
+// for a long chain); failing that, the shortest chain. For a round of few pairs (`latency`: the GPU has lanes to spare and the round
+// lasts as long as its longest chain), the fewest words a lane within twice the smallest window. A band
+// past the widest shape takes the widest. The tuning's figures are BandTuning's (internal.cuh).
 __host__ __device__ inline int band_shape_for(int64_t n, int64_t m, int64_t t, bool latency,
                                               const BandTuning &tuning) {
     const int64_t needed = band_words_needed(n, m, t);
@@ -68,54 +70,65 @@ __host__ __device__ inline int band_shape_for(int64_t n, int64_t m, int64_t t, b
         if (c >= needed && c < smallest) smallest = c;
     }
     if (smallest == INT64_MAX) return kWidestShape;
-    int best = -1;
-    float best_cost = 0.f;
-    int64_t best_chain = INT64_MAX, best_capacity = INT64_MAX;
-    bool best_fits = false;
-    for (int s = 0; s < kBandShapes; ++s) {
-        const int64_t c = band_capacity(s);
-        if (c < needed) continue;
-        const int64_t k = band_words_per_lane(s);
-        if (latency) {
-            if (c > 2 * smallest) continue;
-            if (best < 0 || k < best_chain || (k == best_chain && c < best_capacity)) {
+    if (latency) {
+        int best = -1;
+        int64_t best_k = INT64_MAX, best_capacity = INT64_MAX;
+        for (int s = 0; s < kBandShapes; ++s) {
+            const int64_t c = band_capacity(s), k = band_words_per_lane(s);
+            if (c < needed || c > 2 * smallest) continue;
+            if (best < 0 || k < best_k || (k == best_k && c < best_capacity)) {
                 best = s;
-                best_chain = k;
+                best_k = k;
                 best_capacity = c;
             }
-            continue;
         }
-        if (4 * c > 5 * smallest) continue;
-        const int64_t chain = m * k;
+        return best;
+    }
+    // The cheapest shape whose chain fits, among those within a quarter of the smallest, then within the
+    // tuning's reach.
+    for (int reach = 5; reach <= tuning.reach; reach = reach < tuning.reach ? tuning.reach : reach + 1) {
+        int best = -1;
+        float best_cost = 0.f;
+        for (int s = 0; s < kBandShapes; ++s) {
+            const int64_t c = band_capacity(s);
+            if (c < needed || 4 * c > reach * smallest) continue;
+            if (m * band_words_per_lane(s) > tuning.chain_words) continue;
+            const float cost = float(c) * tuning.word_cost[s];
+            if (best < 0 || cost < best_cost) {
+                best = s;
+                best_cost = cost;
+            }
+        }
+        if (best >= 0) return best;
+    }
+    // No chain fits: the shortest, then the cheapest, within the reach.
+    int best = -1;
+    int64_t best_chain = INT64_MAX;
+    float best_cost = 0.f;
+    for (int s = 0; s < kBandShapes; ++s) {
+        const int64_t c = band_capacity(s);
+        if (c < needed || 4 * c > (tuning.reach > 5 ? tuning.reach : 5) * smallest) continue;
+        const int64_t chain = m * band_words_per_lane(s);
         const float cost = float(c) * tuning.word_cost[s];
-        const bool fits = chain <= tuning.chain_words;
-        bool better;
-        if (best < 0)
-            better = true;
-        else if (fits != best_fits)
-            better = fits;
-        else if (fits)
-            better = cost < best_cost || (cost == best_cost && chain < best_chain);
-        else
-            better = chain < best_chain || (chain == best_chain && cost < best_cost);
-        if (better) {
+        if (best < 0 || chain < best_chain || (chain == best_chain && cost < best_cost)) {
             best = s;
-            best_cost = cost;
             best_chain = chain;
-            best_capacity = c;
-            best_fits = fits;
+            best_cost = cost;
         }
     }
     return best;
 }
 
 // The tuning a context starts with: a word step costs its 40 operations plus a lane's work a column besides
-// its words (about 18 operations) shared by its K words, and chains of up to 40,000 word steps.
+// its words (about 18 operations) shared by its K words, and chains of up to 40,000 word steps whatever the
+// round.
 inline BandTuning default_band_tuning() {
     BandTuning t{};
     t.chain_words = 40000;
     for (int s = 0; s < BandTuning::kShapes; ++s)
         t.word_cost[s] = s < kBandShapes ? 40.f + 18.f / float(band_words_per_lane(s)) : 1e30f;
+    t.chain_share = 0.f;
+    t.reach = 5;
     t.tuned = 0;
     t.full_grids = 0;
     return t;
@@ -139,10 +152,9 @@ double band_shape_rate(dinara_gpu *gpu, int shape, int64_t pairs, const uint8_t 
 int band_shape_blocks(dinara_gpu *gpu, int shape);
 
 // The band autotuner (tune.cu): each shape's sweep rate and the chain bound, measured on the device and
-// set on the context; and the tuning read back or installed (`set`): the chain bound, the grids' scheme and
-// DINARA_BAND_SHAPES word costs.
+// set on the context; and the tuning read back or installed (`set`).
 void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, dinara_band_tune_report &report);
-void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, int64_t *full_grids, float *word_costs);
+void band_tuning_access(dinara_gpu *gpu, bool set, dinara_band_tuning *values);
 
 // Runs band doubling over a batch whose ASCII letters and offsets are on the device already; writes
 // every pair's distance (or its code) to `results` (device) and fills `report`. `letters` starts on a

@@ -133,6 +133,13 @@ namespace dinara {
 struct BandTuning {
     static constexpr int kShapes = 40;
     int64_t chain_words;
+    // A round's chain bound grows with its work: at least chain_words, and chain_share times the round's
+    // word steps (in its smallest windows) over the GPU's lanes, so a pair's chain stays within a share of
+    // the round it runs in.
+    float chain_share;
+    // How much wider than the smallest window a shape may be taken so that a long pair's chain fits, in
+    // quarters of the smallest (5: a quarter wider; 8: twice as wide).
+    int32_t reach;
     float word_cost[kShapes];
     int32_t tuned;  // 1 once the autotuner has set them on this context
     // How a round's launches (one a shape, all at once on side streams) share the GPU: 0 each takes the

@@ -821,7 +821,10 @@ void predictor_train(dinara_gpu *gpu, const dinara_train_options &options, dinar
         squared += e * e;
     }
     if (gpu->band_tuning.chain_words == 0) gpu->band_tuning = default_band_tuning();
-    const BandTuning tuning = gpu->band_tuning;
+    // The first round a batch runs is its largest: where a round's chain bound grows with its work, take it
+    // as unbounded.
+    BandTuning tuning = gpu->band_tuning;
+    if (tuning.chain_share > 0.f) tuning.chain_words = INT64_MAX / 4;
     const double slack = options.slack;
     // Whether a pair settles in its first round at margin `margin` (predict_kernel's threshold).
     auto settles = [&](const HeldPair &h, double margin) {

@@ -14,9 +14,19 @@
 namespace dinara {
 namespace {
 
-constexpr int64_t kChainCandidates[] = {12000, 24000, 48000, 96000};
-constexpr int kChainCount = int(sizeof(kChainCandidates) / sizeof(kChainCandidates[0]));
-static_assert(2 * kChainCount <= 8, "the report holds every candidate");
+// Chain bounds tried: a floor in word steps, a share of the round's work per lane above it (0: none) and
+// the reach in quarters of the smallest window.
+constexpr int64_t kFloorCandidates[] = {24000, 48000, 96000, 12000, 24000, 48000, 24000, 48000};
+constexpr double kShareCandidates[] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0};
+constexpr int32_t kReachCandidates[] = {5, 5, 5, 8, 8, 8, 8, 8};
+constexpr int kChainCount = int(sizeof(kShareCandidates) / sizeof(kShareCandidates[0]));
+static_assert(kChainCount <= 8, "the report holds every candidate");
+
+// First thresholds a tenth above each pair's distance: the rounds a learned start gives, for tuning.
+__global__ void near_starts_kernel(const int64_t *__restrict__ distances, int64_t pairs, int64_t *__restrict__ starts) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < pairs) starts[k] = distances[k] >= 0 ? distances[k] + distances[k] / 10 + 8 : 1;
+}
 
 // Each shape's words a millisecond, timed on pairs at least `length` letters long and at least eight words
 // taller than the shape's window (so every lane sweeps words inside the pattern), at least two full waves
@@ -88,59 +98,85 @@ void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, din
         }
         out.shapes = kBandShapes;
     }
-    // 2. The chain bound and the launches' grids: plain band doubling over pairs of the distribution, twice
-    // a candidate.
+    // 2. The chain bound: band doubling over pairs of the distribution under each candidate, from the plain
+    // start and from starts a tenth above each pair's distance (the one large round a learned start
+    // gives), their device times summed, the fastest of two runs each.
     const GeneratedPairs generated =
         generate_pairs(gpu, o.seed + 1, o.pairs, o.length_low, o.length_high, o.rate_low, o.rate_high);
-    int64_t *results = gpu->features.ensure<int64_t>(size_t(o.pairs));
+    int64_t *results = gpu->features.ensure<int64_t>(2 * size_t(o.pairs));
+    int64_t *starts = results + o.pairs;
+    gpu->band_tuning = tuning;
+    band_doubling(gpu, o.pairs, generated.letters, generated.offsets, nullptr, 0, results, nullptr);
+    near_starts_kernel<<<unsigned((o.pairs + 255) / 256), 256, 0, gpu->stream>>>(results, o.pairs, starts);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
     double best_ms = 0.0;
-    int64_t best_chain = tuning.chain_words;
-    int32_t best_grids = tuning.full_grids;
-    for (int c = 0; c < 2 * kChainCount; ++c) {
-        tuning.chain_words = kChainCandidates[c % kChainCount];
-        tuning.full_grids = c / kChainCount;
+    int best = 0;
+    for (int c = 0; c < kChainCount; ++c) {
+        tuning.chain_words = kFloorCandidates[c];
+        tuning.chain_share = float(kShareCandidates[c]);
+        tuning.reach = kReachCandidates[c];
+        tuning.full_grids = 0;
         gpu->band_tuning = tuning;
-        double fastest_run = 0.0;
-        for (int repeat = 0; repeat < 2; ++repeat) {
-            dinara_band_report band;
-            std::memset(&band, 0, sizeof band);
-            band_doubling(gpu, o.pairs, generated.letters, generated.offsets, nullptr, 0, results, &band);
-            if (repeat == 0 || band.kernel_ms < fastest_run) fastest_run = band.kernel_ms;
+        double total = 0.0;
+        for (int start = 0; start < 2; ++start) {
+            double fastest_run = 0.0;
+            for (int repeat = 0; repeat < 2; ++repeat) {
+                dinara_band_report band;
+                std::memset(&band, 0, sizeof band);
+                band_doubling(gpu, o.pairs, generated.letters, generated.offsets, start ? starts : nullptr, 0, results,
+                              &band);
+                if (repeat == 0 || band.kernel_ms < fastest_run) fastest_run = band.kernel_ms;
+            }
+            total += fastest_run;
         }
-        out.chain_words_tried[c] = tuning.full_grids ? -tuning.chain_words : tuning.chain_words;
-        out.chain_ms[c] = fastest_run;
-        if (c == 0 || fastest_run < best_ms) {
-            best_ms = fastest_run;
-            best_chain = tuning.chain_words;
-            best_grids = tuning.full_grids;
+        out.chain_words_tried[c] = kFloorCandidates[c];
+        out.chain_share_tried[c] = kShareCandidates[c];
+        out.reach_tried[c] = kReachCandidates[c];
+        out.chain_ms[c] = total;
+        if (c == 0 || total < best_ms) {
+            best_ms = total;
+            best = c;
         }
     }
-    out.chain_tried = 2 * kChainCount;
-    out.full_grids = best_grids;
-    tuning.chain_words = best_chain;
-    tuning.full_grids = best_grids;
+    out.chain_tried = kChainCount;
+    tuning.chain_words = kFloorCandidates[best];
+    tuning.chain_share = float(kShareCandidates[best]);
+    tuning.reach = kReachCandidates[best];
+    tuning.full_grids = 0;
     tuning.tuned = 1;
     gpu->band_tuning = tuning;
-    out.chain_words = best_chain;
+    out.chain_words = tuning.chain_words;
+    out.chain_share = tuning.chain_share;
+    out.reach = tuning.reach;
+    out.full_grids = 0;
     out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - began).count();
 }
 
-void band_tuning_access(dinara_gpu *gpu, bool set, int64_t *chain_words, int64_t *full_grids, float *word_costs) {
+void band_tuning_access(dinara_gpu *gpu, bool set, dinara_band_tuning *values) {
     if (gpu->band_tuning.chain_words == 0) gpu->band_tuning = default_band_tuning();
     if (set) {
-        if (*chain_words < 1) throw Failure(DINARA_INVALID_LENGTH, "a chain bound below one word step");
+        if (values->chain_words < 1) throw Failure(DINARA_INVALID_LENGTH, "a chain bound below one word step");
+        if (!(values->chain_share >= 0.0) || !std::isfinite(values->chain_share))
+            throw Failure(DINARA_INVALID_LENGTH, "a chain share that is not a number at or above zero");
         for (int s = 0; s < kBandShapes; ++s)
-            if (!(word_costs[s] > 0.f) || !std::isfinite(word_costs[s]))
+            if (!(values->word_costs[s] > 0.f) || !std::isfinite(values->word_costs[s]))
                 throw Failure(DINARA_INVALID_LENGTH, "a word cost that is not a positive number");
-        gpu->band_tuning.chain_words = *chain_words;
-        gpu->band_tuning.full_grids = *full_grids ? 1 : 0;
-        for (int s = 0; s < kBandShapes; ++s) gpu->band_tuning.word_cost[s] = word_costs[s];
+        gpu->band_tuning.chain_words = values->chain_words;
+        gpu->band_tuning.chain_share = float(values->chain_share);
+        if (values->reach < 5 || values->reach > 8) throw Failure(DINARA_INVALID_LENGTH, "a reach outside 5-8 quarters");
+        gpu->band_tuning.reach = int32_t(values->reach);
+        gpu->band_tuning.full_grids = values->full_grids ? 1 : 0;
+        for (int s = 0; s < kBandShapes; ++s) gpu->band_tuning.word_cost[s] = values->word_costs[s];
         gpu->band_tuning.tuned = 1;
         return;
     }
-    *chain_words = gpu->band_tuning.chain_words;
-    *full_grids = gpu->band_tuning.full_grids;
-    for (int s = 0; s < kBandShapes; ++s) word_costs[s] = gpu->band_tuning.word_cost[s];
+    std::memset(values, 0, sizeof *values);
+    values->chain_words = gpu->band_tuning.chain_words;
+    values->chain_share = gpu->band_tuning.chain_share;
+    values->reach = gpu->band_tuning.reach;
+    values->full_grids = gpu->band_tuning.full_grids;
+    for (int s = 0; s < kBandShapes; ++s) values->word_costs[s] = gpu->band_tuning.word_cost[s];
 }
 
 }  // namespace dinara

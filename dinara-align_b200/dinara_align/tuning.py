@@ -24,8 +24,14 @@ class TuneOptions(ctypes.Structure):
 class TuneReport(ctypes.Structure):
     _fields_ = [("shapes", ctypes.c_int64), ("words_per_ms", ctypes.c_double * 40),
                 ("chain_tried", ctypes.c_int64), ("chain_words_tried", ctypes.c_int64 * 8),
-                ("chain_ms", ctypes.c_double * 8), ("chain_words", ctypes.c_int64), ("full_grids", ctypes.c_int64),
-                ("seconds", ctypes.c_double)]
+                ("chain_share_tried", ctypes.c_double * 8), ("reach_tried", ctypes.c_int64 * 8),
+                ("chain_ms", ctypes.c_double * 8), ("chain_words", ctypes.c_int64), ("chain_share", ctypes.c_double),
+                ("reach", ctypes.c_int64), ("full_grids", ctypes.c_int64), ("seconds", ctypes.c_double)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("chain_words", ctypes.c_int64), ("chain_share", ctypes.c_double), ("reach", ctypes.c_int64),
+                ("full_grids", ctypes.c_int64), ("word_costs", ctypes.c_float * 40)]
 
 
 def _declare(lib):
@@ -34,8 +40,7 @@ def _declare(lib):
     lib.dinara_gpu_band_autotune.restype = ctypes.c_int64
     lib.dinara_gpu_band_autotune.argtypes = [ctypes.c_void_p, ctypes.POINTER(TuneOptions), ctypes.POINTER(TuneReport)]
     lib.dinara_gpu_band_tuning.restype = ctypes.c_int64
-    lib.dinara_gpu_band_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
-                                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_float)]
+    lib.dinara_gpu_band_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(Tuning)]
     lib._tuning_declared = True
     return lib
 
@@ -57,34 +62,40 @@ def autotune(placement: Placement | None = None, *, pairs: int = 50_000, length=
     report = TuneReport()
     native.check(lib.dinara_gpu_band_autotune(handle, ctypes.byref(options), ctypes.byref(report)), handle)
     rates = {f"{g}x{k}": report.words_per_ms[s] for s in range(report.shapes) for g, k in [shape_of(s)]}
-    # Keyed by chain bound; a negative key is the same bound with launches that each fill the GPU.
-    chains = {int(report.chain_words_tried[c]): report.chain_ms[c] for c in range(report.chain_tried)}
+    # Keyed "floor/share/reach": the device time of plain doubling and of near starts together.
+    chains = {f"{report.chain_words_tried[c]}/{report.chain_share_tried[c]:g}/{report.reach_tried[c]}":
+              report.chain_ms[c] for c in range(report.chain_tried)}
     return {"words_per_ms": rates, "chain_ms": chains, "chain_words": int(report.chain_words),
-            "full_grids": int(report.full_grids), "seconds": report.seconds}
+            "chain_share": report.chain_share, "reach": int(report.reach), "full_grids": int(report.full_grids),
+            "seconds": report.seconds}
 
 
 def tuning(placement: Placement | None = None) -> dict:
-    """The context's current tuning: its chain bound and each shape's relative word cost."""
+    """The context's current tuning: its chain bound's floor and share, grid scheme and word costs."""
     lib = _declare(native.lib())
     handle = native.context(_placement(placement))
-    chain, grids = ctypes.c_int64(), ctypes.c_int64()
-    costs = np.zeros(SHAPES, dtype=np.float32)
-    native.check(lib.dinara_gpu_band_tuning(handle, 0, ctypes.byref(chain), ctypes.byref(grids),
-                                            costs.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), handle)
-    return {"chain_words": int(chain.value), "full_grids": int(grids.value), "word_costs": [float(c) for c in costs]}
+    values = Tuning()
+    native.check(lib.dinara_gpu_band_tuning(handle, 0, ctypes.byref(values)), handle)
+    return {"chain_words": int(values.chain_words), "chain_share": float(values.chain_share),
+            "reach": int(values.reach), "full_grids": int(values.full_grids),
+            "word_costs": [float(c) for c in values.word_costs[:SHAPES]]}
 
 
 def install(values: dict, placement: Placement | None = None) -> None:
     """Installs a tuning that `tuning()` returned (on this or another run)."""
     lib = _declare(native.lib())
     handle = native.context(_placement(placement))
-    chain = ctypes.c_int64(int(values["chain_words"]))
-    grids = ctypes.c_int64(int(values.get("full_grids", 0)))
     costs = np.ascontiguousarray(values["word_costs"], dtype=np.float32)
     if costs.shape != (SHAPES,):
         raise ValueError(f"{costs.size} word costs for {SHAPES} shapes")
-    native.check(lib.dinara_gpu_band_tuning(handle, 1, ctypes.byref(chain), ctypes.byref(grids),
-                                            costs.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), handle)
+    given = Tuning()
+    given.chain_words = int(values["chain_words"])
+    given.chain_share = float(values.get("chain_share", 0.0))
+    given.reach = int(values.get("reach", 5))
+    given.full_grids = int(values.get("full_grids", 0))
+    for s, cost in enumerate(costs):
+        given.word_costs[s] = float(cost)
+    native.check(lib.dinara_gpu_band_tuning(handle, 1, ctypes.byref(given)), handle)
 
 
 def save(path: str, placement: Placement | None = None) -> None:

@@ -218,10 +218,10 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
 /*
  * The band autotuner (no reference counterpart; the reference's band doubling runs on the host with one
  * code path). A unit-cost round sweeps each pair's band with a window of G lanes x K 64-bit words, one of
- * DINARA_BAND_SHAPES shapes; which shape a band takes is set by two figures the autotuner measures on the
- * context's own device: each shape's sweep rate (words a millisecond, as a relative word cost) and the
- * bound on a pair's chain of word steps (text letters x K) that gives the fastest band doubling over pairs
- * drawn from the given distribution. Shapes only decide how a band is swept, so distances never depend
+ * DINARA_BAND_SHAPES shapes; which shape a band takes is set by figures the autotuner measures on the
+ * context's own device: each shape's sweep rate (words a millisecond, as a relative word cost), and the
+ * share of a round's work per lane that bounds a pair's chain of word steps (text letters x K), with the
+ * launches' grid scheme, that give the fastest band doubling over pairs drawn from the given distribution. Shapes only decide how a band is swept, so distances never depend
  * on the tuning. A context starts from fixed defaults until this runs.
  */
 #define DINARA_BAND_SHAPES 39
@@ -240,10 +240,14 @@ typedef struct {
 typedef struct {
     int64_t shapes;                  /* shapes timed (0 when measure_shapes was zero) */
     double words_per_ms[40];         /* each shape's sweep rate, shape 6 log2(G) + K - 1 for K <= 6 */
-    int64_t chain_tried;             /* candidates tried (the first 8 reported) */
-    int64_t chain_words_tried[8];    /* each one's chain bound, negative where its launches fill the GPU */
-    double chain_ms[8];              /* the band rounds' device time under each */
-    int64_t chain_words;             /* the bound chosen */
+    int64_t chain_tried;             /* candidate chain bounds tried */
+    int64_t chain_words_tried[8];    /* each one's floor */
+    double chain_share_tried[8];     /* and share */
+    int64_t reach_tried[8];          /* and reach */
+    double chain_ms[8];              /* the band rounds' device time under each, plain and near starts */
+    int64_t chain_words;             /* the bound's floor */
+    double chain_share;              /* the share chosen */
+    int64_t reach;                   /* the reach chosen */
     int64_t full_grids;              /* 1 when the chosen launches each fill the GPU, 0 when they share it */
     double seconds;                  /* wall time of the whole tuning */
 } dinara_band_tune_report;
@@ -251,11 +255,18 @@ typedef struct {
 /* Measures and installs the context's band tuning; `options` may be null for the defaults. */
 int64_t dinara_gpu_band_autotune(dinara_gpu *gpu, const dinara_band_tune_options *options,
                                  dinara_band_tune_report *report);
-/* Reads the context's tuning (`set` 0) or installs one (`set` 1, as a previous run reported it):
- * the chain bound, whether a round's launches each fill the GPU (1) or share it (0), and
- * DINARA_BAND_SHAPES word costs. */
-int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, int64_t *chain_words, int64_t *full_grids,
-                               float *word_costs);
+/* A context's band tuning. A round's bound on a pair's chain of word steps is the larger of chain_words
+ * and chain_share times the round's word steps (in its smallest windows) over the GPU's lanes. */
+typedef struct {
+    int64_t chain_words;   /* the bound's floor */
+    double chain_share;    /* 0: the floor alone */
+    int64_t reach;         /* how much wider than the smallest window a long pair may take, in quarters (5-8) */
+    int64_t full_grids;    /* 1: a round's launches each fill the GPU; 0: they share it by their time */
+    float word_costs[40];  /* each shape's relative time a word step (DINARA_BAND_SHAPES of them) */
+} dinara_band_tuning;
+
+/* Reads the context's tuning (`set` 0) or installs one (`set` 1, as a previous run reported it). */
+int64_t dinara_gpu_band_tuning(dinara_gpu *gpu, int64_t set, dinara_band_tuning *tuning);
 
 /*
  * The learned band predictor (no reference counterpart): a 258 -> 64 -> 64 -> 1 fp32 network over a

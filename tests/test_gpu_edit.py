@@ -134,14 +134,14 @@ def test_autotuned_shapes_change_no_distance(da, oracle):
     report = tuning.autotune(pairs=3000, length=(100, 6000), probe_length=2048)
     assert len(report["words_per_ms"]) == tuning.SHAPES
     assert all(rate > 0 for rate in report["words_per_ms"].values())
-    assert report["chain_words"] * (-1 if report["full_grids"] else 1) in report["chain_ms"]
+    assert f"{report['chain_words']}/{report['chain_share']:g}/{report['reach']}" in report["chain_ms"]
     tape = workloads.uneven_unit_cost(600, high=8000, seed=31)
     expected = _oracle_distances(oracle, tape)
     np.testing.assert_array_equal(da.distances_tape(tape), expected)
     kept = tuning.tuning()
     assert kept["chain_words"] == report["chain_words"]
     # Inverted costs: the chooser now prefers what the device measured slowest, and chains of one step.
-    inverted = {"chain_words": 1, "full_grids": 1 - kept["full_grids"],
+    inverted = {"chain_words": 1, "chain_share": 0.0, "reach": 8, "full_grids": 1 - kept["full_grids"],
                 "word_costs": [1.0 / cost for cost in kept["word_costs"]]}
     tuning.install(inverted)
     np.testing.assert_array_equal(da.distances_tape(tape), expected)

@@ -72,8 +72,7 @@ def test_band_tuning_needs_a_context():
     """The autotuner's entry points refuse a missing context with a code."""
     handle = ctypes.CDLL(LIBRARY)
     handle.dinara_gpu_band_tuning.restype = ctypes.c_int64
-    chain, grids = ctypes.c_int64(0), ctypes.c_int64(0)
-    costs = (ctypes.c_float * 39)()
-    assert handle.dinara_gpu_band_tuning(None, 0, ctypes.byref(chain), ctypes.byref(grids), costs) == -6
+    values = (ctypes.c_byte * 256)()
+    assert handle.dinara_gpu_band_tuning(None, 0, values) == -6
     handle.dinara_gpu_band_autotune.restype = ctypes.c_int64
     assert handle.dinara_gpu_band_autotune(None, None, None) == -6
