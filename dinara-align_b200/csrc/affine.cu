@@ -710,6 +710,51 @@ void launch_bands(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &
 
 }  // namespace
 
+namespace {
+
+// Global scores with free ends: every pair over its whole matrix in 32 bits, one shape (32 lanes of 16
+// columns, strips of 512) with the table in shared memory, the free-end form of the sweep.
+void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
+                     int64_t first, int64_t count) {
+    const Schedule order = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, false, PairLimits());
+    int32_t *table32 = nullptr;
+    upload_table32(gpu, table, false, &table32);
+    const TableArgs targs = table_args(table, false);
+    KernelArgs args;
+    std::memset(&args, 0, sizeof args);
+    args.tape = batch.tape;
+    args.shapes = batch.shapes;
+    args.order = order.order;
+    args.open = table.open;
+    args.extend = table.extend;
+    args.scores = scores;
+    args.free_reference_start = batch.free_reference_start;
+    args.free_reference_end = batch.free_reference_end;
+    args.free_query_start = batch.free_query_start;
+    args.free_query_end = batch.free_query_end;
+    KernelFn fn = batch.bits == 8 ? static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 8, true, true>)
+                                  : static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 2, true, true>);
+    int64_t total = 0;
+    for (int cls = 0; cls < kClasses; ++cls) total += order.counts[cls];
+    int64_t blocks = persistent_blocks(gpu, fn);
+    blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, (total + kBlock / 32 - 1) / (kBlock / 32)));
+    if (batch.max_columns > 512u) {
+        args.carry_stride = int64_t(batch.max_rows) + 1;
+        args.carry = gpu->carry.ensure<int2>(size_t(blocks * (kBlock / 32) * args.carry_stride));
+    }
+    args.begin = 0;
+    args.end = uint32_t(total);
+    PhaseTimer timer(gpu, &gpu->kernel_ms);
+    ClockSpan clock(gpu, kClassWhole, gpu->stream);
+    fn<<<dim3(unsigned(blocks)), kBlock, 0, gpu->stream>>>(args, targs, table32);
+    DINARA_CUDA(cudaGetLastError());
+    clock.stop();
+    gpu->launches += 1;
+    timer.stop();
+}
+
+}  // namespace
+
 bool band_serves(const AffineBatch &batch, const AffineTable &table) {
     if (batch.local || batch.bits != 2 || !table.packed16) return false;
     int32_t best = -128;
@@ -721,6 +766,10 @@ bool band_serves(const AffineBatch &batch, const AffineTable &table) {
 void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
                    int64_t first, int64_t count) {
     if (count <= 0) return;
+    if (batch.free_ends) {
+        free_end_scores(gpu, batch, table, scores, first, count);
+        return;
+    }
     const bool band = band_serves(batch, table);
     PairLimits limits = whole_limits_of(batch, table);
     limits.band = band ? pair_limit_of(table) : 0;

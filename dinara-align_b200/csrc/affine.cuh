@@ -47,6 +47,11 @@ struct AffineBatch {
     // Per-pair flags (the packing's unknown-letter flags): a walk that finds its path leaving the proven
     // band sets its pair's to kWalkFailed, which the host reports as DINARA_DEVICE_FAILURE. May be null.
     uint8_t *flags = nullptr;
+    // Global scores with free ends (scored.mojo:69-240): letters at the reference's start and end and the
+    // query's start and end that may go unaligned for nothing (at most INT32_MAX; a pair reads at most
+    // its own length). `free_ends` is set when any is nonzero.
+    bool free_ends = false;
+    int32_t free_reference_start = 0, free_reference_end = 0, free_query_start = 0, free_query_end = 0;
 };
 
 // The flag value a failed walk leaves (1 is a letter outside the alphabet).

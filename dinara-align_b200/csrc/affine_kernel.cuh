@@ -50,6 +50,9 @@ struct KernelArgs {
     const int64_t *decision_offsets;
     int64_t *ends;  // local: (row << 32) | column of the best cell
     int64_t first_pair;
+    // Free ends (affine_kernel<..., FREE>): letters at the reference's start and end and the query's start
+    // and end that may go unaligned for nothing, each at most its sequence's length once a pair reads it.
+    int32_t free_reference_start, free_reference_end, free_query_start, free_query_end;
     // The widening band (affine_wide_kernel<false, true>): the pair at order[item] is swept over
     // band_widths[item] diagonals from band_low_for_width; the pairs whose band proves nothing are redone
     // wider or whole.
@@ -72,10 +75,20 @@ struct TableArgs {
     int32_t size;
 };
 
+// A border cell's true score with free letters (scored.mojo edge): `letters` in from the origin along a side
+// whose first `free` letters go unaligned for nothing, a gap from where they end past them.
+__device__ __forceinline__ int32_t free_edge(int letters, int free, int32_t open, int32_t extend) {
+    return letters <= free ? 0 : open + (letters - free - 1) * extend;
+}
+
 // One pair per group of G lanes; see the file's notes. Persistent: each warp takes its next GPW pairs of
-// the bucket until the bucket ends.
-template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE>
+// the bucket until the bucket ends. With FREE (global scores, no recording) the letters p.free_* name at
+// each end go unaligned for nothing (scored.mojo:69-240 FROM_EDGE): the first row's and first column's
+// cells hold free_edge, and the score is the best end on the last row within free_query_end letters of
+// the last column or on the last column within free_reference_end letters of the last row.
+template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE, bool FREE = false>
 __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__ table32) {
+    static_assert(!FREE || (!LOCAL && !RECORD), "free ends are for global scores");
     constexpr int W = G * C;
     constexpr int GPW = 32 / G;
     __shared__ uint2 rows16[4];
@@ -112,6 +125,12 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
         int32_t reported = 0;
         int32_t best = 0;
         int64_t best_place = 0;
+        // Free ends: each side's free letters, and this lane's best end so far (a true score).
+        const int free_rs = FREE ? min(p.free_reference_start, rows) : 0;
+        const int free_re = FREE ? min(p.free_reference_end, rows) : 0;
+        const int free_qs = FREE ? min(p.free_query_start, cols) : 0;
+        const int free_qe = FREE ? min(p.free_query_end, cols) : 0;
+        int32_t free_best = -(1 << 30);
         int64_t dec_base = 0;
         const int rows_pad = ((rows + 2) | 3) + 1;
         if (RECORD && work) dec_base = p.decision_offsets[pair - p.first_pair];
@@ -135,11 +154,14 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
             int32_t H[C], D[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {
-                H[k] = top;
-                D[k] = top + first_gap;
+                // The first row, held shifted: with free ends a column's true border less column x extend.
+                H[k] = FREE ? free_edge(first_col + k + 1, free_qs, open, extend) - (first_col + k + 1) * extend : top;
+                D[k] = H[k] + first_gap;
             }
-            int32_t edgeH = top, edgeI = top + first_gap;
+            int32_t edgeH = FREE ? free_edge(first_col + C, free_qs, open, extend) - (first_col + C) * extend : top;
+            int32_t edgeI = edgeH + first_gap;
             int32_t above_left = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
+            if (FREE) above_left = free_edge(first_col, free_qs, open, extend) - first_col * extend;
             const int steps = strip_live ? rows + G : 0;
             const int warp_steps = warp_max(steps);
             uint64_t buffered[4] = {0, 0, 0, 0};
@@ -157,6 +179,8 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                         if (member == 0) {
                             if (s == 0) {
                                 leftH = LOCAL ? 0 : opening;
+                                // The first column with free ends: the row's true border less row x extend.
+                                if (FREE) leftH = free_edge(row, free_rs, open, extend) - row * extend;
                                 leftI = leftH + first_gap;
                             } else {
                                 const int r = min(max(row, 0), rows);
@@ -238,12 +262,33 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                             if (member == G - 1 && s + 1 < strips) {
                                 p.carry[slot * p.carry_stride + row] = make_int2(H[C - 1], I);
                             }
-                            if (!LOCAL && row == rows && owned > 0 && first_col + owned == cols) {
+                            if (!LOCAL && !FREE && row == rows && owned > 0 && first_col + owned == cols) {
                                 // The corner by masks, not by an index into H (which would put H in memory).
 #pragma unroll
                                 for (int k = 0; k < C; ++k) {
                                     const int32_t hit = -int32_t(k == owned - 1);
                                     reported = (reported & ~hit) | (H[k] & hit);
+                                }
+                            }
+                            if (FREE) {
+                                // Ends on the last row within free_qe letters of the last column, and on the
+                                // last column within free_re letters of the last row, as true scores.
+                                if (row == rows) {
+#pragma unroll
+                                    for (int k = 0; k < C; ++k) {
+                                        const int column = first_col + k + 1;
+                                        if (k < owned && column >= cols - free_qe)
+                                            free_best = max(free_best, H[k] + (rows + column) * extend);
+                                    }
+                                }
+                                if (owned > 0 && first_col + owned == cols && rows - row <= free_re) {
+                                    int32_t last = 0;
+#pragma unroll
+                                    for (int k = 0; k < C; ++k) {
+                                        const int32_t hit = -int32_t(k == owned - 1);
+                                        last = (last & ~hit) | (H[k] & hit);
+                                    }
+                                    free_best = max(free_best, last + (row + cols) * extend);
                                 }
                             }
                             if (RECORD) {
@@ -291,6 +336,23 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                     }
                     p.ends[pair - p.first_pair] = end;
                 }
+            }
+        } else if (FREE) {
+            // The best end of the group's lanes, then the first row's and first column's own ends (a free
+            // end reaching the border), or an empty side's run along the other's edge.
+#pragma unroll
+            for (int span = 1; span < G; span <<= 1) free_best = max(free_best, __shfl_xor_sync(kFull, free_best, span, G));
+            if (live && member == 0) {
+                int32_t found = free_best;
+                if (!work) {
+                    found = rows == 0 && cols == 0 ? 0
+                            : cols == 0       ? free_edge(rows - free_re, free_rs, open, extend)
+                                              : free_edge(cols - free_qe, free_qs, open, extend);
+                } else {
+                    if (cols <= free_qe) found = max(found, free_edge(rows, free_rs, open, extend));
+                    if (rows <= free_re) found = max(found, free_edge(cols, free_qs, open, extend));
+                }
+                p.scores[pair] = found;
             }
         } else if (live) {
             const int total = rows + cols;

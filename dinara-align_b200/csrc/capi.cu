@@ -116,6 +116,26 @@ bool check_mode(const dinara_mode *mode) {
     throw Failure(DINARA_INVALID_MODE, "a Scoring aligns only globally or locally on the GPU");
 }
 
+// check_mode for scores, which also take free ends on the GPU (scored.mojo:69-240 FROM_EDGE, the
+// reference's host path; its GPU refuses them): GLOBAL, ends_free with any counts, or LOCAL. Sets the
+// batch's free letters (clamped to INT32_MAX) and returns whether the mode is local.
+bool check_scores_mode(const dinara_mode *mode, AffineBatch &batch) {
+    batch.free_ends = false;
+    if (mode && mode->kind == DINARA_ENDS_FREE && mode->match_score <= 0 &&
+        (mode->reference_start | mode->reference_end | mode->query_start | mode->query_end) != 0) {
+        if (mode->reference_start < 0 || mode->reference_end < 0 || mode->query_start < 0 || mode->query_end < 0)
+            throw Failure(DINARA_INVALID_MODE, "a free end of fewer than no letters");
+        auto clamp = [](int64_t v) { return int32_t(std::min<int64_t>(v, INT32_MAX)); };
+        batch.free_ends = true;
+        batch.free_reference_start = clamp(mode->reference_start);
+        batch.free_reference_end = clamp(mode->reference_end);
+        batch.free_query_start = clamp(mode->query_start);
+        batch.free_query_end = clamp(mode->query_end);
+        return false;
+    }
+    return check_mode(mode);
+}
+
 bool is_pinned(const void *pointer) {
     cudaPointerAttributes attributes;
     if (cudaPointerGetAttributes(&attributes, pointer) != cudaSuccess) {
@@ -989,7 +1009,8 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
                                int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
         if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
-        const bool local = check_mode(mode);
+        AffineBatch ends;
+        const bool local = check_scores_mode(mode, ends);
         const CheckedScoring checked = check_scoring(scoring, local);
         check_offsets(pairs, offsets);
         if (pairs == 0) return 0;
@@ -998,6 +1019,11 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
         start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
         const Packed &packed = streamed.packed;
         AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
+        batch.free_ends = ends.free_ends;
+        batch.free_reference_start = ends.free_reference_start;
+        batch.free_reference_end = ends.free_reference_end;
+        batch.free_query_start = ends.free_query_start;
+        batch.free_query_end = ends.free_query_end;
         int32_t *scores_device = streamed.scores;
         const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
         UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
@@ -1029,7 +1055,8 @@ int64_t dinara_gpu_scores(dinara_gpu *gpu, int64_t pairs, const char *const *ref
                           const int64_t *reference_lengths, const char *const *queries, const int64_t *query_lengths,
                           const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
-        const bool local = check_mode(mode);
+        AffineBatch ends;
+        const bool local = check_scores_mode(mode, ends);
         (void)check_scoring(scoring, local);
         std::vector<char> letters;
         std::vector<int64_t> offsets;
@@ -1330,12 +1357,18 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
     return guard(gpu, [&]() -> int64_t {
         Resident &r = resident_of(gpu);
         if (!r.scoring) throw Failure(DINARA_INVALID_MODE, "the resident batch was loaded for distances");
-        const bool local = check_mode(mode);
+        AffineBatch ends;
+        const bool local = cigars ? check_mode(mode) : check_scores_mode(mode, ends);
         if (r.pairs == 0) return 0;
         DINARA_CUDA(cudaSetDevice(gpu->device));
         Timer timer(gpu);
         AffineBatch batch{r.pairs, r.checked.bits, local, r.packed.tape, r.packed.shapes, r.packed.max_rows,
                           r.packed.max_columns, r.packed.unknown};
+        batch.free_ends = ends.free_ends;
+        batch.free_reference_start = ends.free_reference_start;
+        batch.free_reference_end = ends.free_reference_end;
+        batch.free_query_start = ends.free_query_start;
+        batch.free_query_end = ends.free_query_end;
         int32_t *scores_device = r.results.ensure<int32_t>(size_t(r.pairs));
         const int64_t *offsets = r.offsets.data();
         if (!cigars) {

@@ -151,6 +151,69 @@ int32_t oracle_gotoh_score(const uint8_t *first, int64_t rows, const uint8_t *se
     return result;
 }
 
+/* Free ends, scored.mojo:69-240 (swept_cells, FROM_EDGE) with the letters gap_affine.mojo:421-447 EndsFree
+ * allows: the first row's cell `c` query letters in scores edge(c, query_start) and the first column's
+ * `r` reference letters in edge(r, reference_start), where edge is nothing within the free letters and a
+ * gap from where they end past them; the score is the best end on the last row within `query_end` letters
+ * of the last column, or on the last column within `reference_end` letters of the last row. Against an
+ * empty side the alignment runs along the other's edge and ends within its free letters. Counts past a
+ * sequence's length read as its length. */
+static inline int32_t free_edge(int64_t letters, int64_t free_letters, int32_t open, int32_t extend) {
+    return letters <= free_letters ? 0 : gap_run(open, extend, letters - free_letters);
+}
+
+int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                                const int8_t *table, int32_t size, int32_t open, int32_t extend,
+                                int64_t reference_start, int64_t reference_end, int64_t query_start,
+                                int64_t query_end) {
+    const int64_t rs = reference_start < rows ? reference_start : rows;
+    const int64_t re = reference_end < rows ? reference_end : rows;
+    const int64_t qs = query_start < columns ? query_start : columns;
+    const int64_t qe = query_end < columns ? query_end : columns;
+    if (rows == 0 && columns == 0) return 0;
+    if (columns == 0) return free_edge(rows - re, rs, open, extend);
+    if (rows == 0) return free_edge(columns - qe, qs, open, extend);
+    const int32_t opening = open + extend;
+    const int64_t stride = columns + 1;
+    int32_t *s = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *d = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *i = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    for (int64_t c = 0; c <= columns; ++c) {
+        const int32_t border = free_edge(c, qs, open, extend);
+        s[c] = border;
+        d[c] = border + opening;
+        i[c] = 0;
+    }
+    /* The last column's ends: row 0 among them when every reference letter may be left at the end. */
+    int32_t best = INT32_MIN;
+    if (rows <= re) best = s[columns];
+    for (int64_t r = 1; r <= rows; ++r) {
+        int32_t *ps = s + ((r - 1) & 1) * stride, *pd = d + ((r - 1) & 1) * stride;
+        int32_t *cs = s + (r & 1) * stride, *cd = d + (r & 1) * stride, *ci = i + (r & 1) * stride;
+        const int32_t border = free_edge(r, rs, open, extend);
+        cs[0] = border;
+        cd[0] = border;
+        ci[0] = border + opening;
+        const int8_t *table_row = table + (int64_t)first[r - 1] * size;
+        for (int64_t c = 1; c <= columns; ++c) {
+            int32_t del = max32(ps[c] + open, pd[c] + extend);
+            int32_t ins = max32(cs[c - 1] + open, ci[c - 1] + extend);
+            cs[c] = max32(ps[c - 1] + table_row[second[c - 1]], max32(del, ins));
+            cd[c] = del;
+            ci[c] = ins;
+        }
+        if (rows - r <= re && cs[columns] > best) best = cs[columns];
+    }
+    /* The last row's ends, column 0 among them when every query letter may be left at the end. */
+    const int32_t *last = s + (rows & 1) * stride;
+    for (int64_t c = columns - qe; c <= columns; ++c)
+        if (last[c] > best) best = last[c];
+    free(s);
+    free(d);
+    free(i);
+    return best;
+}
+
 /* Decision, gotoh.mojo:130-170: low two bits the source (0 aligning, 1 deleting, 2 inserting, 3 a
  * local path's start), bit 2 the deletion extends a run, bit 3 the insertion does. */
 enum { ALIGNING = 0, DELETING = 1, INSERTING = 2, ENDS = 3 };

@@ -27,6 +27,12 @@ extern "C" {
 /* Best score of one pair over the whole matrix (gotoh.mojo:285-362 fill_rows; scoring.mojo:450-465
  * swept_score for empty sides). For LOCAL, the end cell (first maximum in row-major order, the
  * `beats` rule of gotoh.mojo:122-127) is written to *end_row / *end_column (0, 0 when the best is 0). */
+/* The best score with up to the given letters at each end of each sequence unaligned for nothing
+ * (scored.mojo:69-240 with gap_affine.mojo:421-447 EndsFree). */
+int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                                const int8_t *table, int32_t size, int32_t open, int32_t extend,
+                                int64_t reference_start, int64_t reference_end, int64_t query_start,
+                                int64_t query_end);
 int32_t oracle_gotoh_score(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                            const int8_t *table, int32_t size, int32_t open, int32_t extend, int32_t mode,
                            int64_t *end_row, int64_t *end_column);

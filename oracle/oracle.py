@@ -46,6 +46,8 @@ def lib() -> ctypes.CDLL:
         i32p = ctypes.POINTER(ctypes.c_int32)
         handle.oracle_gotoh_score.restype = i32
         handle.oracle_gotoh_score.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, i64p, i64p]
+        handle.oracle_gotoh_score_free.restype = i32
+        handle.oracle_gotoh_score_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64]
         handle.oracle_gotoh_align.restype = i32
         handle.oracle_gotoh_align.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, u8p, u8p, i64p]
         handle.oracle_cigar.restype = i64
@@ -113,6 +115,19 @@ def gotoh_score(first, second, table, size, open_, extend, mode=GLOBAL) -> tuple
     score = lib().oracle_gotoh_score(pa, len(a), pb, len(b), pt, size, open_, extend, mode, ctypes.byref(row),
                                      ctypes.byref(column))
     return score, row.value, column.value
+
+
+def gotoh_score_free(a, b, table, size, open_, extend, reference_start=0, reference_end=0, query_start=0,
+                     query_end=0) -> int:
+    """The best score of a (codes, reference down the rows) against b with the given free letters at each
+    end of each (scored.mojo:69-240)."""
+    first, pa = _u8(a)
+    second, pb = _u8(b)
+    t, pt = _i8(table)
+    big = (1 << 62)
+    return int(lib().oracle_gotoh_score_free(pa, len(first), pb, len(second), pt, size, open_, extend,
+                                             min(reference_start, big), min(reference_end, big),
+                                             min(query_start, big), min(query_end, big)))
 
 
 def gotoh_align(first, second, table, size, open_, extend, mode=GLOBAL, eqx=True) -> tuple:

@@ -205,7 +205,9 @@ def test_refusals(da):
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACGT"], da.Scoring("AC-T", tuple([1] * 16)))
     with pytest.raises(ValueError):
-        da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.INFIX)
+        da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.extension(2))  # extensions stay on the host
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.INFIX.with_match_score(2))
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACGT"], scoring, da.Mode.local(2))
     huge = da.Scoring.uniform(2, -4, -4, -100000)

@@ -1,0 +1,83 @@
+"""Global scores with free ends on the GPU against the oracle (the reference's host path for a Scoring's
+free ends, scored.mojo:69-240; its GPU refuses them): the reference's literal, every preset its tests name
+(tests/test_alignment.mojo:2938-2943) on reads cut from and mutated off their references, empty sides,
+pairs wider than one strip, and the refusals that stand."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BIG = 1 << 40
+
+
+def _expected(oracle, scoring, refs, queries, mode):
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    size = len(scoring.alphabet)
+    out = []
+    for r, q in zip(refs, queries):
+        out.append(oracle.gotoh_score_free(oracle.codes(r, scoring.alphabet), oracle.codes(q, scoring.alphabet), table,
+                                           size, op, ex, min(mode.reference_start, BIG), min(mode.reference_end, BIG),
+                                           min(mode.query_start, BIG), min(mode.query_end, BIG)))
+    return out
+
+
+def _reads(rng, count, longest):
+    """References of 0-`longest` letters; queries cut from them and mutated, a sixth unrelated."""
+    refs, queries = [], []
+    for trial in range(count):
+        n = int(rng.integers(0, longest + 1))
+        ref = "".join(rng.choice(list("ACGT"), size=n))
+        if trial % 6 == 0:
+            query = "".join(rng.choice(list("ACGT"), size=int(rng.integers(0, max(2, longest * 3 // 4)))))
+        else:
+            start = int(rng.integers(0, n // 4 + 1))
+            stop = n - int(rng.integers(0, n // 4 + 1))
+            piece = list(ref[start:max(start, stop)])
+            rate = (0.0, 0.02, 0.1)[trial % 3]
+            query = "".join(ch if rng.random() >= rate else rng.choice(list("ACGT")) for ch in piece
+                            if rng.random() >= rate / 3)
+        refs.append(ref)
+        queries.append(query)
+    return refs, queries
+
+
+def test_reference_literal(da):
+    """tests/test_python.py:103-104: the read placed inside its window by Mode.INFIX scores 16."""
+    assert da.score("TTTTACGTACGTTTTT", "ACGTACGT", da.Scoring.dna(), da.Mode.INFIX) == 16
+    assert da.scores(["TTTTACGTACGTTTTT"], ["ACGTACGT"], da.Scoring.dna(), da.Mode.PREFIX) == \
+        [da.score("TTTTACGTACGTTTTT", "ACGTACGT", da.Scoring.dna(), da.Mode.PREFIX)]
+
+
+@pytest.mark.parametrize("mode_name", ["INFIX", "PREFIX", "SUFFIX", "query_both", "few", "overlap"])
+def test_presets_against_the_oracle(da, oracle, mode_name):
+    modes = {"INFIX": da.Mode.INFIX, "PREFIX": da.Mode.PREFIX, "SUFFIX": da.Mode.SUFFIX,
+             "query_both": da.Mode.ends_free(query_start=BIG, query_end=BIG),
+             "few": da.Mode.ends_free(reference_start=8, reference_end=8, query_start=3, query_end=3),
+             "overlap": da.Mode.ends_free(reference_end=40, query_start=40)}
+    mode = modes[mode_name]
+    rng = np.random.default_rng(sum(map(ord, mode_name)))
+    refs, queries = _reads(rng, 240, 260)
+    tabulated = da.Scoring.tabulated("ACGT", [5, -1, -2, -1, -1, 5, -3, -2, -2, -3, 5, -1, -1, -2, -1, 5], -6, -1)
+    for scoring in (da.Scoring.dna(), tabulated):
+        assert da.scores(refs, queries, scoring, mode) == _expected(oracle, scoring, refs, queries, mode)
+
+
+def test_long_pairs_and_random_counts(da, oracle):
+    """Pairs past one 512-column strip and tall ones, each batch with random free counts."""
+    rng = np.random.default_rng(91)
+    scoring = da.Scoring.dna()
+    for batch in range(4):
+        refs, queries = _reads(rng, 60, 2200)
+        counts = [int(x) for x in rng.integers(0, 300, size=4)]
+        mode = da.Mode.ends_free(*counts)
+        assert da.scores(refs, queries, scoring, mode) == _expected(oracle, scoring, refs, queries, mode)
+
+
+def test_free_ends_refused_where_the_gpu_does_not_serve_them(da):
+    """Alignments (CIGARs) with free ends stay refused on the GPU, as are negative counts."""
+    with pytest.raises(ValueError):
+        da.alignments_tape(da.Tape.of(["ACGT"], ["ACG"]), da.Scoring.dna(), da.Mode.INFIX)
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.ends_free(reference_start=-1))

@@ -364,3 +364,55 @@ def test_batch_wavefront_matches_single_pairs(oracle):
     for k, (a, b) in enumerate(zip(refs, queries)):
         assert (costs[k], cigars[k]) == oracle.affine_cigar(a, b, 4, 6, 2, right=True)
         assert costs[k] == least_cost(a, b, 4, 6, 2, 6, 2)
+
+
+def test_free_ends_known_answer(oracle):
+    """The reference's literal (tests/test_python.py:103-104): the query placed inside the reference by
+    Mode.INFIX under Scoring.dna() scores 16."""
+    table = oracle.dna_table(2, -4)
+    op, ex = oracle.kernel_gaps(-4, -2)
+    unbounded = 1 << 40
+    got = oracle.gotoh_score_free(oracle.codes("TTTTACGTACGTTTTT"), oracle.codes("ACGTACGT"), table, 4, op, ex,
+                                  reference_start=unbounded, reference_end=unbounded)
+    assert got == 16
+    # No free letters is the global score.
+    assert oracle.gotoh_score_free(oracle.codes("TTTTACGTACGTTTTT"), oracle.codes("ACGTACGT"), table, 4, op, ex) == \
+        oracle.gotoh_score(oracle.codes("TTTTACGTACGTTTTT"), oracle.codes("ACGTACGT"), table, 4, op, ex)[0]
+
+
+def _trimmed_best(oracle, a, b, table, op, ex, rs, re, qs, qe):
+    """Free ends by brute force: the best global score over every trim the free letters allow, a start
+    trimming one sequence's start (the alignment begins on the first row or the first column) and an end
+    one sequence's end."""
+    n, m = len(a), len(b)
+    best = None
+    starts = [(r0, 0) for r0 in range(min(rs, n) + 1)] + [(0, c0) for c0 in range(1, min(qs, m) + 1)]
+    ends = [(r1, 0) for r1 in range(min(re, n) + 1)] + [(0, c1) for c1 in range(1, min(qe, m) + 1)]
+    for r0, c0 in starts:
+        for r1, c1 in ends:
+            if r0 + r1 > n or c0 + c1 > m:
+                continue
+            score = oracle.gotoh_score(a[r0:n - r1], b[c0:m - c1], table, 4, op, ex)[0]
+            best = score if best is None else max(best, score)
+    return best
+
+
+def test_free_ends_against_trimmed_global_alignments(oracle):
+    """Every preset the reference names (INFIX, PREFIX, SUFFIX, the query's both ends, a few letters at
+    each end, an overlap's; tests/test_alignment.mojo:2938-2943) and random counts, on short pairs and
+    empty sides, under two tables: the oracle's free-end score is the best global score over the trims
+    the free letters allow."""
+    rng = np.random.default_rng(71)
+    big = 1 << 40
+    presets = [(big, big, 0, 0), (0, big, 0, 0), (big, 0, 0, 0), (0, 0, big, big), (8, 8, 3, 3), (0, 40, 40, 0)]
+    for match, mismatch, opening, extension in ((2, -4, -4, -2), (1, -3, -5, -1)):
+        table = oracle.dna_table(match, mismatch)
+        op, ex = oracle.kernel_gaps(opening, extension)
+        for trial in range(60):
+            n, m = int(rng.integers(0, 14)), int(rng.integers(0, 12))
+            a = rng.integers(0, 4, size=n).astype(np.uint8)
+            b = a[: m].copy() if trial % 3 else rng.integers(0, 4, size=m).astype(np.uint8)
+            b = b[rng.random(len(b)) > 0.1]
+            counts = presets[trial % len(presets)] if trial < 36 else tuple(int(x) for x in rng.integers(0, 6, size=4))
+            got = oracle.gotoh_score_free(a, b, table, 4, op, ex, *counts)
+            assert got == _trimmed_best(oracle, a, b, table, op, ex, *counts), (a, b, counts)
