@@ -86,7 +86,10 @@ int64_t dinara_gpu_device_info(dinara_gpu *gpu, char *name, int64_t name_capacit
 
 /*
  * Scores under a Scoring, global or local (replaces the reference's device batch
- * dinara_align/api.mojo:843-892 `scores` -> scoring.mojo:1294-1409 `device_batch_scores`).
+ * dinara_align/api.mojo:843-892 `scores` -> scoring.mojo:1294-1409 `device_batch_scores`), or global
+ * with free ends: a DINARA_ENDS_FREE mode with letter counts at the reference's and the query's starts
+ * and ends (INFIX, PREFIX, SUFFIX, ends_free; no match score of the mode's own), scored as the
+ * reference's host path scores them (scored.mojo:69-240), which its GPU refuses.
  * Pair i is references[i] (reference_lengths[i] bytes) against queries[i]. Writes scores[i] and
  * statuses[i] (0, or the pair's own code: -1 a letter outside the alphabet, -3 scores that could pass
  * 2^28 as ScoreReach refuses, scoring.mojo:218-249). Returns 0, or a code failing the whole batch
@@ -103,7 +106,8 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
                                int64_t *statuses);
 
 /*
- * Alignments under a Scoring, global or local, the CIGAR Gotoh's walk picks among equals (replaces
+ * Alignments under a Scoring, global or local (free ends refused, DINARA_INVALID_MODE), the CIGAR
+ * Gotoh's walk picks among equals (replaces
  * api.mojo:895-1006 `alignments` on the GPU -> scoring.mojo:1436-1478 `device_batch_alignments` ->
  * device_align.mojo:278-441 `batch_kernel[record]`, and the reference's c/dinara.h:225-228 batch
  * shape). Each alignment's CIGAR is allocated here and freed with dinara_free; its spans are placed
