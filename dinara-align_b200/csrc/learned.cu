@@ -542,6 +542,9 @@ struct Margins {
 
 __device__ __host__ inline int length_class(double mean) { return mean < 300 ? 0 : mean < 1000 ? 1 : mean < 4096 ? 2 : 3; }
 
+// Pairs a warp takes at once: each weight it reads from shared memory serves all of them.
+constexpr int kPredictPairs = 4;
+
 __global__ void __launch_bounds__(256) predict_kernel(const float *features, const int64_t *offsets, int64_t pairs,
                                                       const float *params, Margins margins, float slack,
                                                       int64_t *thresholds, float *predicted) {
@@ -552,53 +555,82 @@ __global__ void __launch_bounds__(256) predict_kernel(const float *features, con
     float *b2 = w2 + kH * kH;
     float *w3 = b2 + kH;
     float *b3 = w3 + kH;
-    float *inputs = shared + kParamsRoom;  // 8 warps x 260 (kIn and padding)
+    // Each warp's inputs, kPredictPairs rows of 260 (kIn and padding), then its first layer's outputs.
+    float *inputs = shared + kParamsRoom;
     for (int i = threadIdx.x; i < kPredictorParameters; i += blockDim.x) shared[i] = params[i];
     const int warp_in_block = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *x = inputs + warp_in_block * 260;
+    float *x = inputs + warp_in_block * kPredictPairs * (260 + kH);
+    float *hidden = x + kPredictPairs * 260;
     __syncthreads();
-    for (int64_t pair = int64_t(blockIdx.x) * 8 + warp_in_block; pair < pairs; pair += int64_t(gridDim.x) * 8) {
-        const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
-        for (int i = lane; i < kIn; i += 32) x[i] = __ldg(features + pair * kIn + i);
+    const int64_t stride = int64_t(gridDim.x) * 8 * kPredictPairs;
+    for (int64_t first = (int64_t(blockIdx.x) * 8 + warp_in_block) * kPredictPairs; first < pairs; first += stride) {
+        const int count = int(pairs - first < kPredictPairs ? pairs - first : kPredictPairs);
+        for (int q = 0; q < kPredictPairs; ++q)
+            for (int i = lane; i < kIn; i += 32) x[q * 260 + i] = q < count ? __ldg(features + (first + q) * kIn + i) : 0.f;
         __syncwarp();
-        // Hidden layers: lane j computes units j and j + 32.
-        float h[2];
-        for (int u = 0; u < 2; ++u) {
-            const int j = lane + 32 * u;
-            float v = b1[j];
-            for (int i = 0; i < kIn; ++i) v = fmaf(x[i], w1[i * kH + j], v);
-            h[u] = fmaxf(v, 0.f);
+        // Hidden layers: lane j computes units j and j + 32 of every pair.
+        float h[kPredictPairs][2];
+#pragma unroll
+        for (int q = 0; q < kPredictPairs; ++q) {
+            h[q][0] = b1[lane];
+            h[q][1] = b1[lane + 32];
         }
-        float g[2];
-        for (int u = 0; u < 2; ++u) {
-            const int j = lane + 32 * u;
-            float v = b2[j];
-            for (int i = 0; i < kH; ++i) {
-                const float hi = __shfl_sync(0xffffffffu, h[i / 32], i % 32);
-                v = fmaf(hi, w2[i * kH + j], v);
+        for (int i = 0; i < kIn; ++i) {
+            const float wa = w1[i * kH + lane], wb = w1[i * kH + lane + 32];
+#pragma unroll
+            for (int q = 0; q < kPredictPairs; ++q) {
+                const float xi = x[q * 260 + i];
+                h[q][0] = fmaf(xi, wa, h[q][0]);
+                h[q][1] = fmaf(xi, wb, h[q][1]);
             }
-            g[u] = fmaxf(v, 0.f);
         }
-        float y = g[0] * w3[lane] + g[1] * w3[lane + 32];
-        for (int span = 16; span > 0; span >>= 1) y += __shfl_xor_sync(0xffffffffu, y, span);
-        y += b3[0];
-        if (lane == 0) {
-            const int64_t n = q0 - r0, m = q1 - q0;
-            const double mean = 0.5 * double(n + m);
-            const double guess = fmax(0.0, double(y)) * mean;
-            const int64_t delta = n > m ? n - m : m - n;
-            const double margin = double(margins.by_length[length_class(mean)]);
-            int64_t t = int64_t(ceil(guess * margin + double(slack)));
-            if (t < delta) t = delta;
-            if (t < 1) t = 1;
-            thresholds[pair] = t;
-            if (predicted) predicted[pair] = float(guess);
+#pragma unroll
+        for (int q = 0; q < kPredictPairs; ++q) {
+            hidden[q * kH + lane] = fmaxf(h[q][0], 0.f);
+            hidden[q * kH + lane + 32] = fmaxf(h[q][1], 0.f);
+        }
+        __syncwarp();
+        float g[kPredictPairs][2];
+#pragma unroll
+        for (int q = 0; q < kPredictPairs; ++q) {
+            g[q][0] = b2[lane];
+            g[q][1] = b2[lane + 32];
+        }
+        for (int i = 0; i < kH; ++i) {
+            const float wa = w2[i * kH + lane], wb = w2[i * kH + lane + 32];
+#pragma unroll
+            for (int q = 0; q < kPredictPairs; ++q) {
+                const float hi = hidden[q * kH + i];
+                g[q][0] = fmaf(hi, wa, g[q][0]);
+                g[q][1] = fmaf(hi, wb, g[q][1]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kPredictPairs; ++q) {
+            float y = fmaxf(g[q][0], 0.f) * w3[lane] + fmaxf(g[q][1], 0.f) * w3[lane + 32];
+#pragma unroll
+            for (int span = 16; span > 0; span >>= 1) y += __shfl_xor_sync(0xffffffffu, y, span);
+            y += b3[0];
+            if (lane == 0 && q < count) {
+                const int64_t pair = first + q;
+                const int64_t r0 = offsets[2 * pair], q0 = offsets[2 * pair + 1], q1 = offsets[2 * pair + 2];
+                const int64_t n = q0 - r0, m = q1 - q0;
+                const double mean = 0.5 * double(n + m);
+                const double guess = fmax(0.0, double(y)) * mean;
+                const int64_t delta = n > m ? n - m : m - n;
+                const double margin = double(margins.by_length[length_class(mean)]);
+                int64_t t = int64_t(ceil(guess * margin + double(slack)));
+                if (t < delta) t = delta;
+                if (t < 1) t = 1;
+                thresholds[pair] = t;
+                if (predicted) predicted[pair] = float(guess);
+            }
         }
         __syncwarp();
     }
 }
 
-size_t predict_shared_bytes() { return size_t(kParamsRoom + 8 * 260) * sizeof(float); }
+size_t predict_shared_bytes() { return size_t(kParamsRoom + 8 * kPredictPairs * (260 + kH)) * sizeof(float); }
 
 // Parameter offsets in the flat vector: w1 [kIn][kH], b1, w2 [kH][kH], b2, w3, b3.
 constexpr int kW1 = 0, kB1 = kW1 + kIn * kH, kW2 = kB1 + kH, kB2 = kW2 + kH * kH, kW3 = kB2 + kH, kB3 = kW3 + kH;
@@ -661,7 +693,7 @@ const int64_t *predict_thresholds(dinara_gpu *gpu, int64_t pairs, const uint8_t 
     int per_sm = 0;
     DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, predict_kernel, 256, shared));
     int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
-    blocks = std::min<int64_t>(blocks, (pairs + 7) / 8);
+    blocks = std::min<int64_t>(blocks, (pairs + 8 * kPredictPairs - 1) / (8 * kPredictPairs));
     Margins margins;
     for (int k = 0; k < 4; ++k) margins.by_length[k] = float(gpu->predictor_margins[k]);
     // The sketches first, a warp a pair at full occupancy (reading the letters is the slow part), then the
