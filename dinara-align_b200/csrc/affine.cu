@@ -102,9 +102,10 @@ __global__ void walk_kernel(WalkArgs a) {
         const uint64_t *decisions = layout == 2 ? a.decisions_extra : a.decisions;
         const int G = record_lanes(uint32_t(cols), a.uniform);
         const int W = G * 16;
-        const bool banded = layout == 1 || layout == 3;
+        const bool banded = layout == 1 || layout == 3 || layout == 4;
+        const int width = layout == 4 ? kBandWidth / 2 : kBandWidth;  // layout 4: the narrow band's 32
         const int rows_pad = banded ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
-        const int low = banded ? band_low_for(rows, cols) : 0;
+        const int low = banded ? band_low_for_width(rows, cols, width) : 0;
         const int64_t base = a.decision_offsets[k];
         int state = 0;  // 0 aligning, 1 deleting, 2 inserting
         while (row > 0 && column > 0) {
@@ -116,7 +117,7 @@ __global__ void walk_kernel(WalkArgs a) {
                 // The proof keeps every optimal path inside the band; a place outside it would read
                 // another pair's decisions, so the walk stops there instead and flags the pair, whose
                 // CIGAR the host then reports as a device failure rather than a result.
-                if (place < 0 || place >= kBandWidth) {
+                if (place < 0 || place >= width) {
                     if (a.failed) a.failed[pair] = kWalkFailed;
                     break;
                 }
@@ -132,7 +133,7 @@ __global__ void walk_kernel(WalkArgs a) {
             }
             const uint64_t word = decisions[at];
             uint32_t nibble;
-            if (layout == 3) {
+            if (layout == 3 || layout == 4) {
                 // The 16-bit pair band's planes: bit `slot_in` of deleting, inserting, deletion extending and
                 // insertion extending, 16 bits each; inserting wins over deleting as decide() orders them.
                 const uint32_t del = uint32_t(word >> slot_in) & 1u, ins = uint32_t(word >> (16 + slot_in)) & 1u;
@@ -477,7 +478,7 @@ void widening_band(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
     uint32_t *lists = gpu->wide_pending.ensure<uint32_t>(5 * size_t(count));
     uint32_t *whole = lists + 2 * count;
     int32_t *widths = reinterpret_cast<int32_t *>(lists + 3 * count);
-    unsigned int *counts = gpu->class_counts.ensure<unsigned int>(16) + 9;  // [0] next, [1] whole
+    unsigned int *counts = gpu->class_counts.ensure<unsigned int>(20) + 9;  // [0] next, [1] whole
     DINARA_CUDA(cudaMemsetAsync(counts + 1, 0, sizeof(unsigned int), gpu->stream));
     constexpr int32_t kFirstWidth = 2048;
     constexpr int kBandRounds = 2;
@@ -668,17 +669,29 @@ BandedBatch banded_batch(const AffineBatch &batch, const AffineTable &table, con
     return band;
 }
 
-// Adds the cells a batch's sweeps updated to the context's tally (only while it times).
+// The band cells a call's band launches count while the context times (null otherwise): zeroed here, read
+// by tally_swept.
+unsigned long long *band_counter(dinara_gpu *gpu) {
+    if (!gpu->timing) return nullptr;
+    unsigned long long *counter = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(20) + 16);
+    DINARA_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), gpu->stream));
+    return counter;
+}
+
+// Adds the cells a batch's sweeps updated to the context's tally (only while it times): the whole matrices
+// from their shapes, the bands' cells as their launches counted them (a narrow pass and a wide one where
+// both ran).
 void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool band,
                  const uint32_t *leftovers, int64_t left) {
     if (!gpu->timing) return;
-    unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(16) + 12);
+    unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(20) + 12);
     DINARA_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), gpu->stream));
     swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, out);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     unsigned long long host[2] = {0, 0};
     read_back(gpu, host, out, sizeof host);
+    if (band) read_back(gpu, &host[0], gpu->class_counts.ensure<unsigned int>(20) + 16, sizeof host[0]);
     gpu->swept_cells += int64_t(host[0] + host[1]);
     gpu->band_cells += int64_t(host[0]);
     gpu->whole_cells += int64_t(host[1]);
@@ -696,7 +709,8 @@ int64_t band_pairs(const Schedule &schedule) {
 // Sweeps the band's pairs, the 16-bit pair sweep's first, every unproven pair onto one leftover list.
 void launch_bands(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const Schedule &schedule,
                   int32_t *scores, uint32_t *leftovers, unsigned int *leftover_count, bool record, uint64_t *decisions,
-                  const int64_t *decision_offsets, int64_t first_pair) {
+                  const int64_t *decision_offsets, int64_t first_pair, uint8_t *layouts,
+                  unsigned long long *band_cells) {
     for (int pass = 0; pass < 2; ++pass) {
         const bool pairs_of_16 = pass == 0;
         BandedBatch b = banded_batch(batch, table, schedule, scores, nullptr, leftovers, leftover_count, pairs_of_16);
@@ -704,7 +718,29 @@ void launch_bands(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &
         b.decisions = decisions;
         b.decision_offsets = decision_offsets;
         b.first_pair = first_pair;
-        banded_launch(gpu, b, record, pairs_of_16);
+        b.band_cells = band_cells;
+        if (!pairs_of_16) {
+            banded_launch(gpu, b, record, false);
+            continue;
+        }
+        // The 16-bit pair band in two passes: every pair over 32 diagonals first (most short pairs' scores
+        // prove there, for half the cells), then the pairs it did not prove, or could not hold, over 64.
+        uint32_t *narrow_left = gpu->narrow_leftovers.ensure<uint32_t>(size_t(b.count));
+        unsigned int *narrow_count = gpu->class_counts.ensure<unsigned int>(20) + 11;
+        DINARA_CUDA(cudaMemsetAsync(narrow_count, 0, sizeof(unsigned int), gpu->stream));
+        BandedBatch narrow = b;
+        narrow.leftovers = narrow_left;
+        narrow.leftover_count = narrow_count;
+        narrow.layouts = record ? layouts : nullptr;
+        banded_launch(gpu, narrow, record, true, 2);
+        unsigned int again = 0;
+        read_back(gpu, &again, narrow_count, sizeof again);
+        if (again > 0) {
+            BandedBatch wide = b;
+            wide.order = narrow_left;
+            wide.count = again;
+            banded_launch(gpu, wide, record, true, kBandLanes);
+        }
     }
 }
 
@@ -782,13 +818,14 @@ void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
     args.open = table.open;
     args.extend = table.extend;
     args.scores = scores;
-    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(16);
+    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(20);
     unsigned int *leftover_count = counters + 8;
     uint32_t *leftovers = nullptr;
     if (band_pairs(schedule_all) > 0) {
         leftovers = gpu->leftovers.ensure<uint32_t>(size_t(band_pairs(schedule_all)));
         DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
-        launch_bands(gpu, batch, table, schedule_all, scores, leftovers, leftover_count, false, nullptr, nullptr, 0);
+        launch_bands(gpu, batch, table, schedule_all, scores, leftovers, leftover_count, false, nullptr, nullptr, 0,
+                     nullptr, band_counter(gpu));
     }
     affine_launch_all(gpu, batch, table, schedule_all, false, args);
     unsigned int left = 0;
@@ -856,7 +893,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     args.decision_offsets = word_offsets;
     args.ends = ends;
     args.first_pair = first_pair;
-    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(16);
+    unsigned int *counters = gpu->class_counts.ensure<unsigned int>(20);
     unsigned int *leftover_count = counters + 8;
     uint32_t *leftovers = nullptr;
     uint64_t *extra = nullptr;
@@ -864,7 +901,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
         leftovers = gpu->leftovers.ensure<uint32_t>(size_t(band_pairs(schedule_all)));
         DINARA_CUDA(cudaMemsetAsync(leftover_count, 0, sizeof(unsigned int), gpu->stream));
         launch_bands(gpu, batch, table, schedule_all, scores, leftovers, leftover_count, true, decisions, word_offsets,
-                     first_pair);
+                     first_pair, layouts, band_counter(gpu));
     }
     affine_launch_all(gpu, batch, table, schedule_all, true, args);
     unsigned int left = 0;

@@ -266,9 +266,13 @@ __device__ __forceinline__ uint32_t difference_mad(uint32_t b, uint32_t a, uint3
     return out;
 }
 
-template <bool RECORD>
+// LANES lanes of 16 places a lane group: a band of 32 diagonals (2 lanes, the narrow first pass) or 64
+// (4 lanes). In the narrow pass a pair whose band cannot hold both its ends goes straight to the leftover
+// list, which the wide pass takes; a pair the narrow band proves is marked as its layout 4.
+template <bool RECORD, int LANES>
 __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) {
-    constexpr int G = kBandLanes, C = kBandColumns;
+    constexpr int G = LANES, C = kBandColumns;
+    constexpr int kWidth = G * C;
     constexpr int GPW = 32 / G;      // lane groups a warp
     constexpr int PPW = 2 * GPW;     // pairs a warp
     // Rows a selector window serves: few enough that the unrolled body stays in the instruction cache
@@ -306,7 +310,15 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
             }
             rows[h] = int(sh[h].rows);
             cols[h] = int(sh[h].columns);
-            low[h] = live[h] ? band_low_for(rows[h], cols[h]) : 0;
+            low[h] = live[h] ? band_low_for_width(rows[h], cols[h], kWidth) : 0;
+            if (live[h] && low[h] == INT32_MIN) {
+                // Too narrow a band for this pair: the wide pass takes it (one lane records it once).
+                if (member == 0) b.leftovers[atomicAdd(b.leftover_count, 1u)] = pair[h];
+                live[h] = false;
+                sh[h] = PairShape{0, 0, 0, 0};
+                rows[h] = cols[h] = 0;
+                low[h] = 0;
+            }
             end_place[h] = cols[h] - rows[h] - low[h];
             rows_pad[h] = (rows[h] + 3) & ~3;
             if (RECORD && live[h])
@@ -394,10 +406,10 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
                         }
                         D[k] = dn;
                     }
-                    // Exclusive prefix maximum of the four lanes' running maxima.
+                    // Exclusive prefix maximum of the lanes' running maxima (two or four lanes).
                     uint32_t reach = __shfl_up_sync(kFull, S, 1, G);
                     if (member == 0) reach = unreached2;
-                    {
+                    if (G > 2) {
                         const uint32_t further = __shfl_up_sync(kFull, reach, 1, G);
                         if (member >= 1) reach = max2(reach, further);
                         const uint32_t further2 = __shfl_up_sync(kFull, reach, 2, G);
@@ -466,10 +478,13 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
             const bool holder = live[h] && end_place[h] >= first_place && end_place[h] < first_place + C;
             if (holder) {
                 const int64_t score = int64_t(reported[h]) + int64_t(rows[h] + cols[h]) * b.extend;
-                const bool proven = band_proves(score, rows[h], cols[h], low[h], b.best, b.open, b.extend);
+                const bool proven = band_proves_width(score, rows[h], cols[h], low[h], kWidth, b.best, b.open, b.extend);
                 b.scores[pair[h]] = int32_t(score);
                 if (b.proven) b.proven[pair[h]] = proven ? 1 : 0;
                 if (!proven) b.leftovers[atomicAdd(b.leftover_count, 1u)] = pair[h];
+                // The narrow band's proven pairs walk its two lanes' decisions (layout 4).
+                if (RECORD && proven && kWidth < kBandWidth && b.layouts) b.layouts[pair[h] - b.first_pair] = 4;
+                if (b.band_cells) atomicAdd(b.band_cells, (unsigned long long)rows[h] * kWidth);
             }
         }
     }
@@ -477,13 +492,16 @@ __global__ void __launch_bounds__(kBlock, 2) banded_pairs_kernel(BandedBatch b) 
 
 }  // namespace
 
-void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16) {
+void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16, int lanes) {
     if (batch.count <= 0) return;
-    auto fn = pairs_of_16 ? (record ? &banded_pairs_kernel<true> : &banded_pairs_kernel<false>)
+    const bool narrow = pairs_of_16 && lanes == 2;
+    auto fn = pairs_of_16 ? (narrow ? (record ? &banded_pairs_kernel<true, 2> : &banded_pairs_kernel<false, 2>)
+                                    : (record ? &banded_pairs_kernel<true, kBandLanes>
+                                              : &banded_pairs_kernel<false, kBandLanes>))
                           : (record ? &banded_kernel<true> : &banded_kernel<false>);
     int per_sm = 0;
     DINARA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
-    const int64_t pairs_per_block = (pairs_of_16 ? 2 : 1) * kBlock / kBandLanes;
+    const int64_t pairs_per_block = (pairs_of_16 ? 2 : 1) * kBlock / (narrow ? 2 : kBandLanes);
     int64_t blocks = int64_t(std::max(per_sm, 1)) * gpu->multiprocessors;
     const int64_t needed = (batch.count + pairs_per_block - 1) / pairs_per_block;
     if (blocks > needed) blocks = needed;

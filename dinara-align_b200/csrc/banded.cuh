@@ -100,10 +100,16 @@ struct BandedBatch {
     uint64_t *decisions;
     const int64_t *decision_offsets;
     int64_t first_pair;
+    // Recording, when given: each pair's layout (by pair - first_pair), set to 4 where the narrow band
+    // proved the pair. Counting, when given: the band cells the launch swept (rows x band width a pair).
+    uint8_t *layouts;
+    unsigned long long *band_cells;
 };
 
 // Launches the banded sweep (scores, or with `record` scores and decisions) over `batch.count` pairs; with
-// `pairs_of_16` the 16-bit pair sweep, two pairs a lane group (every pair within band_pair_limit).
-void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16 = false);
+// `pairs_of_16` the 16-bit pair sweep, two pairs a lane group (every pair within band_pair_limit), over a
+// band of `lanes` x 16 diagonals (2: the narrow first pass; 4: the full band).
+void banded_launch(dinara_gpu *gpu, const BandedBatch &batch, bool record, bool pairs_of_16 = false,
+                   int lanes = kBandLanes);
 
 }  // namespace dinara
