@@ -574,9 +574,10 @@ def run_scoring(ctx, workload, tape, steps, warmup) -> dict:
             kernels.append({"kernel": "walk_kernel", "bound": "latency", "ms_per_step": ms,
                             "pairs_per_s": tape.pairs / (ms / 1e3) if ms else None,
                             "work": "one dependent 4-bit decision read a CIGAR step, a thread a pair"})
-        line["roofline"] = dict(kernels[0], traffic=8217.0 * tape.pairs if affine else None,
-                                traffic_unit="bytes a launch of the recording band sweep (ncu capture of 200,000 "
-                                             "pairs, 8,217 bytes a pair, scaled)" if affine else None,
+        line["roofline"] = dict(kernels[0], traffic=6190.0 * tape.pairs if affine else None,
+                                traffic_unit="bytes a step of the recording band sweep, its two launches (ncu "
+                                             "capture of 200,000 pairs, 6,190 bytes a pair, scaled)"
+                                if affine else None,
                                 peak_source="measured in this run: DPX viaddmax chains on every SM, 2 ops each")
     line["kernels"] = kernels
     if affine:
