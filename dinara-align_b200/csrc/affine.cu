@@ -40,7 +40,10 @@ struct WalkArgs {
     const PairShape *shapes;
     const uint64_t *decisions;
     const uint64_t *decisions_extra;  // the band's leftovers, swept whole afterwards
-    const uint8_t *layouts;           // per pair: 0 whole matrix, 1 band, 2 whole matrix in decisions_extra
+    // Per pair: 0 whole matrix, 1 band, 2 whole matrix in decisions_extra, 3 and 4 the 16-bit pair band's
+    // planes over 64 and 32 diagonals, 5 a band-recorded pair's strips over its proven width (widths[k]).
+    const uint8_t *layouts;
+    const int32_t *widths;
     const int64_t *decision_offsets;
     const int64_t *ends;
     const int64_t *slot_offsets;  // per pair: its CIGAR slot, 2 (rows + columns) + 1 bytes
@@ -107,11 +110,45 @@ __global__ void walk_kernel(WalkArgs a) {
         const int rows_pad = banded ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
         const int low = banded ? band_low_for_width(rows, cols, width) : 0;
         const int64_t base = a.decision_offsets[k];
+        // Layout 5: the strip under the walk, its swept rows and its first word (past the earlier strips').
+        int strip = 0, strip_first = 1, strip_last = 0, strip_pad = 0, band_low = 0, band_high = 0;
+        int64_t strip_at = 0;
+        if (layout == 5) {
+            const int proven = a.widths[k];
+            band_low = band_low_for_width(rows, cols, proven);
+            band_high = band_low + proven - 1;
+            strip = (cols - 1) / kRecordStrip;
+            for (int s = 0; s < strip; ++s)
+                strip_at += 32 * int64_t(band_strip_pad(band_strip_first_row(s, band_high),
+                                                        band_strip_last_row(s, rows, cols, band_low)));
+            strip_first = band_strip_first_row(strip, band_high);
+            strip_last = band_strip_last_row(strip, rows, cols, band_low);
+            strip_pad = band_strip_pad(strip_first, strip_last);
+        }
         int state = 0;  // 0 aligning, 1 deleting, 2 inserting
         while (row > 0 && column > 0) {
             int64_t at;
             int slot_in;
-            if (banded) {
+            if (layout == 5) {
+                // Strips are left behind right to left: step back over each one the column has passed.
+                while (strip > (column - 1) / kRecordStrip) {
+                    --strip;
+                    strip_first = band_strip_first_row(strip, band_high);
+                    strip_last = band_strip_last_row(strip, rows, cols, band_low);
+                    strip_pad = band_strip_pad(strip_first, strip_last);
+                    strip_at -= 32 * int64_t(strip_pad);
+                }
+                // The proof keeps every optimal path inside the band, which the swept rows hold; a row
+                // outside them would read another strip's decisions, so the walk stops and flags the pair.
+                if (row < strip_first || row > strip_last) {
+                    if (a.failed) a.failed[pair] = kWalkFailed;
+                    break;
+                }
+                const int within = (column - 1) % kRecordStrip;
+                const int member = within / 16;
+                slot_in = within % 16;
+                at = base + strip_at + int64_t(member) * strip_pad + (row - strip_first + (member & 3));
+            } else if (banded) {
                 // The band's layout: place o = column - row - low, a lane of 16 places a block of rows.
                 const int place = column - row - low;
                 // The proof keeps every optimal path inside the band; a place outside it would read
@@ -194,15 +231,19 @@ __global__ void gather_cigars_kernel(const char *__restrict__ slots, const int64
 }
 
 __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count, bool uniform,
-                                  int32_t band_pair_limit,
-                                  bool band, int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes,
+                                  int32_t band_pair_limit, bool band, const int32_t *__restrict__ widths,
+                                  int64_t *__restrict__ decision_words, int64_t *__restrict__ slot_bytes,
                                   uint8_t *__restrict__ layouts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const PairShape sh = shapes[first_pair + k];
     int64_t words = 0;
     uint8_t layout = 0;
-    if (band && band_eligible(sh.rows, sh.columns)) {
+    if (widths && widths[k] > 0) {
+        // A long pair whose widening band proved a width: its strips' swept rows (layout 5).
+        layout = 5;
+        words = band_record_words(int(sh.rows), int(sh.columns), widths[k]);
+    } else if (band && band_eligible(sh.rows, sh.columns)) {
         // The 16-bit pair band (its pairs' rows and columns within the limit) records planes (layout 3).
         layout = int64_t(sh.rows) + sh.columns <= band_pair_limit ? 3 : 1;
         words = int64_t(kBandLanes) * ((int64_t(sh.rows) + 3) & ~int64_t(3));
@@ -218,16 +259,18 @@ __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t 
     layouts[k] = layout;
 }
 
-// Cells a batch's sweeps update: 64 a row for a banded pair (out[0]), the whole matrix for the rest and
-// again for each leftover of the band (out[1]).
+// Cells a batch's sweeps update: 64 a row for a banded pair (out[0]); the whole matrix for the rest and
+// again for each leftover of the band, and a band-recorded pair's strips (widths, when given) (out[1]).
 __global__ void swept_cells_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count, bool band,
                                    const uint32_t *__restrict__ leftovers, int64_t left,
-                                   unsigned long long *__restrict__ out) {
+                                   const int32_t *__restrict__ widths, unsigned long long *__restrict__ out) {
     unsigned long long banded = 0, whole = 0;
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < count + left;
          k += int64_t(gridDim.x) * blockDim.x) {
         const PairShape sh = k < count ? shapes[first + k] : shapes[leftovers[k - count]];
-        if (k < count && band && band_eligible(sh.rows, sh.columns))
+        if (k < count && widths && widths[k] > 0)
+            whole += (unsigned long long)band_record_cells(int(sh.rows), int(sh.columns), widths[k]);
+        else if (k < count && band && band_eligible(sh.rows, sh.columns))
             banded += (unsigned long long)sh.rows * kBandWidth;
         else
             whole += (unsigned long long)sh.rows * sh.columns;
@@ -252,6 +295,15 @@ __global__ void leftover_words_kernel(const PairShape *__restrict__ shapes, cons
     const int G = record_lanes(sh.columns, uniform);
     const int W = G * 16;
     words[k] = (int64_t(sh.columns) + W - 1) / W * G * (((int64_t(sh.rows) + 2) | 3) + 1);
+}
+
+// The pairs of [first, first + count) a block sweeps when scoring (kWideRows x kWideColumns or more), listed.
+__global__ void long_pairs_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count,
+                                  uint32_t *__restrict__ list, unsigned int *__restrict__ listed) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const PairShape sh = shapes[first + k];
+    if (sh.rows >= kWideRows && sh.columns >= kWideColumns) list[atomicAdd(listed, 1u)] = uint32_t(first + k);
 }
 
 // Points each leftover's decisions at its place in the extra buffer and marks its layout.
@@ -422,15 +474,17 @@ struct PhaseTimer {
 // then whole). Otherwise the band's score, a real alignment's, says how wide a band would prove a score
 // that good: g gap letters outside it must cost more than the score, g > (4 (open - extend) + best (rows +
 // columns) - 2 score) / (best - 2 extend). The pair goes round again at that width (at least twice the
-// last, rounded up to 1,024 diagonals) unless this is the `last` round or that band's strips would sweep
-// three fifths of its rows or more: then to the whole-matrix list. With `swept` null, every pair is
-// routed to `first_width`.
+// last, rounded up to 1,024 diagonals) unless this is the `last` round or that band's strips of
+// `strip_columns` would sweep three fifths of its rows or more: then to the whole-matrix list. With `swept`
+// null, every pair is routed to `first_width`. With `proven`, a pair whose band proves its score leaves the
+// width there (by pair - proven_first).
 __global__ void wide_route_kernel(const PairShape *__restrict__ shapes, const uint32_t *__restrict__ pending,
                                   const int32_t *__restrict__ swept, int64_t count, int32_t first_width, bool last,
                                   const int32_t *__restrict__ scores, int32_t best, int32_t open, int32_t extend,
                                   uint32_t *__restrict__ next, int32_t *__restrict__ next_width,
                                   unsigned int *__restrict__ next_count, uint32_t *__restrict__ whole,
-                                  unsigned int *__restrict__ whole_count) {
+                                  unsigned int *__restrict__ whole_count, int32_t *__restrict__ proven,
+                                  int64_t proven_first, int32_t strip_columns) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const uint32_t pair = pending[k];
@@ -442,7 +496,10 @@ __global__ void wide_route_kernel(const PairShape *__restrict__ shapes, const ui
         const int32_t low = band_low_for_width(rows, columns, done);
         if (low == INT32_MIN) return;
         const int64_t score = scores[pair];
-        if (band_proves_width(score, rows, columns, low, done, best, open, extend)) return;
+        if (band_proves_width(score, rows, columns, low, done, best, open, extend)) {
+            if (proven) proven[pair - proven_first] = int32_t(done);
+            return;
+        }
         const int64_t per_letter = int64_t(best) - 2 * int64_t(extend);
         if (per_letter <= 0) {  // no band proves anything narrower than the matrix
             whole[atomicAdd(whole_count, 1u)] = pair;
@@ -454,7 +511,7 @@ __global__ void wide_route_kernel(const PairShape *__restrict__ shapes, const ui
         width = (width + 1023) / 1024 * 1024;
     }
     const bool banded = !last && width < (int64_t(1) << 30) && band_low_for_width(rows, columns, width) != INT32_MIN &&
-                        10 * (int64_t(sweep::kBlock) * 16 + width) < 6 * rows;
+                        10 * (strip_columns + width) < 6 * rows;
     if (banded) {
         const unsigned at = atomicAdd(next_count, 1u);
         next[at] = pair;
@@ -467,9 +524,13 @@ __global__ void wide_route_kernel(const PairShape *__restrict__ shapes, const ui
 // Scores of long global pairs (the block-a-pair class) by a widening band: a first round sweeps each pair
 // over 2,048 diagonals; a pair its band does not prove goes round once more at the width its band score
 // says would prove it, or is swept whole when that band would cover most of its matrix (or its second
-// band proves nothing either). Every score is the whole matrix's.
+// band proves nothing either). Every score is the whole matrix's. With `proven`, each pair whose band
+// proved its score leaves that band's width there (by pair - proven_first; the rest are left as they were),
+// and the pairs left to the whole matrix are not swept here: their recording gives their scores; a band
+// is then worth its rounds when the recording's strips (kRecordStrip columns) would sweep few of a pair's
+// rows, where the scores' own strips are a block's 4,096 columns.
 void widening_band(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, const uint32_t *order,
-                   int64_t count, KernelArgs args) {
+                   int64_t count, KernelArgs args, int32_t *proven = nullptr, int64_t proven_first = 0) {
     if (count <= 0) return;
     const TableArgs targs = table_args(table, false);
     int32_t best = -128;
@@ -491,7 +552,8 @@ void widening_band(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
         DINARA_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned int), gpu->stream));
         wide_route_kernel<<<unsigned((left + 255) / 256), 256, 0, gpu->stream>>>(
             batch.shapes, pending, swept, left, kFirstWidth, round == kBandRounds, args.scores, best, table.open,
-            table.extend, next, next_widths, counts, whole, counts + 1);
+            table.extend, next, next_widths, counts, whole, counts + 1, proven, proven_first,
+            proven ? kRecordStrip : 16 * kBlock);
         DINARA_CUDA(cudaGetLastError());
         gpu->launches += 1;
         unsigned int routed = 0;
@@ -515,7 +577,7 @@ void widening_band(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable 
         swept = next_widths;
     }
     unsigned int swept_whole = 0;
-    read_back(gpu, &swept_whole, counts + 1, sizeof swept_whole);
+    if (!proven) read_back(gpu, &swept_whole, counts + 1, sizeof swept_whole);
     if (swept_whole > 0) {
         int64_t blocks = persistent_blocks(gpu, &affine_wide_kernel<false, false>);
         blocks = std::max<int64_t>(1, std::min<int64_t>(blocks, swept_whole));
@@ -545,17 +607,20 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
         if (bucket == kBandClass || bucket == kBandPairsClass) continue;
         if (b.end[bucket] <= b.begin[bucket]) continue;
         const bool wide = bucket == kWideClass;
-        const bool pairs16 = !wide && bucket >= kWholePairsClass;
-        const int cls = pairs16 ? bucket - kWholePairsClass : wide ? 4 : bucket;
+        // Recording, a long global pair whose widening band proved a width: its strips over that band.
+        const bool band_record = bucket == kBandRecordClass;
+        const bool pairs16 = !wide && !band_record && bucket >= kWholePairsClass;
+        const int cls = pairs16 ? bucket - kWholePairsClass : wide || band_record ? 4 : bucket;
         if (wide && !batch.local && !record && band_serves(batch, table)) {
             // Long global pairs take the widening band first.
             widening_band(gpu, batch, table, schedule.order + b.begin[bucket], b.end[bucket] - b.begin[bucket], args);
             continue;
         }
-        KernelFn fn = wide      ? (batch.local ? &affine_wide_kernel<true, false> : &affine_wide_kernel<false, false>)
-                      : pairs16 ? pick_pairs_kernel(cls, batch.local)
-                                : pick_kernel(cls, batch.local, record, batch.bits, smem);
-        const int G = wide ? kBlock : smem && !pairs16 ? 32 : affine_lanes(cls);
+        KernelFn fn = band_record ? &affine_kernel<32, 16, false, true, 2, false, false, true>
+                      : wide      ? (batch.local ? &affine_wide_kernel<true, false> : &affine_wide_kernel<false, false>)
+                      : pairs16   ? pick_pairs_kernel(cls, batch.local)
+                                  : pick_kernel(cls, batch.local, record, batch.bits, smem);
+        const int G = wide ? kBlock : (smem && !pairs16) || band_record ? 32 : affine_lanes(cls);
         const int groups_per_block = (pairs16 ? 2 : 1) * kBlock / G;
         int64_t blocks = persistent_blocks(gpu, fn);
         const int64_t needed = (b.end[bucket] - b.begin[bucket] + groups_per_block - 1) / groups_per_block;
@@ -563,7 +628,7 @@ void affine_launch_all(dinara_gpu *gpu, const AffineBatch &batch, const AffineTa
         if (blocks < 1) blocks = 1;
         // Carry slots, one a group, each as long as the tallest pair: only a launch whose pairs may be
         // wider than one strip reads them.
-        const int width = wide ? 16 * kBlock : smem && !pairs16 ? 512 : affine_lanes(cls) * affine_columns(cls);
+        const int width = wide ? 16 * kBlock : (smem && !pairs16) || band_record ? 512 : affine_lanes(cls) * affine_columns(cls);
         args.carry = nullptr;
         args.carry_stride = 0;
         if (batch.max_columns > uint32_t(width)) {
@@ -680,13 +745,13 @@ unsigned long long *band_counter(dinara_gpu *gpu) {
 
 // Adds the cells a batch's sweeps updated to the context's tally (only while it times): the whole matrices
 // from their shapes, the bands' cells as their launches counted them (a narrow pass and a wide one where
-// both ran).
+// both ran), band-recorded pairs' strips from their widths (when given).
 void tally_swept(dinara_gpu *gpu, const PairShape *shapes, int64_t first, int64_t count, bool band,
-                 const uint32_t *leftovers, int64_t left) {
+                 const uint32_t *leftovers, int64_t left, const int32_t *widths = nullptr) {
     if (!gpu->timing) return;
     unsigned long long *out = reinterpret_cast<unsigned long long *>(gpu->class_counts.ensure<unsigned int>(20) + 12);
     DINARA_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), gpu->stream));
-    swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, out);
+    swept_cells_kernel<<<256, 256, 0, gpu->stream>>>(shapes, first, count, band, leftovers, left, widths, out);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     unsigned long long host[2] = {0, 0};
@@ -789,6 +854,36 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     timer.stop();
 }
 
+// Long global pairs of an alignment batch: their scores by the widening band, and each pair's proven width
+// (by pair - first_pair; 0 for a pair its band left to the whole matrix), so that its recording sweeps its
+// band's rows alone. Null when the range holds no long pair.
+int32_t *proven_band_widths(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
+                            int64_t first_pair, int64_t count) {
+    uint32_t *list = gpu->long_pairs.ensure<uint32_t>(size_t(count));
+    unsigned int *listed = gpu->class_counts.ensure<unsigned int>(20) + 18;
+    DINARA_CUDA(cudaMemsetAsync(listed, 0, sizeof(unsigned int), gpu->stream));
+    long_pairs_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(batch.shapes, first_pair, count, list,
+                                                                             listed);
+    DINARA_CUDA(cudaGetLastError());
+    gpu->launches += 1;
+    unsigned int found = 0;
+    read_back(gpu, &found, listed, sizeof found);
+    if (found == 0) return nullptr;
+    int32_t *widths = gpu->record_widths.ensure<int32_t>(size_t(count));
+    DINARA_CUDA(cudaMemsetAsync(widths, 0, sizeof(int32_t) * size_t(count), gpu->stream));
+    KernelArgs args;
+    std::memset(&args, 0, sizeof args);
+    args.tape = batch.tape;
+    args.shapes = batch.shapes;
+    args.open = table.open;
+    args.extend = table.extend;
+    args.scores = scores;
+    PhaseTimer timer(gpu, &gpu->record_ms);
+    widening_band(gpu, batch, table, list, found, args, widths, first_pair);
+    timer.stop();
+    return widths;
+}
+
 }  // namespace
 
 bool band_serves(const AffineBatch &batch, const AffineTable &table) {
@@ -854,9 +949,12 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     const int threads = 256;
     const unsigned blocks = unsigned((count + threads - 1) / threads);
     const int32_t band_pair_limit = band ? pair_limit_of(table) : 0;
+    // Long global pairs take the widening band's scores first, then record over their proven bands.
+    const int32_t *widths = band && !batch.local && batch.max_rows >= kWideRows && batch.max_columns >= kWideColumns
+                                ? proven_band_widths(gpu, batch, table, scores, first_pair, count)
+                                : nullptr;
     slot_sizes_kernel<<<blocks, threads, 0, gpu->stream>>>(batch.shapes, first_pair, count, uniform, band_pair_limit,
-                                                           band, words,
-                                                           slot_bytes, layouts);
+                                                           band, widths, words, slot_bytes, layouts);
     gpu->launches += 1;
     DINARA_CUDA(cudaGetLastError());
     size_t scratch = 0;
@@ -879,6 +977,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(size_t(count) + 1);
     PairLimits limits;
     limits.band = band ? pair_limit_of(table) : 0;
+    limits.band_widths = widths;
+    limits.band_first = first_pair;
     const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band, limits);
 
     PhaseTimer timer(gpu, &gpu->record_ms);
@@ -893,6 +993,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     args.decision_offsets = word_offsets;
     args.ends = ends;
     args.first_pair = first_pair;
+    args.band_widths = widths;
     unsigned int *counters = gpu->class_counts.ensure<unsigned int>(20);
     unsigned int *leftover_count = counters + 8;
     uint32_t *leftovers = nullptr;
@@ -942,6 +1043,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.decisions = decisions;
     w.decisions_extra = extra ? extra : decisions;
     w.layouts = layouts;
+    w.widths = widths;
     w.decision_offsets = word_offsets;
     w.ends = ends;
     w.slot_offsets = slot_offsets;
@@ -964,7 +1066,7 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     walk_clock.stop();
     gpu->launches += 1;
     timer.stop();
-    tally_swept(gpu, batch.shapes, first_pair, count, band, leftovers, left);
+    tally_swept(gpu, batch.shapes, first_pair, count, band, leftovers, left, widths);
 
     // The CIGARs' offsets, then each turned round into place.
     int64_t *offsets = gpu->cigar_offsets.ensure<int64_t>(size_t(count) + 2);

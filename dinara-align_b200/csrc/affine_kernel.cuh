@@ -55,7 +55,8 @@ struct KernelArgs {
     int32_t free_reference_start, free_reference_end, free_query_start, free_query_end;
     // The widening band (affine_wide_kernel<false, true>): the pair at order[item] is swept over
     // band_widths[item] diagonals from band_low_for_width; the pairs whose band proves nothing are redone
-    // wider or whole.
+    // wider or whole. A band-recorded pair (affine_kernel<..., BANDED>) reads its proven width at
+    // band_widths[pair - first_pair].
     const int32_t *band_widths;
 };
 
@@ -67,6 +68,43 @@ __host__ __device__ inline int32_t band_low_for_width(int64_t rows, int64_t colu
     if (span + 1 > width) return INT32_MIN;
     const int64_t slack = (width - 1 - span) / 2;
     return int32_t((delta < 0 ? delta : 0) - slack);
+}
+
+// A band-recorded pair (affine_kernel<..., BANDED>): 32 lanes of 16 columns, strips of kRecordStrip
+// columns, strip s sweeping only the rows its columns share with the pair's band [low, high] of
+// diagonals (column less row) and keeping decisions for those rows alone.
+constexpr int kRecordStrip = 512;
+__host__ __device__ inline int band_strip_first_row(int s, int high) {
+    const int r = s * kRecordStrip + 1 - high;
+    return r > 1 ? r : 1;
+}
+__host__ __device__ inline int band_strip_last_row(int s, int rows, int columns, int low) {
+    const int end = (s + 1) * kRecordStrip < columns ? (s + 1) * kRecordStrip : columns;
+    return end - low < rows ? end - low : rows;
+}
+// Words a strip's lane keeps: its rows, the lane's skew of up to 3 and a whole last sector of 4.
+__host__ __device__ inline int band_strip_pad(int first_row, int last_row) {
+    return ((last_row - first_row + 1 + 2) | 3) + 1;
+}
+// A band-recorded pair's decision words: 32 lanes a strip.
+__host__ __device__ inline int64_t band_record_words(int rows, int columns, int width) {
+    const int low = band_low_for_width(rows, columns, width);
+    const int high = low + width - 1;
+    int64_t words = 0;
+    for (int s = 0; s * kRecordStrip < columns; ++s)
+        words += 32 * int64_t(band_strip_pad(band_strip_first_row(s, high), band_strip_last_row(s, rows, columns, low)));
+    return words;
+}
+// The cells a band-recorded pair's strips sweep: each strip's rows by its columns.
+__host__ __device__ inline int64_t band_record_cells(int rows, int columns, int width) {
+    const int low = band_low_for_width(rows, columns, width);
+    const int high = low + width - 1;
+    int64_t cells = 0;
+    for (int s = 0; s * kRecordStrip < columns; ++s) {
+        const int strip_columns = columns - s * kRecordStrip < kRecordStrip ? columns - s * kRecordStrip : kRecordStrip;
+        cells += int64_t(band_strip_last_row(s, rows, columns, low) - band_strip_first_row(s, high) + 1) * strip_columns;
+    }
+    return cells;
 }
 
 struct TableArgs {
@@ -86,9 +124,20 @@ __device__ __forceinline__ int32_t free_edge(int letters, int free, int32_t open
 // each end go unaligned for nothing (scored.mojo:69-240 FROM_EDGE): the first row's and first column's
 // cells hold free_edge, and the score is the best end on the last row within free_query_end letters of
 // the last column or on the last column within free_reference_end letters of the last row.
-template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE, bool FREE = false>
+//
+// With BANDED (global recording, 32 lanes of 16 columns) a pair's strip sweeps only the rows its columns
+// share with a band of diagonals whose score a sweep over it has proven (band_proves_width), and every
+// cell around those rows is unreached (kOut). Each cell's value is then a real path's score within the
+// swept rows, and every optimal path of the whole matrix lies in the band, so along such a path each
+// decision's terms are the whole matrix's (a term an optimal path reaches equals it; one no optimal path
+// reaches is below the cell's value either way), and the walk takes the whole matrix's CIGAR. Decisions
+// are kept strip by strip for the swept rows only (band_strip_pad words a lane).
+template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE, bool FREE = false, bool BANDED = false>
 __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__ table32) {
     static_assert(!FREE || (!LOCAL && !RECORD), "free ends are for global scores");
+    static_assert(!BANDED || (!LOCAL && RECORD && !FREE && G == 32 && G * C == kRecordStrip),
+                  "a band-recorded pair is global, recorded, and swept in strips of kRecordStrip columns");
+    constexpr int32_t kOut = -(1 << 28);  // unreached: below every score ScoreReach lets a pair hold
     constexpr int W = G * C;
     constexpr int GPW = 32 / G;
     __shared__ uint2 rows16[4];
@@ -134,11 +183,26 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
         int64_t dec_base = 0;
         const int rows_pad = ((rows + 2) | 3) + 1;
         if (RECORD && work) dec_base = p.decision_offsets[pair - p.first_pair];
+        // BANDED: the band's diagonals [low, high], the strip's first decision word past the pair's earlier
+        // strips', and the previous strip's last swept row.
+        int low = 0, high = 0;
+        if (BANDED && work) {
+            const int width = p.band_widths[pair - p.first_pair];
+            low = band_low_for_width(rows, cols, width);
+            high = low + width - 1;
+        }
+        int64_t strip_base = 0;
+        int previous_last = rows;
 
         for (int s = 0; s < warp_strips; ++s) {
             const bool strip_live = s < strips;
             const int first_col = s * W + member * C;
             const int owned = min(max(cols - first_col, 0), C);
+            // The strip's rows (BANDED: those its columns share with the band) and its lanes' words.
+            const int first_row = BANDED ? band_strip_first_row(s, high) : 1;
+            const int last_row = BANDED ? band_strip_last_row(s, rows, cols, low) : rows;
+            const int strip_pad = BANDED ? band_strip_pad(first_row, last_row) : rows_pad;
+            const bool from_top = !BANDED || first_row == 1;
             uint32_t sel[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {
@@ -154,26 +218,36 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
             int32_t H[C], D[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {
-                // The first row, held shifted: with free ends a column's true border less column x extend.
+                // The first row, held shifted: with free ends a column's true border less column x extend;
+                // BANDED, a strip starting lower has only unreached cells above it.
                 H[k] = FREE ? free_edge(first_col + k + 1, free_qs, open, extend) - (first_col + k + 1) * extend : top;
                 D[k] = H[k] + first_gap;
+                if (!from_top) H[k] = D[k] = kOut;
             }
             int32_t edgeH = FREE ? free_edge(first_col + C, free_qs, open, extend) - (first_col + C) * extend : top;
             int32_t edgeI = edgeH + first_gap;
             int32_t above_left = LOCAL ? 0 : (first_col == 0 ? 0 : opening);
             if (FREE) above_left = free_edge(first_col, free_qs, open, extend) - first_col * extend;
-            const int steps = strip_live ? rows + G : 0;
+            if (!from_top) {
+                // Above and left of the first row: the previous strip's last column for lane 0, else unreached.
+                edgeH = edgeI = kOut;
+                above_left = member == 0 && s > 0 && strip_live ? p.carry[slot * p.carry_stride + (first_row - 1)].x
+                                                                 : kOut;
+            }
+            const int steps = strip_live ? last_row - first_row + 1 + G : 0;
             const int warp_steps = warp_max(steps);
             uint64_t buffered[4] = {0, 0, 0, 0};
             uint64_t *lane_block = nullptr;
-            if (RECORD) lane_block = p.decisions + dec_base + int64_t(s * G + member) * rows_pad;
+            if (RECORD)
+                lane_block = p.decisions + dec_base +
+                             (BANDED ? strip_base + int64_t(member) * strip_pad : int64_t(s * G + member) * rows_pad);
 
             for (int step0 = 1; step0 <= warp_steps; step0 += 4) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int step = step0 + u;
                     if (step <= warp_steps) {
-                        const int row = step - member;
+                        const int row = first_row - 1 + step - member;
                         int32_t leftH = __shfl_up_sync(kFull, edgeH, 1, G);
                         int32_t leftI = __shfl_up_sync(kFull, edgeI, 1, G);
                         if (member == 0) {
@@ -182,6 +256,8 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                 // The first column with free ends: the row's true border less row x extend.
                                 if (FREE) leftH = free_edge(row, free_rs, open, extend) - row * extend;
                                 leftI = leftH + first_gap;
+                            } else if (BANDED && row > previous_last) {
+                                leftH = leftI = kOut;  // left of the previous strip's swept rows: unreached
                             } else {
                                 const int r = min(max(row, 0), rows);
                                 const int2 c = p.carry[slot * p.carry_stride + r];
@@ -191,7 +267,7 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                         }
                         int32_t diag = above_left;
                         above_left = leftH;
-                        if (strip_live && row >= 1 && row <= rows) {
+                        if (strip_live && row >= first_row && row <= last_row) {
                             const uint32_t rl = letter_at<BITS>(p.tape, sh.first_word, uint32_t(row - 1));
                             uint2 tr = make_uint2(0, 0);
                             const int32_t *trow = nullptr;
@@ -293,8 +369,8 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                             }
                             if (RECORD) {
                                 buffered[u] = (uint64_t(word_hi) << 32) | word_lo;
-                                if (u == 3 || row == rows) {
-                                    uint64_t *at = lane_block + ((row - 1 + (member & 3)) & ~3);
+                                if (u == 3 || row == last_row) {
+                                    uint64_t *at = lane_block + ((row - first_row + (member & 3)) & ~3);
                                     reinterpret_cast<uint4 *>(at)[0] = make_uint4(
                                         uint32_t(buffered[0]), uint32_t(buffered[0] >> 32), uint32_t(buffered[1]),
                                         uint32_t(buffered[1] >> 32));
@@ -308,6 +384,10 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                 }
             }
             __syncwarp();
+            if (BANDED) {
+                strip_base += int64_t(G) * strip_pad;
+                previous_last = last_row;
+            }
         }
 
         // Results: a global score is the corner shifted back; a local one the group's best.
@@ -636,7 +716,7 @@ __global__ void __launch_bounds__(kBlock) affine_wide_kernel(KernelArgs p, Table
             const int owned = min(max(cols - first_col, 0), C);
             // The strip's rows: those its columns share with the band (all of them when not banded).
             const int first_row = BANDED ? max(1, s * W - high) : 1;
-            const int last_row = BANDED ? min(rows, s * W + W - 1 - low) : rows;
+            const int last_row = BANDED ? min(rows, s * W + W - low) : rows;
             uint32_t sel[C];
 #pragma unroll
             for (int k = 0; k < C; ++k) {

@@ -92,7 +92,11 @@ __device__ void classify_pair(const PairShape *__restrict__ shapes, const uint32
     const bool empty = shape.rows == 0 || shape.columns == 0;
     int cls;
     uint32_t strips = 0;
-    if (band && band_eligible(shape.rows, shape.columns)) {
+    if (limits.band_widths && limits.band_widths[pair - limits.band_first] > 0) {
+        cls = kBandRecordClass;
+        strips = (shape.columns + 511) / 512;
+        if (strips > 255) strips = 255;
+    } else if (band && band_eligible(shape.rows, shape.columns)) {
         cls = int64_t(shape.rows) + shape.columns <= limits.band ? kBandPairsClass : kBandClass;
     } else {
         cls = empty ? 0 : affine_shape_for(shape.columns, record != 0);

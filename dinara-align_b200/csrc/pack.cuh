@@ -18,13 +18,15 @@ void pack_pairs(dinara_gpu *gpu, const uint8_t *letters_device, const int64_t *o
 // Classes: the whole-matrix shape classes 0-4 (affine_shape_for with `record`); with `band` the proven
 // band, kBandClass, and of those the pairs whose rows and columns sum to at most `limits.band`,
 // kBandPairsClass, for the 16-bit pair band sweep; the whole-matrix pairs the 16-bit pair score sweep
-// takes, kWholePairsClass plus the shape class; and long pairs one block sweeps, kWideClass. `order` is
-// valid on the device until the next call.
-constexpr int kClasses = 13;
+// takes, kWholePairsClass plus the shape class; long pairs one block sweeps, kWideClass; and, recording,
+// pairs whose widening band proved a width (`limits.band_widths`), kBandRecordClass. `order` is valid on
+// the device until the next call.
+constexpr int kClasses = 14;
 constexpr int kBandClass = 5;
 constexpr int kBandPairsClass = 6;
 constexpr int kWholePairsClass = 7;
 constexpr int kWideClass = 12;
+constexpr int kBandRecordClass = 13;
 // A pair a whole block sweeps (kWideClass), scoring without a CIGAR: at least this tall and this wide.
 constexpr uint32_t kWideRows = 4096, kWideColumns = 2048;
 struct Schedule {
@@ -44,6 +46,10 @@ struct PairLimits {
     // Local: a pair fits when best x swept columns + rows x row_step is at most `whole`.
     int32_t best = 1;
     int32_t row_step = 0;
+    // Recording: each pair's proven band width by pair - band_first (0: none), when given; a pair with one
+    // goes to kBandRecordClass.
+    const int32_t *band_widths = nullptr;
+    int64_t band_first = 0;
 };
 
 // The order of pairs [first, first + count), or of the `count` pairs listed in `list` (device) when given.

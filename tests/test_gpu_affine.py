@@ -152,6 +152,97 @@ def test_long_pairs_on_a_whole_block(da, oracle, local):
     np.testing.assert_array_equal(da.scores_tape(tape, scoring, mode), expected)
 
 
+def _cigar_score(reference, query, cigar, scoring):
+    """The score of the alignment a CIGAR spells under a uniform Scoring (a gap of L letters scores
+    opening + L x extension), with the letters it consumes on each side."""
+    import re
+
+    alphabet = scoring.alphabet
+    table = np.asarray(scoring.table).reshape(len(alphabet), len(alphabet))
+    score, r, q = 0, 0, 0
+    for count, op in re.findall(r"(\d+)([=XMDI])", cigar):
+        count = int(count)
+        if op in "=XM":
+            for k in range(count):
+                score += int(table[alphabet.index(reference[r + k]), alphabet.index(query[q + k])])
+            r += count
+            q += count
+        else:
+            score += scoring.opening + count * scoring.extension
+            if op == "D":
+                r += count
+            else:
+                q += count
+    return score, r, q
+
+
+@pytest.mark.parametrize("scoring_name", ["config2", "dna"])
+def test_long_cigars_over_a_proven_band(da, oracle, scoring_name):
+    """Global CIGARs of long pairs (4,096 x 2,048 letters and more) recorded strip by strip over the band
+    their widening band proved: few and many errors, a long deletion and a long insertion that take the
+    path far off the main diagonal, a path that leaves the main diagonal and comes back, next to short
+    pairs. Scores and CIGARs equal the whole-matrix oracle's; the recording sweeps well under the whole
+    matrices' cells; and a 20 kbp pair's CIGAR spells the oracle's score."""
+    import ctypes
+
+    from dinara_align import _native as native, workloads
+
+    rng = np.random.default_rng(83)
+    scoring = da.Scoring.uniform(*SCORINGS[scoring_name])
+    refs, queries = [], []
+    tape = workloads.pairs_with_errors(rng, np.array([4300, 4600, 5000, 4800, 4400, 200, 180]),
+                                       np.array([0.01, 0.05, 0.12, 0.3, 0.05, 0.05, 0.1]), workloads.HALF_QUARTERS)
+    for p in range(tape.pairs):
+        refs.append(tape.reference(p).decode())
+        queries.append(tape.query(p).decode())
+    a = "".join(rng.choice(list("ACGT"), size=4500))
+    def letters(n):
+        return "".join(rng.choice(list("ACGT"), size=n))
+
+    refs += [a, a, a, a]
+    queries += [a[:2000] + a[2600:],                 # 600 letters deleted
+                a[:1500] + letters(700) + a[1500:],  # 700 inserted
+                a[:1000] + a[1900:] + letters(900),  # off the main diagonal and back
+                a[:2000] + letters(1800) + a[2000:]]  # the first band's ends 1,800 diagonals apart
+    batch = da.Tape.of(refs, queries)
+    expected_scores, expected_cigars = _oracle_batch(oracle, da, batch, scoring, False, True)
+    found = da.alignments(refs, queries, scoring)
+    assert [x.score for x in found] == list(expected_scores)
+    assert [x.cigar for x in found] == expected_cigars
+
+    # The recording swept the long pairs' bands, not their whole matrices.
+    class Timing(ctypes.Structure):
+        _fields_ = [("total_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double), ("record_ms", ctypes.c_double),
+                    ("launches", ctypes.c_int64), ("cells", ctypes.c_int64), ("class_ms", ctypes.c_double * 8),
+                    ("class_launches", ctypes.c_int64 * 8), ("band_cells", ctypes.c_int64),
+                    ("whole_cells", ctypes.c_int64)]
+
+    lib = native.lib()
+    handle = native.context(0)
+    struct, _table, _alphabet = scoring._struct()
+    mode = da.Mode.GLOBAL._struct()
+    native.check(lib.dinara_gpu_resident_load(handle, batch.pairs, batch.letters.ctypes.data,
+                                              native.pointer(batch.offsets, ctypes.c_int64), ctypes.byref(struct)),
+                 handle)
+    timing = Timing()
+    native.check(lib.dinara_gpu_resident_align(handle, ctypes.byref(mode), 1, 1, ctypes.byref(timing)), handle)
+    whole = sum(len(r) * len(q) for r, q in zip(refs, queries))
+    assert 0 < timing.cells < 0.8 * whole
+
+    # A 20 kbp pair: its CIGAR consumes both sequences and scores what the oracle's two-row sweep gives.
+    b = "".join(rng.choice(list("ACGT"), size=20000))
+    long_tape = workloads.pairs_with_errors(rng, np.array([20000]), 0.04, workloads.HALF_QUARTERS)
+    long_refs = [b, long_tape.reference(0).decode()]
+    long_queries = [b[:9000] + b[9400:], long_tape.query(0).decode()]
+    got = da.alignments(long_refs, long_queries, scoring)
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    for reference, query, alignment in zip(long_refs, long_queries, got):
+        want = oracle.gotoh_score(oracle.codes(reference), oracle.codes(query), table, 4, op, ex)[0]
+        assert alignment.score == want
+        assert _cigar_score(reference, query, alignment.cigar, scoring) == (want, len(reference), len(query))
+
+
 def test_local_spans_placed_as_reference(da, oracle):
     """Local spans by as_alignment's rule (scoring.mojo:724-744): the aligned letters' last place."""
     refs = ["GGGGACGTACGTGGGG", "ACGTTTTTACGT" * 3, "TTTTACGTACGTTTTT"]
