@@ -813,10 +813,30 @@ void launch_bands(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &
 
 namespace {
 
+// Each pair's span with free ends from its best end and the start found back from it: the reference's
+// letters from end row less the back sweep's row to the end row, then the query's likewise.
+__global__ void free_spans_kernel(const int64_t *__restrict__ ends, const int64_t *__restrict__ found, int64_t count,
+                                  int64_t *__restrict__ spans) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t end_row = ends[k] >> 32, end_column = ends[k] & 0xffffffff;
+    const int64_t back_row = found[k] >> 32, back_column = found[k] & 0xffffffff;
+    int64_t *span = spans + 4 * k;
+    span[0] = end_row - back_row;
+    span[1] = end_row;
+    span[2] = end_column - back_column;
+    span[3] = end_column;
+}
+
 // Global scores with free ends: every pair over its whole matrix in 32 bits, one shape (32 lanes of 16
-// columns, strips of 512) with the table in shared memory, the free-end form of the sweep.
+// columns, strips of 512) with the table in shared memory, the free-end form of the sweep. With `spans`
+// (4 a pair of the range, by pair - first), each pair's span as the reference places it
+// (scoring.mojo:690-722 mode_span, scored.mojo:616-633 started_span): its end, of equal best ends the one
+// furthest along the reference less the query; then a sweep back over both prefixes to that end, read
+// backwards, with the letters free at the start free at its end, whose best end nearest the other way
+// (the least along the reference less the query, reversed) is the start.
 void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
-                     int64_t first, int64_t count) {
+                     int64_t first, int64_t count, int64_t *spans) {
     const Schedule order = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, false, PairLimits());
     int32_t *table32 = nullptr;
     upload_table32(gpu, table, false, &table32);
@@ -829,10 +849,17 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     args.open = table.open;
     args.extend = table.extend;
     args.scores = scores;
+    args.first_pair = first;
     args.free_reference_start = batch.free_reference_start;
     args.free_reference_end = batch.free_reference_end;
     args.free_query_start = batch.free_query_start;
     args.free_query_end = batch.free_query_end;
+    int64_t *ends = nullptr;
+    if (spans) {
+        ends = gpu->free_spans.ensure<int64_t>(2 * size_t(count));
+        args.free_ends_out = ends;
+        args.free_highest = 1;
+    }
     KernelFn fn = batch.bits == 8 ? static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 8, true, true>)
                                   : static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 2, true, true>);
     int64_t total = 0;
@@ -851,6 +878,26 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     DINARA_CUDA(cudaGetLastError());
     clock.stop();
     gpu->launches += 1;
+    if (spans) {
+        // The sweep back: each pair's prefixes to its end, backwards, the start's free letters free at the
+        // (backward) end and none at its start; its scores, the same, go to scratch.
+        KernelArgs back = args;
+        back.scores = gpu->free_scores.ensure<int32_t>(size_t(batch.pairs));
+        back.extents = ends;
+        back.free_ends_out = ends + count;
+        back.free_highest = 0;
+        back.free_reference_start = 0;
+        back.free_reference_end = batch.free_reference_start;
+        back.free_query_start = 0;
+        back.free_query_end = batch.free_query_start;
+        ClockSpan back_clock(gpu, kClassWhole, gpu->stream);
+        fn<<<dim3(unsigned(blocks)), kBlock, 0, gpu->stream>>>(back, targs, table32);
+        DINARA_CUDA(cudaGetLastError());
+        back_clock.stop();
+        free_spans_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(ends, ends + count, count, spans);
+        DINARA_CUDA(cudaGetLastError());
+        gpu->launches += 2;
+    }
     timer.stop();
 }
 
@@ -895,10 +942,10 @@ bool band_serves(const AffineBatch &batch, const AffineTable &table) {
 }
 
 void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
-                   int64_t first, int64_t count) {
+                   int64_t first, int64_t count, int64_t *spans) {
     if (count <= 0) return;
     if (batch.free_ends) {
-        free_end_scores(gpu, batch, table, scores, first, count);
+        free_end_scores(gpu, batch, table, scores, first, count, spans);
         return;
     }
     const bool band = band_serves(batch, table);

@@ -62,9 +62,11 @@ constexpr uint8_t kWalkFailed = 2;
 bool band_serves(const AffineBatch &batch, const AffineTable &table);
 
 // Scores of pairs [first, first + count) of a packed batch into `scores` (device, indexed by pair): the
-// proven band where it serves, every other pair over its whole matrix, longest first.
+// proven band where it serves, every other pair over its whole matrix, longest first. With free ends and
+// `spans` (device, 4 a pair of the range), each pair's span as the reference places it: the reference's
+// first and last letter places, then the query's.
 void affine_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
-                   int64_t first, int64_t count);
+                   int64_t first, int64_t count, int64_t *spans = nullptr);
 
 // Alignments of pairs [first_pair, first_pair + count): scores into `scores` (indexed by pair), spans (4
 // per pair of the range: first row, last row, first column, last column of the walk) into `spans`, and

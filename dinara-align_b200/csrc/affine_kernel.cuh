@@ -58,6 +58,14 @@ struct KernelArgs {
     // wider or whole. A band-recorded pair (affine_kernel<..., BANDED>) reads its proven width at
     // band_widths[pair - first_pair].
     const int32_t *band_widths;
+    // Free ends' places (affine_kernel<..., FREE>): with `free_ends_out`, each pair's best end there (row << 32
+    // | column, by pair - first_pair), of equal ends the one furthest along the reference less the query
+    // with `free_highest`, else the least so (scored.mojo:69-100); with `extents`, each pair is its
+    // prefixes of extents[pair - first_pair] (row << 32 | column) letters, both read backwards (the sweep
+    // back from an end for its start, scored.mojo:616-633).
+    int64_t *free_ends_out;
+    const int64_t *extents;
+    int32_t free_highest;
 };
 
 // The lowest diagonal (column less row) of a band of `width` diagonals holding a pair's main and end
@@ -167,7 +175,14 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
             pair = p.order[item];
             sh = p.shapes[pair];
         }
-        const int rows = int(sh.rows), cols = int(sh.columns);
+        int rows = int(sh.rows), cols = int(sh.columns);
+        // FREE with extents: the pair's prefixes, read backwards.
+        const bool backwards = FREE && p.extents != nullptr;
+        if (backwards && live) {
+            const int64_t extent = p.extents[pair - p.first_pair];
+            rows = int(extent >> 32);
+            cols = int(extent & 0xffffffff);
+        }
         const bool work = live && rows > 0 && cols > 0;
         const int strips = work ? (cols + W - 1) / W : 0;
         const int warp_strips = warp_max(strips);
@@ -180,6 +195,18 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
         const int free_qs = FREE ? min(p.free_query_start, cols) : 0;
         const int free_qe = FREE ? min(p.free_query_end, cols) : 0;
         int32_t free_best = -(1 << 30);
+        int free_key = 0;      // the best end's rows less columns
+        int64_t free_at = 0;   // and its place, row << 32 | column
+        const bool highest = FREE && p.free_highest != 0;
+        // An end of `value` at (r, c) against the best so far: higher, or as high on the favoured side.
+        auto offer = [&](int32_t value, int r, int c) {
+            const int key = r - c;
+            if (value > free_best || (value == free_best && (highest ? key > free_key : key < free_key))) {
+                free_best = value;
+                free_key = key;
+                free_at = (int64_t(r) << 32) | int64_t(c);
+            }
+        };
         int64_t dec_base = 0;
         const int rows_pad = ((rows + 2) | 3) + 1;
         if (RECORD && work) dec_base = p.decision_offsets[pair - p.first_pair];
@@ -208,7 +235,7 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
             for (int k = 0; k < C; ++k) {
                 const int col = first_col + k;
                 if (strip_live && col < cols) {
-                    const uint32_t x = letter_at<BITS>(p.tape, sh.second_word, uint32_t(col));
+                    const uint32_t x = letter_at<BITS>(p.tape, sh.second_word, uint32_t(backwards ? cols - 1 - col : col));
                     sel[k] = SMEM_TABLE ? x : selector_of(x);
                 } else {
                     sel[k] = SMEM_TABLE ? 32u : kPadSelector;
@@ -268,7 +295,8 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                         int32_t diag = above_left;
                         above_left = leftH;
                         if (strip_live && row >= first_row && row <= last_row) {
-                            const uint32_t rl = letter_at<BITS>(p.tape, sh.first_word, uint32_t(row - 1));
+                            const uint32_t rl =
+                                letter_at<BITS>(p.tape, sh.first_word, uint32_t(backwards ? rows - row : row - 1));
                             uint2 tr = make_uint2(0, 0);
                             const int32_t *trow = nullptr;
                             if (SMEM_TABLE)
@@ -354,7 +382,7 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                     for (int k = 0; k < C; ++k) {
                                         const int column = first_col + k + 1;
                                         if (k < owned && column >= cols - free_qe)
-                                            free_best = max(free_best, H[k] + (rows + column) * extend);
+                                            offer(H[k] + (rows + column) * extend, rows, column);
                                     }
                                 }
                                 if (owned > 0 && first_col + owned == cols && rows - row <= free_re) {
@@ -364,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                         const int32_t hit = -int32_t(k == owned - 1);
                                         last = (last & ~hit) | (H[k] & hit);
                                     }
-                                    free_best = max(free_best, last + (row + cols) * extend);
+                                    offer(last + (row + cols) * extend, row, cols);
                                 }
                             }
                             if (RECORD) {
@@ -421,18 +449,46 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
             // The best end of the group's lanes, then the first row's and first column's own ends (a free
             // end reaching the border), or an empty side's run along the other's edge.
 #pragma unroll
-            for (int span = 1; span < G; span <<= 1) free_best = max(free_best, __shfl_xor_sync(kFull, free_best, span, G));
+            for (int span = 1; span < G; span <<= 1) {
+                const int32_t their_value = __shfl_xor_sync(kFull, free_best, span, G);
+                const int64_t their_at = __shfl_xor_sync(kFull, free_at, span, G);
+                offer(their_value, int(their_at >> 32), int(their_at & 0xffffffff));
+            }
             if (live && member == 0) {
-                int32_t found = free_best;
                 if (!work) {
-                    found = rows == 0 && cols == 0 ? 0
-                            : cols == 0       ? free_edge(rows - free_re, free_rs, open, extend)
-                                              : free_edge(cols - free_qe, free_qs, open, extend);
+                    if (rows == 0 && cols == 0) {
+                        free_best = 0;
+                        free_at = 0;
+                    } else {
+                        // scored.mojo:155-176: the run along the other side's edge, ending within its free
+                        // letters at the end. Of equal ends, the furthest when the run goes along the
+                        // reference and the highest end is favoured (or along the query and the lowest),
+                        // else the nearest; free_edge never rises with the letters, so the equal ones run
+                        // from the nearest allowed to the last that still scores as it does.
+                        const bool along_reference = rows > 0;
+                        const int length = along_reference ? rows : cols;
+                        const int start_free = along_reference ? free_rs : free_qs;
+                        const int lo = max(length - (along_reference ? free_re : free_qe), 0);
+                        const int32_t top = free_edge(lo, start_free, open, extend);
+                        int reach = lo, beyond = length;
+                        if (along_reference == highest) {
+                            while (reach < beyond) {
+                                const int mid = beyond - (beyond - reach) / 2;
+                                if (free_edge(mid, start_free, open, extend) == top)
+                                    reach = mid;
+                                else
+                                    beyond = mid - 1;
+                            }
+                        }
+                        free_best = top;
+                        free_at = along_reference ? int64_t(reach) << 32 : int64_t(reach);
+                    }
                 } else {
-                    if (cols <= free_qe) found = max(found, free_edge(rows, free_rs, open, extend));
-                    if (rows <= free_re) found = max(found, free_edge(cols, free_qs, open, extend));
+                    if (cols <= free_qe) offer(free_edge(rows, free_rs, open, extend), rows, 0);
+                    if (rows <= free_re) offer(free_edge(cols, free_qs, open, extend), 0, cols);
                 }
-                p.scores[pair] = found;
+                p.scores[pair] = free_best;
+                if (p.free_ends_out) p.free_ends_out[pair - p.first_pair] = free_at;
             }
         } else if (live) {
             const int total = rows + cols;

@@ -1004,49 +1004,136 @@ int64_t dinara_gpu_device_info(dinara_gpu *gpu, char *name, int64_t name_capacit
 
 void dinara_free(char *cigar) { std::free(cigar); }
 
+}  // extern "C"
+
+namespace {
+
+// Scores of a tape's pairs (dinara_gpu_scores_tape's work); with free ends and `spans` (host, 4 a pair),
+// also each pair's span as the reference places it (affine_scores).
+void run_scores(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, int64_t *statuses,
+                int64_t *spans) {
+    if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+    AffineBatch ends;
+    const bool local = check_scores_mode(mode, ends);
+    const CheckedScoring checked = check_scoring(scoring, local);
+    check_offsets(pairs, offsets);
+    if (pairs == 0) return;
+    if (!ends.free_ends) spans = nullptr;
+    DINARA_CUDA(cudaSetDevice(gpu->device));
+    StreamedBatch streamed;
+    start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
+    const Packed &packed = streamed.packed;
+    AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
+    batch.free_ends = ends.free_ends;
+    batch.free_reference_start = ends.free_reference_start;
+    batch.free_reference_end = ends.free_reference_end;
+    batch.free_query_start = ends.free_query_start;
+    batch.free_query_end = ends.free_query_end;
+    int32_t *scores_device = streamed.scores;
+    const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
+    UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
+        std::memcpy(scores + unit.first, unit.stage + unit.layout.scores, size_t(unit.count) * sizeof(int32_t));
+        if (spans)
+            std::memcpy(spans + 4 * unit.first, unit.stage + unit.layout.spans,
+                        size_t(4 * unit.count) * sizeof(int64_t));
+        statuses_of(checked, local, unit.first, unit.count, offsets, unit.stage + unit.layout.unknown, statuses);
+    });
+    run_units(gpu, streamed, units.size(), kLanes, finisher, [&](dinara_gpu *ctx, size_t k) {
+        const int64_t first = units[k].first, count = units[k].second;
+        streamed.pack_unit(ctx, offsets, first, count);
+        int64_t *spans_device = spans ? ctx->ranges.ensure<int64_t>(size_t(4 * count)) : nullptr;
+        affine_scores(ctx, batch, checked.table, scores_device, first, count, spans_device);
+        StagedUnit unit;
+        unit.first = first;
+        unit.count = count;
+        unit.layout = StageLayout(count, 0, spans != nullptr);
+        uint8_t *stage = finisher.stage_for(int64_t(k), unit.layout.bytes);
+        unit.stage = stage;
+        DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.scores, scores_device + first,
+                                    size_t(count) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.unknown, packed.unknown + first, size_t(count),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+        if (spans)
+            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.spans, spans_device, size_t(4 * count) * sizeof(int64_t),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+        finisher.push(int64_t(k), unit, ctx->stream);
+    });
+    finisher.finish();
+}
+
+// Whether a mode asks a Scoring for free ends (ends_free with any letters free, no match score).
+bool free_end_mode(const dinara_mode *mode) {
+    return mode && mode->kind == DINARA_ENDS_FREE && mode->match_score <= 0 &&
+           (mode->reference_start | mode->reference_end | mode->query_start | mode->query_end) != 0;
+}
+
+// Alignments with free ends under a Scoring, as the reference's host path makes them (scoring.mojo:800-813):
+// each pair's score and span from the free-end sweeps (run_scores), then the span's letters aligned
+// globally (dinara_gpu_alignments_tape), whose CIGAR is the alignment's. A pair whose span's global score
+// differs from its free-end score, or whose span is out of its letters, reports a device failure.
+void free_end_alignments(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                         const dinara_scoring *scoring, const dinara_mode *mode, int64_t eqx, int32_t *scores,
+                         int64_t *spans, int64_t *cigar_offsets, char **cigar_bytes, int64_t *statuses) {
+    const size_t room = size_t(std::max<int64_t>(pairs, 1));
+    std::vector<int64_t> own_spans(spans ? 0 : 4 * room);
+    int64_t *placed = spans ? spans : own_spans.data();
+    std::vector<int64_t> first_statuses(room, 0);
+    run_scores(gpu, pairs, letters, offsets, scoring, mode, scores, first_statuses.data(), placed);
+    // The spans' letters as a tape of their own.
+    std::vector<int64_t> inner_offsets(size_t(2 * pairs + 1), 0);
+    std::vector<int64_t> failed(room, 0);
+    int64_t total = 0;
+    for (int64_t p = 0; p < pairs; ++p) {
+        int64_t *span = placed + 4 * p;
+        const int64_t rows = offsets[2 * p + 1] - offsets[2 * p];
+        const int64_t columns = offsets[2 * p + 2] - offsets[2 * p + 1];
+        if (!(0 <= span[0] && span[0] <= span[1] && span[1] <= rows && 0 <= span[2] && span[2] <= span[3] &&
+              span[3] <= columns)) {
+            failed[size_t(p)] = 1;
+            span[0] = span[1] = span[2] = span[3] = 0;
+        }
+        inner_offsets[size_t(2 * p)] = total;
+        total += span[1] - span[0];
+        inner_offsets[size_t(2 * p + 1)] = total;
+        total += span[3] - span[2];
+    }
+    inner_offsets[size_t(2 * pairs)] = total;
+    std::vector<char> inner(size_t(std::max<int64_t>(total, 1)));
+    split_work(pairs, [&](int64_t begin, int64_t end) {
+        for (int64_t p = begin; p < end; ++p) {
+            const int64_t *span = placed + 4 * p;
+            std::memcpy(inner.data() + inner_offsets[size_t(2 * p)], letters + offsets[2 * p] + span[0],
+                        size_t(span[1] - span[0]));
+            std::memcpy(inner.data() + inner_offsets[size_t(2 * p + 1)], letters + offsets[2 * p + 1] + span[2],
+                        size_t(span[3] - span[2]));
+        }
+    });
+    dinara_mode global = *mode;
+    global.reference_start = global.reference_end = global.query_start = global.query_end = 0;
+    std::vector<int32_t> inner_scores(room, 0);
+    std::vector<int64_t> inner_spans(4 * room, 0), inner_statuses(room, 0);
+    const int64_t code = dinara_gpu_alignments_tape(gpu, pairs, inner.data(), inner_offsets.data(), scoring, &global,
+                                                    eqx, inner_scores.data(), inner_spans.data(), cigar_offsets,
+                                                    cigar_bytes, inner_statuses.data());
+    if (code != 0) throw Failure(code, gpu->error);
+    if (!statuses) return;
+    for (int64_t p = 0; p < pairs; ++p) {
+        int64_t status = first_statuses[size_t(p)] != 0 ? first_statuses[size_t(p)] : inner_statuses[size_t(p)];
+        if (status == 0 && (failed[size_t(p)] || inner_scores[size_t(p)] != scores[p])) status = DINARA_DEVICE_FAILURE;
+        statuses[p] = status;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
 int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
                                const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores,
                                int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
-        if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
-        AffineBatch ends;
-        const bool local = check_scores_mode(mode, ends);
-        const CheckedScoring checked = check_scoring(scoring, local);
-        check_offsets(pairs, offsets);
-        if (pairs == 0) return 0;
-        DINARA_CUDA(cudaSetDevice(gpu->device));
-        StreamedBatch streamed;
-        start_batch(streamed, gpu, pairs, letters, offsets, checked.codes, checked.bits);
-        const Packed &packed = streamed.packed;
-        AffineBatch batch{pairs, checked.bits, local, packed.tape, packed.shapes, packed.max_rows, packed.max_columns};
-        batch.free_ends = ends.free_ends;
-        batch.free_reference_start = ends.free_reference_start;
-        batch.free_reference_end = ends.free_reference_end;
-        batch.free_query_start = ends.free_query_start;
-        batch.free_query_end = ends.free_query_end;
-        int32_t *scores_device = streamed.scores;
-        const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
-        UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
-            std::memcpy(scores + unit.first, unit.stage + unit.layout.scores, size_t(unit.count) * sizeof(int32_t));
-            statuses_of(checked, local, unit.first, unit.count, offsets, unit.stage + unit.layout.unknown, statuses);
-        });
-        run_units(gpu, streamed, units.size(), kLanes, finisher, [&](dinara_gpu *ctx, size_t k) {
-            const int64_t first = units[k].first, count = units[k].second;
-            streamed.pack_unit(ctx, offsets, first, count);
-            affine_scores(ctx, batch, checked.table, scores_device, first, count);
-            StagedUnit unit;
-            unit.first = first;
-            unit.count = count;
-            unit.layout = StageLayout(count, 0, false);
-            uint8_t *stage = finisher.stage_for(int64_t(k), unit.layout.bytes);
-            unit.stage = stage;
-            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.scores, scores_device + first,
-                                        size_t(count) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-            DINARA_CUDA(cudaMemcpyAsync(stage + unit.layout.unknown, packed.unknown + first, size_t(count),
-                                        cudaMemcpyDeviceToHost, ctx->stream));
-            finisher.push(int64_t(k), unit, ctx->stream);
-        });
-        finisher.finish();
+        run_scores(gpu, pairs, letters, offsets, scoring, mode, scores, statuses, nullptr);
         return 0;
     });
 }
@@ -1074,6 +1161,11 @@ int64_t dinara_gpu_alignments_tape(dinara_gpu *gpu, int64_t pairs, const char *l
                                    int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
         if (!gpu) throw Failure(DINARA_INVALID_MODE, "no context");
+        if (free_end_mode(mode)) {
+            free_end_alignments(gpu, pairs, letters, offsets, scoring, mode, eqx, scores, spans, cigar_offsets,
+                                cigar_bytes, statuses);
+            return 0;
+        }
         const bool local = check_mode(mode);
         const CheckedScoring checked = check_scoring(scoring, local);
         check_offsets(pairs, offsets);
@@ -1198,7 +1290,8 @@ int64_t dinara_gpu_alignments(dinara_gpu *gpu, int64_t pairs, const char *const 
                               const int64_t *query_lengths, const dinara_scoring *scoring, const dinara_mode *mode,
                               int64_t eqx, dinara_alignment *alignments, int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
-        const bool local = check_mode(mode);
+        AffineBatch ends;
+        const bool local = free_end_mode(mode) ? check_scores_mode(mode, ends) : check_mode(mode);
         (void)check_scoring(scoring, local);
         std::vector<char> letters;
         std::vector<int64_t> offsets;

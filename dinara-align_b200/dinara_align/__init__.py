@@ -139,8 +139,9 @@ class Anchor:
 @dataclass(frozen=True)
 class Mode:
     """Which alignments count (the reference's `Mode`, fields in `dinara_mode` order). The GPU serves
-    `Mode.GLOBAL` and, under a `Scoring`, `Mode.local()`, and for a `Scoring`'s scores free ends:
-    `INFIX`, `PREFIX`, `SUFFIX` and `ends_free(...)` (with no match score of the mode's own)."""
+    `Mode.GLOBAL` and, under a `Scoring`, `Mode.local()` and free ends: `INFIX`, `PREFIX`, `SUFFIX` and
+    `ends_free(...)` (with no match score of the mode's own), scores and alignments, the latter placed as
+    the reference's host path places them."""
 
     kind: int = _ENDS
     reference_start: int = 0

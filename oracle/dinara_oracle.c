@@ -162,17 +162,49 @@ static inline int32_t free_edge(int64_t letters, int64_t free_letters, int32_t o
     return letters <= free_letters ? 0 : gap_run(open, extend, letters - free_letters);
 }
 
-int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
-                                const int8_t *table, int32_t size, int32_t open, int32_t extend,
-                                int64_t reference_start, int64_t reference_end, int64_t query_start,
-                                int64_t query_end) {
+/* An end of `value` at (r, c) against the best so far (scored.mojo:69-100 swept_cells' rule for ends from
+ * the edges): higher, or as high and further along the reference less the query with `highest` (the
+ * least so without). Each diagonal meets the last row and the last column at most once between them, so
+ * no two ends tie on both. */
+static inline void offer_end(int32_t value, int64_t r, int64_t c, int highest, int32_t *best, int64_t *best_row,
+                             int64_t *best_column) {
+    const int64_t key = r - c, best_key = *best_row - *best_column;
+    if (value > *best || (value == *best && (highest ? key > best_key : key < best_key))) {
+        *best = value;
+        *best_row = r;
+        *best_column = c;
+    }
+}
+
+int32_t oracle_gotoh_end_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                              const int8_t *table, int32_t size, int32_t open, int32_t extend,
+                              int64_t reference_start, int64_t reference_end, int64_t query_start,
+                              int64_t query_end, int32_t highest, int64_t *end_row, int64_t *end_column) {
     const int64_t rs = reference_start < rows ? reference_start : rows;
     const int64_t re = reference_end < rows ? reference_end : rows;
     const int64_t qs = query_start < columns ? query_start : columns;
     const int64_t qe = query_end < columns ? query_end : columns;
-    if (rows == 0 && columns == 0) return 0;
-    if (columns == 0) return free_edge(rows - re, rs, open, extend);
-    if (rows == 0) return free_edge(columns - qe, qs, open, extend);
+    if (rows == 0 || columns == 0) {
+        /* scored.mojo:155-176: along the other's edge, every end within its free letters at the end in
+         * turn; of equal ones the later when the run goes along the reference and `highest` is asked (or
+         * along the query and it is not), else the earlier. */
+        const int64_t length = rows + columns;
+        const int along_reference = rows > 0;
+        const int64_t start = along_reference ? rs : qs, finish = along_reference ? re : qe;
+        int32_t top = INT32_MIN;
+        int64_t reach = 0;
+        for (int64_t letters = 0; letters <= length; ++letters) {
+            if (length - letters > finish) continue;
+            const int32_t value = free_edge(letters, start, open, extend);
+            if (value > top || (value == top && along_reference == (highest != 0))) {
+                top = value;
+                reach = letters;
+            }
+        }
+        *end_row = rows > 0 ? reach : 0;
+        *end_column = columns > 0 ? reach : 0;
+        return length == 0 ? 0 : top;
+    }
     const int32_t opening = open + extend;
     const int64_t stride = columns + 1;
     int32_t *s = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
@@ -184,9 +216,11 @@ int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_
         d[c] = border + opening;
         i[c] = 0;
     }
-    /* The last column's ends: row 0 among them when every reference letter may be left at the end. */
     int32_t best = INT32_MIN;
-    if (rows <= re) best = s[columns];
+    *end_row = 0;
+    *end_column = 0;
+    /* The last column's ends: row 0 among them when every reference letter may be left at the end. */
+    if (rows <= re) offer_end(s[columns], 0, columns, highest, &best, end_row, end_column);
     for (int64_t r = 1; r <= rows; ++r) {
         int32_t *ps = s + ((r - 1) & 1) * stride, *pd = d + ((r - 1) & 1) * stride;
         int32_t *cs = s + (r & 1) * stride, *cd = d + (r & 1) * stride, *ci = i + (r & 1) * stride;
@@ -202,16 +236,24 @@ int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_
             cd[c] = del;
             ci[c] = ins;
         }
-        if (rows - r <= re && cs[columns] > best) best = cs[columns];
+        if (rows - r <= re) offer_end(cs[columns], r, columns, highest, &best, end_row, end_column);
     }
     /* The last row's ends, column 0 among them when every query letter may be left at the end. */
     const int32_t *last = s + (rows & 1) * stride;
-    for (int64_t c = columns - qe; c <= columns; ++c)
-        if (last[c] > best) best = last[c];
+    for (int64_t c = columns - qe; c <= columns; ++c) offer_end(last[c], rows, c, highest, &best, end_row, end_column);
     free(s);
     free(d);
     free(i);
     return best;
+}
+
+int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                                const int8_t *table, int32_t size, int32_t open, int32_t extend,
+                                int64_t reference_start, int64_t reference_end, int64_t query_start,
+                                int64_t query_end) {
+    int64_t row = 0, column = 0;
+    return oracle_gotoh_end_free(first, rows, second, columns, table, size, open, extend, reference_start,
+                                 reference_end, query_start, query_end, 1, &row, &column);
 }
 
 /* Decision, gotoh.mojo:130-170: low two bits the source (0 aligning, 1 deleting, 2 inserting, 3 a

@@ -33,6 +33,13 @@ int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_
                                 const int8_t *table, int32_t size, int32_t open, int32_t extend,
                                 int64_t reference_start, int64_t reference_end, int64_t query_start,
                                 int64_t query_end);
+/* The same score and where it ends (*end_row reference letters, *end_column query letters): of equal best
+ * ends the one furthest along the reference less the query with `highest`, the least so without
+ * (scored.mojo:69-100, 155-176). */
+int32_t oracle_gotoh_end_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                              const int8_t *table, int32_t size, int32_t open, int32_t extend,
+                              int64_t reference_start, int64_t reference_end, int64_t query_start,
+                              int64_t query_end, int32_t highest, int64_t *end_row, int64_t *end_column);
 int32_t oracle_gotoh_score(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                            const int8_t *table, int32_t size, int32_t open, int32_t extend, int32_t mode,
                            int64_t *end_row, int64_t *end_column);

@@ -48,6 +48,9 @@ def lib() -> ctypes.CDLL:
         handle.oracle_gotoh_score.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, i64p, i64p]
         handle.oracle_gotoh_score_free.restype = i32
         handle.oracle_gotoh_score_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64]
+        handle.oracle_gotoh_end_free.restype = i32
+        handle.oracle_gotoh_end_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64, i32,
+                                                 ctypes.POINTER(i64), ctypes.POINTER(i64)]
         handle.oracle_gotoh_align.restype = i32
         handle.oracle_gotoh_align.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, u8p, u8p, i64p]
         handle.oracle_cigar.restype = i64
@@ -128,6 +131,44 @@ def gotoh_score_free(a, b, table, size, open_, extend, reference_start=0, refere
     return int(lib().oracle_gotoh_score_free(pa, len(first), pb, len(second), pt, size, open_, extend,
                                              min(reference_start, big), min(reference_end, big),
                                              min(query_start, big), min(query_end, big)))
+
+
+def gotoh_end_free(a, b, table, size, open_, extend, reference_start=0, reference_end=0, query_start=0,
+                   query_end=0, highest=True) -> tuple:
+    """(score, end_row, end_column) with free ends: the best end, of equal ones the furthest along the
+    reference less the query (`highest`) or the least so (scored.mojo:69-100, 155-176)."""
+    first, pa = _u8(a)
+    second, pb = _u8(b)
+    t, pt = _i8(table)
+    big = (1 << 62)
+    row, column = ctypes.c_int64(), ctypes.c_int64()
+    score = lib().oracle_gotoh_end_free(pa, len(first), pb, len(second), pt, size, open_, extend,
+                                        min(reference_start, big), min(reference_end, big), min(query_start, big),
+                                        min(query_end, big), 1 if highest else 0, ctypes.byref(row),
+                                        ctypes.byref(column))
+    return int(score), row.value, column.value
+
+
+def free_ends_alignment(a, b, table, size, open_, extend, reference_start=0, reference_end=0, query_start=0,
+                        query_end=0, eqx=True) -> tuple:
+    """(score, cigar, (reference start, reference end, query start, query end)) of a pair in codes with free
+    ends under a Scoring, as the reference's host path places and aligns it (scoring.mojo:690-722 mode_span,
+    scored.mojo:616-633 started_span, scoring.mojo:800-813): the best end, of equal ones the furthest along
+    the reference less the query; the start by a sweep back over both prefixes to it, reversed, the letters
+    free at the start free at its end, taking its end the least so; and the letters between them aligned
+    globally by the full-matrix walk."""
+    a = np.asarray(a, dtype=np.uint8)
+    b = np.asarray(b, dtype=np.uint8)
+    rs, re_ = min(reference_start, len(a)), min(reference_end, len(a))
+    qs, qe = min(query_start, len(b)), min(query_end, len(b))
+    score, end_row, end_column = gotoh_end_free(a, b, table, size, open_, extend, rs, re_, qs, qe, True)
+    back, row, column = gotoh_end_free(a[:end_row][::-1].copy(), b[:end_column][::-1].copy(), table, size, open_,
+                                       extend, 0, rs, 0, qs, False)
+    start_row, start_column = end_row - row, end_column - column
+    inner, cigar = gotoh_align(a[start_row:end_row], b[start_column:end_column], table, size, open_, extend,
+                               GLOBAL, eqx)[:2]
+    assert back == score == inner, (score, back, inner)
+    return score, cigar, (start_row, end_row, start_column, end_column)
 
 
 def gotoh_align(first, second, table, size, open_, extend, mode=GLOBAL, eqx=True) -> tuple:

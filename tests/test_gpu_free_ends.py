@@ -1,7 +1,7 @@
-"""Global scores with free ends on the GPU against the oracle (the reference's host path for a Scoring's
-free ends, scored.mojo:69-240; its GPU refuses them): the reference's literal, every preset its tests name
-(tests/test_alignment.mojo:2938-2943) on reads cut from and mutated off their references, empty sides,
-pairs wider than one strip, and the refusals that stand."""
+"""Scores and alignments with free ends on the GPU against the oracle (the reference's host path for a
+Scoring's free ends, scored.mojo:69-240 and scoring.mojo:690-813; its GPU refuses them): the reference's
+literal, every preset its tests name (tests/test_alignment.mojo:2938-2943) on reads cut from and mutated
+off their references, empty sides, pairs wider than one strip, and the refusals that stand."""
 
 import numpy as np
 import pytest
@@ -44,8 +44,12 @@ def _reads(rng, count, longest):
 
 
 def test_reference_literal(da):
-    """tests/test_python.py:103-104: the read placed inside its window by Mode.INFIX scores 16."""
+    """tests/test_python.py:103-104: the read placed inside its window by Mode.INFIX scores 16, at the
+    reference's fifth letter, with the CIGAR 8=."""
     assert da.score("TTTTACGTACGTTTTT", "ACGTACGT", da.Scoring.dna(), da.Mode.INFIX) == 16
+    placed = da.align("TTTTACGTACGTTTTT", "ACGTACGT", da.Scoring.dna(), da.Mode.INFIX)
+    assert (placed.score, placed.reference_start, placed.cigar) == (16, 4, "8=")
+    assert (placed.reference_end, placed.query_start, placed.query_end) == (12, 0, 8)
     assert da.scores(["TTTTACGTACGTTTTT"], ["ACGTACGT"], da.Scoring.dna(), da.Mode.PREFIX) == \
         [da.score("TTTTACGTACGTTTTT", "ACGTACGT", da.Scoring.dna(), da.Mode.PREFIX)]
 
@@ -75,9 +79,51 @@ def test_long_pairs_and_random_counts(da, oracle):
         assert da.scores(refs, queries, scoring, mode) == _expected(oracle, scoring, refs, queries, mode)
 
 
+def _expected_alignments(oracle, scoring, refs, queries, mode):
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    size = len(scoring.alphabet)
+    counts = [min(mode.reference_start, BIG), min(mode.reference_end, BIG), min(mode.query_start, BIG),
+              min(mode.query_end, BIG)]
+    return [oracle.free_ends_alignment(oracle.codes(r, scoring.alphabet), oracle.codes(q, scoring.alphabet), table,
+                                       size, op, ex, *counts) for r, q in zip(refs, queries)]
+
+
+@pytest.mark.parametrize("mode_name", ["INFIX", "PREFIX", "SUFFIX", "query_both", "few", "overlap"])
+def test_alignments_against_the_oracle(da, oracle, mode_name):
+    """Each preset's alignments: the score, the span as the reference places it (the best end furthest
+    along the reference less the query, the start found back from it) and the span's global CIGAR, under
+    two tables, on reads, unrelated pairs, repeats and empty sides, next to pairs past one strip."""
+    modes = {"INFIX": da.Mode.INFIX, "PREFIX": da.Mode.PREFIX, "SUFFIX": da.Mode.SUFFIX,
+             "query_both": da.Mode.ends_free(query_start=BIG, query_end=BIG),
+             "few": da.Mode.ends_free(reference_start=8, reference_end=8, query_start=3, query_end=3),
+             "overlap": da.Mode.ends_free(reference_end=40, query_start=40)}
+    mode = modes[mode_name]
+    rng = np.random.default_rng(sum(map(ord, mode_name)) + 1)
+    refs, queries = _reads(rng, 160, 300)
+    refs += ["ACACACACACACACAC", "", "ACGT", "", "AAAAAAAA"]
+    queries += ["ACAC", "ACG", "", "", "AAAA"]
+    long_refs, long_queries = _reads(rng, 6, 1400)
+    refs += long_refs
+    queries += long_queries
+    tabulated = da.Scoring.tabulated("ACGT", [5, -1, -2, -1, -1, 5, -3, -2, -2, -3, 5, -1, -1, -2, -1, 5], -6, -1)
+    for scoring in (da.Scoring.dna(), tabulated):
+        found = da.alignments(refs, queries, scoring, mode)
+        expected = _expected_alignments(oracle, scoring, refs, queries, mode)
+        for k, (alignment, (score, cigar, span)) in enumerate(zip(found, expected)):
+            got = (alignment.score, alignment.cigar, (alignment.reference_start, alignment.reference_end,
+                                                      alignment.query_start, alignment.query_end))
+            assert got == (score, cigar, span), (k, refs[k], queries[k])
+
+
 def test_free_ends_refused_where_the_gpu_does_not_serve_them(da):
-    """Alignments (CIGARs) with free ends stay refused on the GPU, as are negative counts."""
+    """Extensions stay refused on the GPU, as are negative counts and a match score of the mode's own
+    beside the table's."""
     with pytest.raises(ValueError):
-        da.alignments_tape(da.Tape.of(["ACGT"], ["ACG"]), da.Scoring.dna(), da.Mode.INFIX)
+        da.alignments_tape(da.Tape.of(["ACGT"], ["ACG"]), da.Scoring.dna(), da.Mode.extension(1))
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.ends_free(reference_start=-1))
+    with pytest.raises(ValueError):
+        da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.ends_free(reference_start=-1))
+    with pytest.raises(ValueError):
+        da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.INFIX.with_match_score(2))

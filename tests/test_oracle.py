@@ -416,3 +416,68 @@ def test_free_ends_against_trimmed_global_alignments(oracle):
             counts = presets[trial % len(presets)] if trial < 36 else tuple(int(x) for x in rng.integers(0, 6, size=4))
             got = oracle.gotoh_score_free(a, b, table, 4, op, ex, *counts)
             assert got == _trimmed_best(oracle, a, b, table, op, ex, *counts), (a, b, counts)
+
+
+def test_free_end_alignment_known_answer(oracle):
+    """The reference's literal (tests/test_python.py:103-104): Mode.INFIX under Scoring.dna() places the
+    query at the reference's fifth letter, scoring 16 with the CIGAR 8=."""
+    table = oracle.dna_table(2, -4)
+    op, ex = oracle.kernel_gaps(-4, -2)
+    unbounded = 1 << 40
+    score, cigar, span = oracle.free_ends_alignment(oracle.codes("TTTTACGTACGTTTTT"), oracle.codes("ACGTACGT"),
+                                                    table, 4, op, ex, unbounded, unbounded, 0, 0)
+    assert (score, span[0], cigar) == (16, 4, "8=")
+    assert span == (4, 12, 0, 8)
+
+
+def _placed_by_brute_force(oracle, a, b, table, op, ex, rs, re, qs, qe):
+    """The score and span free ends give, by brute force: every allowed start (on the first column within
+    `rs` reference letters, or on the first row within `qs` query letters) against every allowed end (on
+    the last column within `re` letters of the last row, or on the last row within `qe` of the last
+    column), each scored by the global alignment between them. The end is the best, of equal ones the
+    furthest along the reference less the query; the start, of those reaching it at that score, the same."""
+    n, m = len(a), len(b)
+    rs, re, qs, qe = min(rs, n), min(re, n), min(qs, m), min(qe, m)
+    starts = [(r, 0) for r in range(rs + 1)] + [(0, c) for c in range(1, qs + 1)]
+    ends = [(n - r, m) for r in range(re + 1)] + [(n, m - c) for c in range(1, qe + 1)]
+
+    def between(start, end):
+        if start[0] > end[0] or start[1] > end[1]:
+            return None
+        return oracle.gotoh_score(a[start[0]:end[0]], b[start[1]:end[1]], table, 4, op, ex)[0]
+
+    best, best_end = None, None
+    for end in ends:
+        values = [v for v in (between(start, end) for start in starts) if v is not None]
+        if not values:
+            continue
+        value = max(values)
+        if best is None or value > best or (value == best and end[0] - end[1] > best_end[0] - best_end[1]):
+            best, best_end = value, end
+    start = max((s for s in starts if between(s, best_end) == best), key=lambda s: s[0] - s[1])
+    return best, (start[0], best_end[0], start[1], best_end[1])
+
+
+def test_free_end_alignments_by_brute_force(oracle):
+    """The oracle's free-end alignment against a brute force over every allowed start and end, for the
+    presets and random counts of the score test, on short pairs, repeats and empty sides, under two tables:
+    the same score and span, and the span's letters aligned globally scoring it."""
+    rng = np.random.default_rng(73)
+    big = 1 << 40
+    presets = [(big, big, 0, 0), (0, big, 0, 0), (big, 0, 0, 0), (0, 0, big, big), (8, 8, 3, 3), (0, 40, 40, 0)]
+    for match, mismatch, opening, extension in ((2, -4, -4, -2), (1, -3, -5, -1)):
+        table = oracle.dna_table(match, mismatch)
+        op, ex = oracle.kernel_gaps(opening, extension)
+        for trial in range(60):
+            n, m = int(rng.integers(0, 12)), int(rng.integers(0, 10))
+            if trial % 4 == 3:
+                a = np.tile(rng.integers(0, 4, size=2).astype(np.uint8), 6)[:n]  # repeats: many equal ends
+            else:
+                a = rng.integers(0, 4, size=n).astype(np.uint8)
+            b = a[: m].copy() if trial % 3 else rng.integers(0, 4, size=m).astype(np.uint8)
+            b = b[rng.random(len(b)) > 0.1]
+            counts = presets[trial % len(presets)] if trial < 36 else tuple(int(x) for x in rng.integers(0, 6, size=4))
+            score, cigar, span = oracle.free_ends_alignment(a, b, table, 4, op, ex, *counts)
+            assert (score, span) == _placed_by_brute_force(oracle, a, b, table, op, ex, *counts), (a, b, counts)
+            inner = oracle.gotoh_align(a[span[0]:span[1]], b[span[2]:span[3]], table, 4, op, ex)
+            assert (inner[0], inner[1]) == (score, cigar)
