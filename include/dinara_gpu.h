@@ -34,7 +34,8 @@ extern "C" {
 #define DINARA_DEVICE_FAILURE (-8)      /* a CUDA call failed; dinara_gpu_error() says which */
 #define DINARA_DEVICE_TIMEOUT (-9)      /* a bounded wait (device flag or host wait) ran out */
 
-/* dinara_mode kinds (c/dinara.h:69-76); the GPU serves ENDS_FREE with no free ends (global) and LOCAL. */
+/* dinara_mode kinds (c/dinara.h:69-76); under a Scoring the GPU serves ENDS_FREE (global, or with free
+ * letters at the ends) and LOCAL. */
 #define DINARA_ENDS_FREE 0
 #define DINARA_EXTENSION 1
 #define DINARA_LOCAL 2
@@ -106,8 +107,12 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
                                int64_t *statuses);
 
 /*
- * Alignments under a Scoring, global or local (free ends refused, DINARA_INVALID_MODE), the CIGAR
- * Gotoh's walk picks among equals (replaces
+ * Alignments under a Scoring, global, local, or with free ends (a DINARA_ENDS_FREE mode with letter
+ * counts, as dinara_gpu_scores takes it), the CIGAR Gotoh's walk picks among equals. Free ends are placed
+ * as the reference's host path places them (scoring.mojo:690-813): the best end, of equal ones the
+ * furthest along the reference less the query, the start found by a sweep back from it, and the
+ * letters between aligned globally; a pair whose span's global score differs from its free-end score
+ * reports DINARA_DEVICE_FAILURE in its status. (Replaces
  * api.mojo:895-1006 `alignments` on the GPU -> scoring.mojo:1436-1478 `device_batch_alignments` ->
  * device_align.mojo:278-441 `batch_kernel[record]`, and the reference's c/dinara.h:225-228 batch
  * shape). Each alignment's CIGAR is allocated here and freed with dinara_free; its spans are placed
