@@ -828,13 +828,39 @@ __global__ void free_spans_kernel(const int64_t *__restrict__ ends, const int64_
     span[3] = end_column;
 }
 
+// Each pair's whole extent (rows << 32 | columns), for an extension swept from the ends.
+__global__ void extents_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count,
+                               int64_t *__restrict__ extents) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const PairShape sh = shapes[first + k];
+    extents[k] = (int64_t(sh.rows) << 32) | int64_t(sh.columns);
+}
+
+// An extension's span from its stop: from the origin to the stop, or (swept from the ends) from the stop,
+// counted back from the ends, to the ends.
+__global__ void extension_spans_kernel(const PairShape *__restrict__ shapes, int64_t first, const int64_t *__restrict__ stops,
+                                       int64_t count, bool from_end, int64_t *__restrict__ spans) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const PairShape sh = shapes[first + k];
+    const int64_t row = stops[k] >> 32, column = stops[k] & 0xffffffff;
+    int64_t *span = spans + 4 * k;
+    span[0] = from_end ? int64_t(sh.rows) - row : 0;
+    span[1] = from_end ? int64_t(sh.rows) : row;
+    span[2] = from_end ? int64_t(sh.columns) - column : 0;
+    span[3] = from_end ? int64_t(sh.columns) : column;
+}
+
 // Global scores with free ends: every pair over its whole matrix in 32 bits, one shape (32 lanes of 16
 // columns, strips of 512) with the table in shared memory, the free-end form of the sweep. With `spans`
 // (4 a pair of the range, by pair - first), each pair's span as the reference places it
 // (scoring.mojo:690-722 mode_span, scored.mojo:616-633 started_span): its end, of equal best ends the one
 // furthest along the reference less the query; then a sweep back over both prefixes to that end, read
 // backwards, with the letters free at the start free at its end, whose best end nearest the other way
-// (the least along the reference less the query, reversed) is the start.
+// (the least along the reference less the query, reversed) is the start. An extension (batch.extension)
+// takes one launch of the same form with no letters free and every cell a candidate stop (ORIGIN), from
+// the origin or, read backwards, from the ends; its span runs from its anchor to the stop.
 void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
                      int64_t first, int64_t count, int64_t *spans) {
     const Schedule order = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, false, PairLimits());
@@ -855,13 +881,28 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     args.free_query_start = batch.free_query_start;
     args.free_query_end = batch.free_query_end;
     int64_t *ends = nullptr;
-    if (spans) {
+    if (spans || batch.extension) {
         ends = gpu->free_spans.ensure<int64_t>(2 * size_t(count));
         args.free_ends_out = ends;
         args.free_highest = 1;
     }
     KernelFn fn = batch.bits == 8 ? static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 8, true, true>)
                                   : static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 2, true, true>);
+    if (batch.extension) {
+        // An extension's stop: the free-end form with no letters free, every cell a candidate; from the
+        // ends, each pair whole and read backwards.
+        fn = batch.bits == 8 ? static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 8, true, true, false, true>)
+                             : static_cast<KernelFn>(&affine_kernel<32, 16, false, false, 2, true, true, false, true>);
+        args.free_reference_start = args.free_reference_end = args.free_query_start = args.free_query_end = 0;
+        if (batch.from_end) {
+            int64_t *extents = ends + count;
+            extents_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(batch.shapes, first, count,
+                                                                                 extents);
+            DINARA_CUDA(cudaGetLastError());
+            gpu->launches += 1;
+            args.extents = extents;
+        }
+    }
     int64_t total = 0;
     for (int cls = 0; cls < kClasses; ++cls) total += order.counts[cls];
     int64_t blocks = persistent_blocks(gpu, fn);
@@ -878,7 +919,14 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     DINARA_CUDA(cudaGetLastError());
     clock.stop();
     gpu->launches += 1;
-    if (spans) {
+    if (batch.extension) {
+        if (spans) {
+            extension_spans_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(
+                batch.shapes, first, ends, count, batch.from_end, spans);
+            DINARA_CUDA(cudaGetLastError());
+            gpu->launches += 1;
+        }
+    } else if (spans) {
         // The sweep back: each pair's prefixes to its end, backwards, the start's free letters free at the
         // (backward) end and none at its start; its scores, the same, go to scratch.
         KernelArgs back = args;

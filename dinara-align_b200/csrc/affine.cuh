@@ -52,6 +52,10 @@ struct AffineBatch {
     // its own length). `free_ends` is set when any is nonzero.
     bool free_ends = false;
     int32_t free_reference_start = 0, free_reference_end = 0, free_query_start = 0, free_query_end = 0;
+    // An extension's stop (scoring.mojo:673-688 extension_span): from the origin, or with `from_end` from
+    // both sequences' ends (read backwards), to the best cell anywhere; `free_ends` is then set too, with no
+    // letters free.
+    bool extension = false, from_end = false;
 };
 
 // The flag value a failed walk leaves (1 is a letter outside the alphabet).

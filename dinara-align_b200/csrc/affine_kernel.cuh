@@ -140,11 +140,18 @@ __device__ __forceinline__ int32_t free_edge(int letters, int free, int32_t open
 // decision's terms are the whole matrix's (a term an optimal path reaches equals it; one no optimal path
 // reaches is below the cell's value either way), and the walk takes the whole matrix's CIGAR. Decisions
 // are kept strip by strip for the swept rows only (band_strip_pad words a lane).
-template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE, bool FREE = false, bool BANDED = false>
+//
+// With ORIGIN (and FREE with no free letters: a global sweep from the origin) the result is an extension's
+// stop (scored.mojo:69-100 and 272-300, FROM_ORIGIN): the best cell anywhere above zero, of equal ones the
+// furthest along both sequences together, then along the reference; none above zero stops at the origin,
+// scoring 0.
+template <int G, int C, bool LOCAL, bool RECORD, int BITS, bool SMEM_TABLE, bool FREE = false, bool BANDED = false,
+          bool ORIGIN = false>
 __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs t, const int32_t *__restrict__ table32) {
     static_assert(!FREE || (!LOCAL && !RECORD), "free ends are for global scores");
     static_assert(!BANDED || (!LOCAL && RECORD && !FREE && G == 32 && G * C == kRecordStrip),
                   "a band-recorded pair is global, recorded, and swept in strips of kRecordStrip columns");
+    static_assert(!ORIGIN || FREE, "an extension's stop is found by the free-end form");
     constexpr int32_t kOut = -(1 << 28);  // unreached: below every score ScoreReach lets a pair hold
     constexpr int W = G * C;
     constexpr int GPW = 32 / G;
@@ -198,12 +205,23 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
         int free_key = 0;      // the best end's rows less columns
         int64_t free_at = 0;   // and its place, row << 32 | column
         const bool highest = FREE && p.free_highest != 0;
-        // An end of `value` at (r, c) against the best so far: higher, or as high on the favoured side.
+        if (ORIGIN) free_best = 0;  // an extension's stop beats the origin's 0 only above it
+        // An end of `value` at (r, c) against the best so far: higher, or as high on the favoured side
+        // (ORIGIN: above zero, and as high further along both, then along the reference).
         auto offer = [&](int32_t value, int r, int c) {
-            const int key = r - c;
-            if (value > free_best || (value == free_best && (highest ? key > free_key : key < free_key))) {
+            bool better;
+            if (ORIGIN) {
+                const int along = r + c, best_along = int(free_at >> 32) + int(free_at & 0xffffffff);
+                better = value > 0 && (value > free_best ||
+                                       (value == free_best && (along > best_along ||
+                                                               (along == best_along && r > int(free_at >> 32)))));
+            } else {
+                const int key = r - c;
+                better = value > free_best || (value == free_best && (highest ? key > free_key : key < free_key));
+            }
+            if (better) {
                 free_best = value;
-                free_key = key;
+                free_key = r - c;
                 free_at = (int64_t(r) << 32) | int64_t(c);
             }
         };
@@ -374,7 +392,12 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                     reported = (reported & ~hit) | (H[k] & hit);
                                 }
                             }
-                            if (FREE) {
+                            if (ORIGIN) {
+                                // An extension may stop at any cell, as a true score.
+#pragma unroll
+                                for (int k = 0; k < C; ++k)
+                                    if (k < owned) offer(H[k] + (row + first_col + k + 1) * extend, row, first_col + k + 1);
+                            } else if (FREE) {
                                 // Ends on the last row within free_qe letters of the last column, and on the
                                 // last column within free_re letters of the last row, as true scores.
                                 if (row == rows) {
@@ -455,7 +478,9 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                 offer(their_value, int(their_at >> 32), int(their_at & 0xffffffff));
             }
             if (live && member == 0) {
-                if (!work) {
+                if (ORIGIN) {
+                    // An extension's stop: the group's best above zero, or the origin.
+                } else if (!work) {
                     if (rows == 0 && cols == 0) {
                         free_best = 0;
                         free_at = 0;

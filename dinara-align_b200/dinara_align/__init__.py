@@ -139,9 +139,9 @@ class Anchor:
 @dataclass(frozen=True)
 class Mode:
     """Which alignments count (the reference's `Mode`, fields in `dinara_mode` order). The GPU serves
-    `Mode.GLOBAL` and, under a `Scoring`, `Mode.local()` and free ends: `INFIX`, `PREFIX`, `SUFFIX` and
-    `ends_free(...)` (with no match score of the mode's own), scores and alignments, the latter placed as
-    the reference's host path places them."""
+    `Mode.GLOBAL` and, under a `Scoring`, `Mode.local()`, free ends (`INFIX`, `PREFIX`, `SUFFIX` and
+    `ends_free(...)`) and `extension(0, ...)` (no match score of the mode's own), scores and alignments,
+    the latter placed as the reference's host path places them."""
 
     kind: int = _ENDS
     reference_start: int = 0
@@ -168,7 +168,8 @@ class Mode:
     @staticmethod
     def extension(match_score: int, anchor: int = Anchor.START, *, zdrop: int = -1, end_bonus: int = -1) -> "Mode":
         """A seed's extension from both starts (or `anchor` END, both ends), a match earning
-        `match_score`; the GPU path refuses it."""
+        `match_score`. Under a `Scoring` (match score 0: the table's own) the GPU serves it, scores and
+        alignments, with an end bonus; a Z-drop that could stop the sweep it refuses."""
         return Mode(_EXTENSION, match_score=match_score, anchor=anchor, zdrop=zdrop, end_bonus=end_bonus)
 
     @staticmethod

@@ -247,6 +247,56 @@ int32_t oracle_gotoh_end_free(const uint8_t *first, int64_t rows, const uint8_t 
     return best;
 }
 
+/* An extension's stop, scored.mojo:69-100 and 272-300 (FROM_ORIGIN): Gotoh's global recurrence from the
+ * origin, its stop the best cell anywhere above zero, of equal ones the furthest along both sequences
+ * together, then along the reference; none above zero stops at the origin, scoring 0. */
+int32_t oracle_gotoh_extension(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                               const int8_t *table, int32_t size, int32_t open, int32_t extend, int64_t *end_row,
+                               int64_t *end_column) {
+    int32_t best = 0;
+    *end_row = 0;
+    *end_column = 0;
+    if (rows == 0 || columns == 0) return 0;
+    const int32_t opening = open + extend;
+    const int64_t stride = columns + 1;
+    int32_t *s = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *d = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *i = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    for (int64_t c = 0; c <= columns; ++c) {
+        const int32_t border = c == 0 ? 0 : gap_run(open, extend, c);
+        s[c] = border;
+        d[c] = border + opening;
+        i[c] = 0;
+    }
+    for (int64_t r = 1; r <= rows; ++r) {
+        int32_t *ps = s + ((r - 1) & 1) * stride, *pd = d + ((r - 1) & 1) * stride;
+        int32_t *cs = s + (r & 1) * stride, *cd = d + (r & 1) * stride, *ci = i + (r & 1) * stride;
+        const int32_t border = gap_run(open, extend, r);
+        cs[0] = border;
+        cd[0] = border;
+        ci[0] = border + opening;
+        const int8_t *table_row = table + (int64_t)first[r - 1] * size;
+        for (int64_t c = 1; c <= columns; ++c) {
+            int32_t del = max32(ps[c] + open, pd[c] + extend);
+            int32_t ins = max32(cs[c - 1] + open, ci[c - 1] + extend);
+            cs[c] = max32(ps[c - 1] + table_row[second[c - 1]], max32(del, ins));
+            cd[c] = del;
+            ci[c] = ins;
+            const int64_t along = r + c, best_along = *end_row + *end_column;
+            if (cs[c] > 0 && (cs[c] > best || (cs[c] == best && (along > best_along ||
+                                                                  (along == best_along && r > *end_row))))) {
+                best = cs[c];
+                *end_row = r;
+                *end_column = c;
+            }
+        }
+    }
+    free(s);
+    free(d);
+    free(i);
+    return best;
+}
+
 int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                                 const int8_t *table, int32_t size, int32_t open, int32_t extend,
                                 int64_t reference_start, int64_t reference_end, int64_t query_start,

@@ -40,6 +40,12 @@ int32_t oracle_gotoh_end_free(const uint8_t *first, int64_t rows, const uint8_t 
                               const int8_t *table, int32_t size, int32_t open, int32_t extend,
                               int64_t reference_start, int64_t reference_end, int64_t query_start,
                               int64_t query_end, int32_t highest, int64_t *end_row, int64_t *end_column);
+/* An extension's best score from the origin and where it stops (scored.mojo:69-100, 272-300 FROM_ORIGIN):
+ * the best cell above zero, of equal ones the furthest along both together, then along the reference;
+ * (0, 0) scoring 0 when none is above zero. */
+int32_t oracle_gotoh_extension(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                               const int8_t *table, int32_t size, int32_t open, int32_t extend, int64_t *end_row,
+                               int64_t *end_column);
 int32_t oracle_gotoh_score(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                            const int8_t *table, int32_t size, int32_t open, int32_t extend, int32_t mode,
                            int64_t *end_row, int64_t *end_column);

@@ -48,6 +48,9 @@ def lib() -> ctypes.CDLL:
         handle.oracle_gotoh_score.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, i64p, i64p]
         handle.oracle_gotoh_score_free.restype = i32
         handle.oracle_gotoh_score_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64]
+        handle.oracle_gotoh_extension.restype = i32
+        handle.oracle_gotoh_extension.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, ctypes.POINTER(i64),
+                                                  ctypes.POINTER(i64)]
         handle.oracle_gotoh_end_free.restype = i32
         handle.oracle_gotoh_end_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64, i32,
                                                  ctypes.POINTER(i64), ctypes.POINTER(i64)]
@@ -169,6 +172,43 @@ def free_ends_alignment(a, b, table, size, open_, extend, reference_start=0, ref
                                GLOBAL, eqx)[:2]
     assert back == score == inner, (score, back, inner)
     return score, cigar, (start_row, end_row, start_column, end_column)
+
+
+def gotoh_extension(a, b, table, size, open_, extend) -> tuple:
+    """(score, stop_row, stop_column) of an extension from the origin (scored.mojo:69-100, 272-300)."""
+    first, pa = _u8(a)
+    second, pb = _u8(b)
+    t, pt = _i8(table)
+    row, column = ctypes.c_int64(), ctypes.c_int64()
+    score = lib().oracle_gotoh_extension(pa, len(first), pb, len(second), pt, size, open_, extend, ctypes.byref(row),
+                                         ctypes.byref(column))
+    return int(score), row.value, column.value
+
+
+def extension_alignment(a, b, table, size, open_, extend, from_end=False, end_bonus=-1, eqx=True) -> tuple:
+    """(score, cigar, (reference start, reference end, query start, query end)) of an extension under a
+    Scoring with no Z-drop, as the reference's host path makes it (scoring.mojo:673-722 extension_span and
+    mode_span, 800-813): the best stop from the starts, or from the ends over both sequences reversed; with
+    an end bonus, the alignment reaching the query's far end (free ends: the reference's far end free) when
+    its score plus the bonus passes the stop's; then the span's letters aligned globally."""
+    a = np.asarray(a, dtype=np.uint8)
+    b = np.asarray(b, dtype=np.uint8)
+    n, m = len(a), len(b)
+    if from_end:
+        score, row, column = gotoh_extension(a[::-1].copy(), b[::-1].copy(), table, size, open_, extend)
+        span = (n - row, n, m - column, m)
+    else:
+        score, row, column = gotoh_extension(a, b, table, size, open_, extend)
+        span = (0, row, 0, column)
+    if end_bonus > 0:
+        big = 1 << 62
+        counts = (big, 0, 0, 0) if from_end else (0, big, 0, 0)
+        reach, _cigar, reach_span = free_ends_alignment(a, b, table, size, open_, extend, *counts, eqx=eqx)
+        if reach + end_bonus > score:
+            score, span = reach, reach_span
+    inner, cigar = gotoh_align(a[span[0]:span[1]], b[span[2]:span[3]], table, size, open_, extend, GLOBAL, eqx)[:2]
+    assert inner == score, (inner, score)
+    return score, cigar, span
 
 
 def gotoh_align(first, second, table, size, open_, extend, mode=GLOBAL, eqx=True) -> tuple:

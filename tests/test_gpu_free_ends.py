@@ -117,13 +117,69 @@ def test_alignments_against_the_oracle(da, oracle, mode_name):
 
 
 def test_free_ends_refused_where_the_gpu_does_not_serve_them(da):
-    """Extensions stay refused on the GPU, as are negative counts and a match score of the mode's own
-    beside the table's."""
-    with pytest.raises(ValueError):
-        da.alignments_tape(da.Tape.of(["ACGT"], ["ACG"]), da.Scoring.dna(), da.Mode.extension(1))
+    """Negative counts stay refused, as does a match score of the mode's own beside the table's."""
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.ends_free(reference_start=-1))
     with pytest.raises(ValueError):
         da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.ends_free(reference_start=-1))
     with pytest.raises(ValueError):
         da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.INFIX.with_match_score(2))
+
+
+def _expected_extensions(oracle, scoring, refs, queries, from_end, bonus):
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    size = len(scoring.alphabet)
+    return [oracle.extension_alignment(oracle.codes(r, scoring.alphabet), oracle.codes(q, scoring.alphabet), table,
+                                       size, op, ex, from_end, bonus) for r, q in zip(refs, queries)]
+
+
+@pytest.mark.parametrize("anchor", ["start", "end"])
+def test_extensions_against_the_oracle(da, oracle, anchor):
+    """Extensions from both starts and from both ends (a seed's extension, scoring.mojo:673-722): with no end
+    bonus, a small one and one near 2^62, and a Z-drop too large ever to stop the sweep (the reference's own
+    check, tests/test_alignment.mojo:2576-2592), the scores, spans and CIGARs equal the oracle's under two
+    tables, on reads sharing their anchor with the reference, unrelated pairs, empty sides and pairs past
+    one strip; scores alone agree with the alignments'."""
+    from_end = anchor == "end"
+    rng = np.random.default_rng(97 + from_end)
+    refs, queries = [], []
+    for trial in range(150):
+        n = int(rng.integers(0, 400 if trial % 25 else 1500))
+        ref = "".join(rng.choice(list("ACGT"), size=n))
+        shared = int(rng.integers(0, n + 1))
+        piece = ref[n - shared:] if from_end else ref[:shared]
+        rate = (0.0, 0.03, 0.1)[trial % 3]
+        piece = "".join(ch if rng.random() >= rate else rng.choice(list("ACGT")) for ch in piece
+                        if rng.random() >= rate / 3)
+        tail = "".join(rng.choice(list("ACGT"), size=int(rng.integers(0, 60))))
+        query = "".join(rng.choice(list("ACGT"), size=int(rng.integers(0, 200)))) if trial % 7 == 0 else (
+            tail + piece if from_end else piece + tail)
+        refs.append(ref)
+        queries.append(query)
+    refs += ["", "ACGT", ""]
+    queries += ["ACG", "", ""]
+    anchor_value = da.Anchor.END if from_end else da.Anchor.START
+    tabulated = da.Scoring.tabulated("ACGT", [5, -1, -2, -1, -1, 5, -3, -2, -2, -3, 5, -1, -1, -2, -1, 5], -6, -1)
+    for scoring in (da.Scoring.dna(), tabulated):
+        for bonus in (-1, 12, 1 << 62):
+            for zdrop in (-1, 1 << 62):
+                mode = da.Mode.extension(0, anchor_value, zdrop=zdrop, end_bonus=bonus)
+                found = da.alignments(refs, queries, scoring, mode)
+                expected = _expected_extensions(oracle, scoring, refs, queries, from_end, bonus)
+                for k, (alignment, (score, cigar, span)) in enumerate(zip(found, expected)):
+                    got = (alignment.score, alignment.cigar, (alignment.reference_start, alignment.reference_end,
+                                                              alignment.query_start, alignment.query_end))
+                    assert got == (score, cigar, span), (k, refs[k], queries[k], bonus, zdrop)
+                assert da.scores(refs, queries, scoring, mode) == [score for score, _c, _s in expected]
+
+
+def test_extension_refusals(da):
+    """A Z-drop that could stop the sweep needs whole anti-diagonals, which the GPU's row sweep does not
+    take in order, and an extension's match score beside the table's is the reference's own refusal."""
+    with pytest.raises(ValueError):
+        da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(0, zdrop=100))
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(0, zdrop=0))
+    with pytest.raises(ValueError):
+        da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(1))

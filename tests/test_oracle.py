@@ -481,3 +481,40 @@ def test_free_end_alignments_by_brute_force(oracle):
             assert (score, span) == _placed_by_brute_force(oracle, a, b, table, op, ex, *counts), (a, b, counts)
             inner = oracle.gotoh_align(a[span[0]:span[1]], b[span[2]:span[3]], table, 4, op, ex)
             assert (inner[0], inner[1]) == (score, cigar)
+
+
+def test_extensions_by_brute_force(oracle):
+    """An extension's stop against a brute force over every prefix pair, each scored by its global alignment:
+    the best above zero, of equal ones the furthest along both together, then along the reference, or the
+    origin; from the ends, the same over both sequences reversed. With an end bonus the alignment reaching
+    the query's far end wins when its score plus the bonus passes the stop's. The span's letters aligned
+    globally score what the extension does."""
+    rng = np.random.default_rng(79)
+    big = 1 << 40
+    for match, mismatch, opening, extension in ((2, -4, -4, -2), (1, -3, -5, -1)):
+        table = oracle.dna_table(match, mismatch)
+        op, ex = oracle.kernel_gaps(opening, extension)
+        for trial in range(50):
+            n, m = int(rng.integers(0, 12)), int(rng.integers(0, 12))
+            a = rng.integers(0, 4, size=n).astype(np.uint8)
+            if trial % 4 == 3:
+                a = np.tile(rng.integers(0, 4, size=2).astype(np.uint8), 6)[:n]
+            b = a[: m].copy() if trial % 3 else rng.integers(0, 4, size=m).astype(np.uint8)
+            b = b[rng.random(len(b)) > 0.1]
+            for from_end in (False, True):
+                x, y = (a[::-1].copy(), b[::-1].copy()) if from_end else (a, b)
+                best, stop = 0, (0, 0)
+                for r in range(1, len(x) + 1):
+                    for c in range(1, len(y) + 1):
+                        value = oracle.gotoh_score(x[:r], y[:c], table, 4, op, ex)[0]
+                        if value > 0 and (value > best or (value == best and (r + c > sum(stop) or (
+                                r + c == sum(stop) and r > stop[0])))):
+                            best, stop = value, (r, c)
+                span = (len(x) - stop[0], len(x), len(y) - stop[1], len(y)) if from_end else (0, stop[0], 0, stop[1])
+                score, cigar, got = oracle.extension_alignment(a, b, table, 4, op, ex, from_end)
+                assert (score, got) == (best, span), (a, b, from_end)
+                for bonus in (3, 50, 1 << 61):
+                    counts = (big, 0, 0, 0) if from_end else (0, big, 0, 0)
+                    reach, reach_cigar, reach_span = oracle.free_ends_alignment(a, b, table, 4, op, ex, *counts)
+                    want = (reach, reach_cigar, reach_span) if reach + bonus > best else (best, cigar, span)
+                    assert oracle.extension_alignment(a, b, table, 4, op, ex, from_end, bonus) == want
