@@ -35,7 +35,8 @@ extern "C" {
 #define DINARA_DEVICE_TIMEOUT (-9)      /* a bounded wait (device flag or host wait) ran out */
 
 /* dinara_mode kinds (c/dinara.h:69-76); under a Scoring the GPU serves ENDS_FREE (global, or with free
- * letters at the ends) and LOCAL. */
+ * letters at the ends), EXTENSION (no match score of the mode's own; a Z-drop that could stop the sweep
+ * refused, DINARA_INVALID_MODE) and LOCAL. */
 #define DINARA_ENDS_FREE 0
 #define DINARA_EXTENSION 1
 #define DINARA_LOCAL 2
@@ -90,7 +91,8 @@ int64_t dinara_gpu_device_info(dinara_gpu *gpu, char *name, int64_t name_capacit
  * dinara_align/api.mojo:843-892 `scores` -> scoring.mojo:1294-1409 `device_batch_scores`), or global
  * with free ends: a DINARA_ENDS_FREE mode with letter counts at the reference's and the query's starts
  * and ends (INFIX, PREFIX, SUFFIX, ends_free; no match score of the mode's own), scored as the
- * reference's host path scores them (scored.mojo:69-240), which its GPU refuses.
+ * reference's host path scores them (scored.mojo:69-240), which its GPU refuses; or as an extension
+ * (DINARA_EXTENSION, match score 0, from either anchor, with an end bonus; scoring.mojo:673-722).
  * Pair i is references[i] (reference_lengths[i] bytes) against queries[i]. Writes scores[i] and
  * statuses[i] (0, or the pair's own code: -1 a letter outside the alphabet, -3 scores that could pass
  * 2^28 as ScoreReach refuses, scoring.mojo:218-249). Returns 0, or a code failing the whole batch
@@ -107,8 +109,10 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
                                int64_t *statuses);
 
 /*
- * Alignments under a Scoring, global, local, or with free ends (a DINARA_ENDS_FREE mode with letter
- * counts, as dinara_gpu_scores takes it), the CIGAR Gotoh's walk picks among equals. Free ends are placed
+ * Alignments under a Scoring, global, local, with free ends (a DINARA_ENDS_FREE mode with letter
+ * counts, as dinara_gpu_scores takes it) or as extensions, the CIGAR Gotoh's walk picks among equals.
+ * An extension's span runs from its anchor to its stop (or the end bonus's choice, scoring.mojo:673-722)
+ * and is aligned globally. Free ends are placed
  * as the reference's host path places them (scoring.mojo:690-813): the best end, of equal ones the
  * furthest along the reference less the query, the start found by a sweep back from it, and the
  * letters between aligned globally; a pair whose span's global score differs from its free-end score
