@@ -46,9 +46,11 @@ struct WalkArgs {
     const int32_t *widths;
     const int64_t *decision_offsets;
     const int64_t *ends;
-    const int64_t *slot_offsets;  // per pair: its CIGAR slot, 2 (rows + columns) + 1 bytes
+    const int64_t *slot_offsets;  // per pair: its CIGAR slot, a 32-bit run word a letter of the pair and 8 bytes
     char *slots;
     int64_t *lengths;             // per pair: the CIGAR's bytes
+    int64_t *run_counts;          // per pair: the CIGAR's runs, left in its slot back to front
+    const uint32_t *order;        // the pairs in the sweep's order, when given
     uint8_t *failed;              // per pair of the batch: set to kWalkFailed when a path leaves its band
     int64_t *spans;               // per pair: first row, last row, first column, last column
     int64_t first_pair, count;
@@ -56,29 +58,31 @@ struct WalkArgs {
     bool local, eqx, uniform;
 };
 
-__device__ __forceinline__ void emit_run(char *slot, int64_t &written, char op, int64_t count) {
-    // Written back to front: the op, then the count's digits from the last.
-    slot[written++] = op;
-    do {
-        slot[written++] = char('0' + count % 10);
-        count /= 10;
-    } while (count > 0);
+// A run of the CIGAR as the walk leaves it, one 32-bit word: the op in the top two bits (kRunD a letter
+// of the reference alone, kRunI of the query alone, kRunM an aligned pair (a match with eqx), kRunX a
+// mismatch with eqx) and its length in the low 30 (a pair's letters stay far below 2^30: ScoreReach).
+constexpr uint32_t kRunD = 0, kRunI = 1, kRunM = 2, kRunX = 3;
+constexpr uint32_t kRunLength = (1u << 30) - 1;
+
+__device__ __forceinline__ int decimal_digits(uint32_t n) {
+    return 1 + (n >= 10u) + (n >= 100u) + (n >= 1000u) + (n >= 10000u) + (n >= 100000u) + (n >= 1000000u) +
+           (n >= 10000000u) + (n >= 100000000u) + (n >= 1000000000u);
 }
 
-template <int BITS>
-__device__ __forceinline__ uint32_t walk_letter(const uint32_t *tape, uint32_t word, uint32_t index) {
-    return letter_at<BITS>(tape, word, index);
-}
-
+// One thread a pair walks its decisions back from its end (gotoh.mojo:189-200 `advance`), taking the pairs
+// in the sweep's order (a class at a time, longest first), so a warp's walks are alike in layout and end
+// together. Each step is one dependent read of a decision word and selects; the CIGAR leaves as runs
+// (back to front), their text's length counted, for cigar_text_kernel to spell.
 template <int BITS>
 __global__ void walk_kernel(WalkArgs a) {
-    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= a.count) return;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.count) return;
+    const int64_t k = a.order ? int64_t(a.order[i]) - a.first_pair : i;
     const int64_t pair = a.first_pair + k;
     const PairShape sh = a.shapes[pair];
     const int rows = int(sh.rows), cols = int(sh.columns);
-    char *slot = a.slots + a.slot_offsets[k];
-    int64_t written = 0;
+    uint32_t *runs = reinterpret_cast<uint32_t *>(a.slots + a.slot_offsets[k]);
+    int64_t run_count = 0, text = 0;
     int row, column;
     if (a.local) {
         const int64_t end = a.ends[k];
@@ -89,23 +93,26 @@ __global__ void walk_kernel(WalkArgs a) {
         column = cols;
     }
     const int end_row = row, end_col = column;
-    char run = 0;
-    int64_t count = 0;
-    auto add = [&](char op) {
-        if (op == run) {
-            ++count;
-        } else {
-            if (count > 0) emit_run(slot, written, run, count);
+    uint32_t run = kRunD, length = 0;
+    // `n` more letters of op `op`: a new run when the op changes, the last one left as a word.
+    auto add = [&](uint32_t op, uint32_t n) {
+        if (op != run) {
+            if (length > 0) {
+                runs[run_count++] = (run << 30) | length;
+                text += 1 + decimal_digits(length);
+            }
             run = op;
-            count = 1;
+            length = 0;
         }
+        length += n;
     };
     if (rows > 0 && cols > 0) {
         const int layout = a.layouts[k];
         const uint64_t *decisions = layout == 2 ? a.decisions_extra : a.decisions;
         const int G = record_lanes(uint32_t(cols), a.uniform);
-        const int W = G * 16;
+        const int lane_shift = __ffs(G * 16) - 1;  // a strip is G lanes of 16 columns
         const bool banded = layout == 1 || layout == 3 || layout == 4;
+        const bool planes = layout == 3 || layout == 4;
         const int width = layout == 4 ? kBandWidth / 2 : kBandWidth;  // layout 4: the narrow band's 32
         const int rows_pad = banded ? ((rows + 3) & ~3) : (((rows + 2) | 3) + 1);
         const int low = banded ? band_low_for_width(rows, cols, width) : 0;
@@ -126,6 +133,13 @@ __global__ void walk_kernel(WalkArgs a) {
             strip_pad = band_strip_pad(strip_first, strip_last);
         }
         int state = 0;  // 0 aligning, 1 deleting, 2 inserting
+        // The decision sector under the walk (four words, 32 bytes, from a multiple of four: every layout's
+        // lane blocks start there and run up by rows) and the tape words under its letters, kept in registers:
+        // a step reads memory only when it leaves them, about one step in four.
+        int64_t sector = -1;
+        uint64_t held0 = 0, held1 = 0, held2 = 0, held3 = 0;
+        constexpr uint32_t per_word = 32 / BITS;
+        uint32_t row_word_at = ~0u, column_word_at = ~0u, row_word = 0, column_word = 0;
         while (row > 0 && column > 0) {
             int64_t at;
             int slot_in;
@@ -148,68 +162,82 @@ __global__ void walk_kernel(WalkArgs a) {
                 const int member = within / 16;
                 slot_in = within % 16;
                 at = base + strip_at + int64_t(member) * strip_pad + (row - strip_first + (member & 3));
-            } else if (banded) {
-                // The band's layout: place o = column - row - low, a lane of 16 places a block of rows.
+            } else {
+                // The band's layout: place o = column - row - low, a lane of 16 places a block of rows. The
+                // proof keeps every optimal path inside the band; a place outside it would read another
+                // pair's decisions, so the walk stops there instead and flags the pair, whose CIGAR the host
+                // then reports as a device failure rather than a result.
                 const int place = column - row - low;
-                // The proof keeps every optimal path inside the band; a place outside it would read
-                // another pair's decisions, so the walk stops there instead and flags the pair, whose
-                // CIGAR the host then reports as a device failure rather than a result.
-                if (place < 0 || place >= width) {
+                if (banded && unsigned(place) >= unsigned(width)) {
                     if (a.failed) a.failed[pair] = kWalkFailed;
                     break;
                 }
-                slot_in = place % 16;
-                at = base + int64_t(place / 16) * rows_pad + (row - 1);
-            } else {
+                // The whole matrix's: strips of G lanes, each lane's rows skewed by its place in a sector.
                 const int off = column - 1;
-                const int s = off / W;
-                const int within = off % W;
-                const int member = within / 16;
-                slot_in = within % 16;
-                at = base + int64_t(s * G + member) * rows_pad + (row - 1 + (member & 3));
+                const int member = (off & ((1 << lane_shift) - 1)) >> 4;
+                const int64_t whole_at =
+                    base + int64_t((off >> lane_shift) * G + member) * rows_pad + (row - 1 + (member & 3));
+                const int64_t band_at = base + int64_t(place >> 4) * rows_pad + (row - 1);
+                at = banded ? band_at : whole_at;
+                slot_in = (banded ? place : off) & 15;
             }
-            const uint64_t word = decisions[at];
-            uint32_t nibble;
-            if (layout == 3 || layout == 4) {
-                // The 16-bit pair band's planes: bit `slot_in` of deleting, inserting, deletion extending and
-                // insertion extending, 16 bits each; inserting wins over deleting as decide() orders them.
-                const uint32_t del = uint32_t(word >> slot_in) & 1u, ins = uint32_t(word >> (16 + slot_in)) & 1u;
-                const uint32_t dext = uint32_t(word >> (32 + slot_in)) & 1u, iext = uint32_t(word >> (48 + slot_in)) & 1u;
-                nibble = (ins ? 2u : del) | (dext << 2) | (iext << 3);
-            } else {
-                nibble = uint32_t(word >> (4 * slot_in)) & 15u;
+            if ((at & ~int64_t(3)) != sector) {
+                sector = at & ~int64_t(3);
+                const uint4 low_words = *reinterpret_cast<const uint4 *>(decisions + sector);
+                const uint4 high_words = *reinterpret_cast<const uint4 *>(decisions + sector + 2);
+                held0 = uint64_t(low_words.x) | (uint64_t(low_words.y) << 32);
+                held1 = uint64_t(low_words.z) | (uint64_t(low_words.w) << 32);
+                held2 = uint64_t(high_words.x) | (uint64_t(high_words.y) << 32);
+                held3 = uint64_t(high_words.z) | (uint64_t(high_words.w) << 32);
             }
+            const int within_sector = int(at & 3);
+            const uint64_t word = within_sector == 0   ? held0
+                                  : within_sector == 1 ? held1
+                                  : within_sector == 2 ? held2
+                                                       : held3;
+            // The 16-bit pair band's planes: bit `slot_in` of deleting, inserting, deletion extending and
+            // insertion extending, 16 bits each; inserting wins over deleting as decide() orders them.
+            // Otherwise a nibble a place.
+            const uint32_t deleting = uint32_t(word >> slot_in) & 1u, inserting = uint32_t(word >> (16 + slot_in)) & 1u;
+            const uint32_t from_planes = (inserting ? 2u : deleting) | ((uint32_t(word >> (32 + slot_in)) & 1u) << 2) |
+                                         ((uint32_t(word >> (48 + slot_in)) & 1u) << 3);
+            const uint32_t nibble = planes ? from_planes : uint32_t(word >> (4 * slot_in)) & 15u;
             if (a.local && state == 0 && (nibble & 3u) == 3u) break;
             const int moving = state == 0 ? int(nibble & 3u) : state;
-            if (moving == 1) {
-                add('D');
-                row -= 1;
-                state = (nibble >> 2) & 1u ? 1 : 0;
-            } else if (moving == 2) {
-                add('I');
-                column -= 1;
-                state = (nibble >> 3) & 1u ? 2 : 0;
-            } else {
-                char op = 'M';
-                if (a.eqx) {
-                    const uint32_t x = walk_letter<BITS>(a.tape, sh.first_word, uint32_t(row - 1));
-                    const uint32_t y = walk_letter<BITS>(a.tape, sh.second_word, uint32_t(column - 1));
-                    op = x == y ? '=' : 'X';
+            uint32_t op = moving == 1 ? kRunD : moving == 2 ? kRunI : kRunM;
+            if (a.eqx && op == kRunM) {
+                const uint32_t x_at = uint32_t(row - 1), y_at = uint32_t(column - 1);
+                if (x_at / per_word != row_word_at) {
+                    row_word_at = x_at / per_word;
+                    row_word = __ldg(a.tape + sh.first_word + row_word_at);
                 }
-                add(op);
-                row -= 1;
-                column -= 1;
-                state = 0;
+                if (y_at / per_word != column_word_at) {
+                    column_word_at = y_at / per_word;
+                    column_word = __ldg(a.tape + sh.second_word + column_word_at);
+                }
+                constexpr uint32_t mask = BITS == 8 ? 0xFFu : (1u << BITS) - 1u;
+                const uint32_t x = (row_word >> (BITS * (x_at % per_word))) & mask;
+                const uint32_t y = (column_word >> (BITS * (y_at % per_word))) & mask;
+                op = x == y ? kRunM : kRunX;
             }
+            add(op, 1);
+            state = moving == 1 ? int((nibble >> 2) & 1u) : moving == 2 ? 2 * int((nibble >> 3) & 1u) : 0;
+            row -= moving != 2;
+            column -= moving != 1;
         }
     }
     if (!a.local) {
         // gotoh.mojo:440-447: a global walk's rest is gaps against the letters left, rows first.
-        for (; row > 0; --row) add('D');
-        for (; column > 0; --column) add('I');
+        if (row > 0) add(kRunD, uint32_t(row));
+        if (column > 0) add(kRunI, uint32_t(column));
+        row = column = 0;
     }
-    if (count > 0) emit_run(slot, written, run, count);
-    a.lengths[k] = written;
+    if (length > 0) {
+        runs[run_count++] = (run << 30) | length;
+        text += 1 + decimal_digits(length);
+    }
+    a.lengths[k] = text;
+    a.run_counts[k] = run_count;
     int64_t *span = a.spans + 4 * k;
     span[0] = row;
     span[1] = end_row;
@@ -217,17 +245,46 @@ __global__ void walk_kernel(WalkArgs a) {
     span[3] = end_col;
 }
 
-// Each pair's CIGAR, written back to front in its slot, turned round into the packed output.
-__global__ void gather_cigars_kernel(const char *__restrict__ slots, const int64_t *__restrict__ slot_offsets,
-                                     const int64_t *__restrict__ lengths, const int64_t *__restrict__ offsets,
-                                     char *__restrict__ out, int64_t count) {
+// Each pair's CIGAR text from its runs, which the walk left back to front: a warp a pair, 32 runs at a time
+// in the CIGAR's order, each lane's place in the text by a prefix sum of the runs' lengths in letters.
+__global__ void cigar_text_kernel(const char *__restrict__ slots, const int64_t *__restrict__ slot_offsets,
+                                  const int64_t *__restrict__ run_counts, const int64_t *__restrict__ offsets, bool eqx,
+                                  char *__restrict__ out, int64_t count) {
     const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= count) return;
-    const char *from = slots + slot_offsets[warp];
-    const int64_t n = lengths[warp];
+    const uint32_t *runs = reinterpret_cast<const uint32_t *>(slots + slot_offsets[warp]);
+    const int64_t n = run_counts[warp];
     char *to = out + offsets[warp];
-    for (int64_t i = lane; i < n; i += 32) to[i] = from[n - 1 - i];
+    // The ops' letters by run op, a byte each.
+    const uint32_t ops = uint32_t('D') | (uint32_t('I') << 8) | (uint32_t(eqx ? '=' : 'M') << 16) | (uint32_t('X') << 24);
+    int64_t at = 0;
+    for (int64_t first = 0; first < n; first += 32) {
+        const int64_t j = first + lane;
+        uint32_t word = 0;
+        int letters = 0;
+        if (j < n) {
+            word = runs[n - 1 - j];
+            letters = 1 + decimal_digits(word & kRunLength);
+        }
+        int through = letters;  // inclusive prefix sum over the warp's runs
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int before = __shfl_up_sync(kFull, through, d);
+            if (lane >= d) through += before;
+        }
+        if (j < n) {
+            // The count's digits, then the op, ending at the run's last letter.
+            char *p = to + at + through - 1;
+            *p-- = char((ops >> (8 * (word >> 30))) & 0xFFu);
+            uint32_t value = word & kRunLength;
+            do {
+                *p-- = char('0' + value % 10u);
+                value /= 10u;
+            } while (value > 0);
+        }
+        at += __shfl_sync(kFull, through, 31);
+    }
 }
 
 __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t first_pair, int64_t count, bool uniform,
@@ -255,7 +312,7 @@ __global__ void slot_sizes_kernel(const PairShape *__restrict__ shapes, int64_t 
         words = strips * G * rows_pad;
     }
     decision_words[k] = words;
-    slot_bytes[k] = 2 * (int64_t(sh.rows) + sh.columns) + 8;
+    slot_bytes[k] = 4 * (int64_t(sh.rows) + sh.columns) + 8;
     layouts[k] = layout;
 }
 
@@ -1069,12 +1126,17 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     uint64_t *decisions = gpu->decisions.ensure<uint64_t>(size_t(totals[0]) + 8);
     char *slots = gpu->walk_out.ensure<char>(size_t(totals[1]) + 8);
     int64_t *ends = gpu->spans.ensure<int64_t>(size_t(count) + 1);
-    int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(size_t(count) + 1);
+    int64_t *lengths = gpu->cigar_lengths.ensure<int64_t>(2 * (size_t(count) + 1));
+    int64_t *run_counts = lengths + (count + 1);
     PairLimits limits;
     limits.band = band ? pair_limit_of(table) : 0;
     limits.band_widths = widths;
     limits.band_first = first_pair;
     const Schedule schedule_all = dinara::schedule(gpu, batch.shapes, nullptr, first_pair, count, true, band, limits);
+    // The walk takes the pairs in this order; a later schedule (the band's leftovers) reuses its buffer.
+    uint32_t *walk_order = gpu->walk_order.ensure<uint32_t>(size_t(count));
+    DINARA_CUDA(cudaMemcpyAsync(walk_order, schedule_all.order, size_t(count) * sizeof(uint32_t),
+                                cudaMemcpyDeviceToDevice, gpu->stream));
 
     PhaseTimer timer(gpu, &gpu->record_ms);
     KernelArgs args;
@@ -1144,6 +1206,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.slot_offsets = slot_offsets;
     w.slots = slots;
     w.lengths = lengths;
+    w.run_counts = run_counts;
+    w.order = walk_order;
     w.failed = batch.flags;
     w.spans = spans;
     w.first_pair = first_pair;
@@ -1153,17 +1217,20 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     w.eqx = eqx;
     w.uniform = uniform;
     ClockSpan walk_clock(gpu, kClassWalk, gpu->stream);
+    // Blocks of 128: the walk's registers leave room for 28 warps an SM, which 256-thread blocks would cut
+    // to 24.
+    const unsigned walk_blocks = unsigned((count + 127) / 128);
     if (batch.bits == 8)
-        walk_kernel<8><<<blocks, threads, 0, gpu->stream>>>(w);
+        walk_kernel<8><<<walk_blocks, 128, 0, gpu->stream>>>(w);
     else
-        walk_kernel<2><<<blocks, threads, 0, gpu->stream>>>(w);
+        walk_kernel<2><<<walk_blocks, 128, 0, gpu->stream>>>(w);
     DINARA_CUDA(cudaGetLastError());
     walk_clock.stop();
     gpu->launches += 1;
     timer.stop();
     tally_swept(gpu, batch.shapes, first_pair, count, band, leftovers, left, widths);
 
-    // The CIGARs' offsets, then each turned round into place.
+    // The CIGARs' offsets, then each spelled from its runs.
     int64_t *offsets = gpu->cigar_offsets.ensure<int64_t>(size_t(count) + 2);
     DINARA_CUDA(cudaMemsetAsync(lengths + count, 0, sizeof(int64_t), gpu->stream));
     size_t scratch3 = 0;
@@ -1174,7 +1241,8 @@ int64_t affine_alignments(dinara_gpu *gpu, const AffineBatch &batch, const Affin
     read_back(gpu, &total, offsets + count, sizeof(int64_t));
     char *out = gpu->cigar_bytes.ensure<char>(size_t(total) + 8);
     const unsigned gather_blocks = unsigned((count * 32 + threads - 1) / threads);
-    gather_cigars_kernel<<<gather_blocks, threads, 0, gpu->stream>>>(slots, slot_offsets, lengths, offsets, out, count);
+    cigar_text_kernel<<<gather_blocks, threads, 0, gpu->stream>>>(slots, slot_offsets, run_counts, offsets, eqx, out,
+                                                                  count);
     DINARA_CUDA(cudaGetLastError());
     gpu->launches += 1;
     return total;
