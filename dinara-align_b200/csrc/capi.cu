@@ -927,6 +927,38 @@ struct Timer {
 };
 
 // The learned band's first thresholds, with the device time they took.
+// A partner context takes its context's band tuning and trained predictor (the parameters copied on the
+// context's stream), so that a unit it runs chooses windows and first thresholds as the context would.
+void share_band_state(dinara_gpu *from, dinara_gpu *to) {
+    to->band_tuning = from->band_tuning;
+    to->predictor_ready = from->predictor_ready;
+    for (int k = 0; k < 4; ++k) to->predictor_margins[k] = from->predictor_margins[k];
+    to->predictor_margin = from->predictor_margin;
+    to->predictor_slack = from->predictor_slack;
+    if (from->predictor_ready) {
+        float *parameters = to->weights.ensure<float>(size_t(kPredictorParameters));
+        DINARA_CUDA(cudaMemcpyAsync(parameters, from->weights.as<float>(), size_t(kPredictorParameters) * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, from->stream));
+    }
+}
+
+// Adds a unit's band report to the batch's.
+void add_band_report(dinara_band_report &into, const dinara_band_report &unit) {
+    into.rounds += unit.rounds;
+    into.pair_rounds += unit.pair_rounds;
+    into.words_swept += unit.words_swept;
+    into.first_round_hits += unit.first_round_hits;
+    into.overshoot += unit.overshoot;
+    into.undershoot += unit.undershoot;
+    into.kernel_ms += unit.kernel_ms;
+    into.predict_ms += unit.predict_ms;
+    for (int r = 0; r < 16; ++r) {
+        into.round_pairs[r] += unit.round_pairs[r];
+        into.round_launches[r] += unit.round_launches[r];
+        into.round_ms[r] += unit.round_ms[r];
+    }
+}
+
 const int64_t *timed_predictions(dinara_gpu *gpu, int64_t pairs, const uint8_t *letters, const int64_t *offsets,
                                  double *ms) {
     DINARA_CUDA(cudaEventRecord(gpu->start, gpu->stream));
@@ -939,6 +971,96 @@ const int64_t *timed_predictions(dinara_gpu *gpu, int64_t pairs, const uint8_t *
     DINARA_CUDA(cudaEventElapsedTime(&elapsed, gpu->start, gpu->stop));
     *ms = elapsed;
     return starts;
+}
+
+// Distances of a batch of several units, its letters streamed: the letters go up in pieces on the upload
+// stream while earlier units run, each unit (its first thresholds, then its band doubling) starting once
+// its letters are there, the units round the context and its partners (each its own lane, stream and
+// scratch), so that a unit's upload overlaps others' rounds and one unit's last long pairs overlap
+// another's bulk. Every distance is the one band doubling gives the whole batch: a pair's rounds depend on
+// that pair alone.
+void streamed_distances(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
+                        const std::vector<int64_t> &relative, const dinara_band_plan *plan,
+                        const std::vector<std::pair<int64_t, int64_t>> &units, int64_t *results,
+                        dinara_band_report *report) {
+    const int64_t policy = plan ? plan->policy : DINARA_BAND_PLAIN;
+    const int64_t first_letter = offsets[0];
+    const int64_t total = offsets[2 * pairs] - first_letter;
+    uint8_t *letters_device = gpu->letters.as<uint8_t>();
+    int64_t *offsets_device = gpu->offsets.as<int64_t>();
+    int64_t *results_device = gpu->scores.ensure<int64_t>(size_t(pairs));
+    to_device(gpu, offsets_device, relative.data(), relative.size() * sizeof(int64_t), gpu->pinned_small);
+    int64_t *given = nullptr;
+    if (policy == DINARA_BAND_GIVEN) {
+        given = gpu->predictions.ensure<int64_t>(size_t(pairs));
+        to_device(gpu, given, plan->start_thresholds, size_t(pairs) * sizeof(int64_t), gpu->pinned_small);
+    }
+    const size_t lanes = std::min(kLanes, units.size());
+    dinara_gpu *contexts[kMaxLanes] = {gpu};
+    for (size_t l = 1; l < lanes; ++l) {
+        contexts[l] = partner_of(contexts[l - 1]);
+        share_band_state(gpu, contexts[l]);
+    }
+    cudaEvent_t inputs_ready = nullptr;
+    DINARA_CUDA(cudaEventCreateWithFlags(&inputs_ready, cudaEventDisableTiming));
+    DINARA_CUDA(cudaEventRecord(inputs_ready, gpu->stream));
+    std::vector<dinara_band_report> unit_reports(units.size());
+    for (dinara_band_report &r : unit_reports) std::memset(&r, 0, sizeof r);
+    std::exception_ptr failures[kMaxLanes];
+    {
+        LetterUpload upload(gpu, letters_device, reinterpret_cast<const uint8_t *>(letters) + first_letter,
+                            size_t(total));
+        auto lane = [&](size_t l) {
+            try {
+                dinara_gpu *ctx = contexts[l];
+                AllocationScope scope(ctx->stream);
+                DINARA_CUDA(cudaSetDevice(gpu->device));
+                if (ctx != gpu) DINARA_CUDA(cudaStreamWaitEvent(ctx->stream, inputs_ready, 0));
+                for (size_t k = l; k < units.size(); k += lanes) {
+                    const int64_t first = units[k].first, count = units[k].second;
+                    upload.wait_for(size_t(offsets[2 * (first + count)] - first_letter), ctx->stream);
+                    const int64_t *unit_offsets = offsets_device + 2 * first;
+                    const int64_t *starts = nullptr;
+                    double predict_ms = 0.0;
+                    if (policy == DINARA_BAND_GIVEN)
+                        starts = given + first;
+                    else if (policy == DINARA_BAND_LEARNED)
+                        starts = timed_predictions(ctx, count, letters_device, unit_offsets, &predict_ms);
+                    band_doubling(ctx, count, letters_device, unit_offsets, starts, plan ? plan->default_start : 0,
+                                  results_device + first, report ? &unit_reports[k] : nullptr);
+                    unit_reports[k].predict_ms = predict_ms;
+                }
+            } catch (...) {
+                failures[l] = std::current_exception();
+            }
+        };
+        std::thread helpers[kMaxLanes];
+        for (size_t l = 1; l < lanes; ++l) helpers[l] = std::thread(lane, l);
+        lane(0);
+        for (size_t l = 1; l < lanes; ++l) helpers[l].join();
+        for (size_t l = 1; l < lanes; ++l) {
+            // The results' copy waits for every partner's units.
+            cudaEvent_t joined = nullptr;
+            if (cudaEventCreateWithFlags(&joined, cudaEventDisableTiming) == cudaSuccess) {
+                if (cudaEventRecord(joined, contexts[l]->stream) == cudaSuccess)
+                    cudaStreamWaitEvent(gpu->stream, joined, 0);
+                cudaEventDestroy(joined);
+            } else {
+                cudaStreamSynchronize(contexts[l]->stream);
+            }
+        }
+    }
+    cudaEventDestroy(inputs_ready);
+    for (std::exception_ptr &failure : failures)
+        if (failure) std::rethrow_exception(failure);
+    to_host_now(gpu, results, results_device, size_t(pairs) * sizeof(int64_t));
+    if (report) {
+        for (const dinara_band_report &r : unit_reports) add_band_report(*report, r);
+        int64_t cells = 0;
+        for (int64_t p = 0; p < pairs; ++p)
+            cells += (offsets[2 * p + 1] - offsets[2 * p]) * (offsets[2 * p + 2] - offsets[2 * p + 1]);
+        report->full_cells = cells;
+    }
 }
 
 }  // namespace
@@ -1397,6 +1519,11 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
         for (int64_t k = 0; k <= 2 * pairs; ++k) relative[size_t(k)] = offsets[k] - first;
         uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
         int64_t *offsets_device = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
+        const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
+        if (units.size() > 1) {
+            streamed_distances(gpu, pairs, letters, offsets, relative, plan, units, results, report);
+            return 0;
+        }
         to_device(gpu, letters_device, letters + first, size_t(total), gpu->pinned_in);
         to_device(gpu, offsets_device, relative.data(), relative.size() * sizeof(int64_t), gpu->pinned_small);
         const int64_t *starts = nullptr;

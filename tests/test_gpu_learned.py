@@ -68,6 +68,11 @@ def test_learned_band_is_exact_and_gains(da, oracle, learned, tmp_path):
     np.testing.assert_array_equal(plain, expected)
     np.testing.assert_array_equal(learned_found, expected)
     assert learned_report["words_swept"] < 0.8 * plain_report["words_swept"], (plain_report, learned_report)
+    # A batch of several units streams its letters, each unit predicted and doubled on its own lane with
+    # the context's predictor: the same distances.
+    big = workloads.uneven_unit_cost(70_000, high=600, seed=23)
+    expected_big = oracle.batch_distances(big.letters[: big.offsets[-1]], big.offsets, start=-1, threads=8)
+    np.testing.assert_array_equal(da.distances_tape(big, policy=da._native.BAND_LEARNED), expected_big)
     predicted, thresholds = predictor.predict(tape)
     assert (thresholds >= 1).all() and np.isfinite(predicted).all()
     # The blob keeps every length class's margin: loaded back, the thresholds are the same.
