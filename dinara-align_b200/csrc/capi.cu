@@ -419,6 +419,8 @@ constexpr int64_t kUnitPairs = 32768;
 // Units run on this many lanes: the context, its partner, the partner's partner, and so on.
 constexpr size_t kLanes = 4;
 constexpr size_t kMaxLanes = 4;
+// Units (and lanes) of a streamed distance batch.
+constexpr int64_t kDistanceUnits = 2;
 
 // The caller's letters copied to the device a piece at a time on the context's upload stream. From
 // page-locked memory every piece is queued at once; from pageable memory a helper thread stages each
@@ -527,9 +529,10 @@ class LetterUpload {
 // decisions fit the budget, as they mostly do, the cuts are binary searches over the offsets.
 template <class W>
 std::vector<std::pair<int64_t, int64_t>> plan_units(int64_t pairs, const int64_t *offsets, bool split, W &&words_of,
-                                                    bool budgeted, int64_t budget_words) {
+                                                    bool budgeted, int64_t budget_words,
+                                                    int64_t most_units = kMaxUnits) {
     const int64_t letters = offsets[2 * pairs] - offsets[0];
-    const int64_t units = split ? std::min(kMaxUnits, std::max<int64_t>(1, pairs / kUnitPairs)) : 1;
+    const int64_t units = split ? std::min(most_units, std::max<int64_t>(1, pairs / kUnitPairs)) : 1;
     // Unit u ends where the share of letters of units 0..u does: halves at both ends.
     auto share_end = [&](int64_t u) {
         if (u >= units) return letters;
@@ -973,11 +976,13 @@ const int64_t *timed_predictions(dinara_gpu *gpu, int64_t pairs, const uint8_t *
     return starts;
 }
 
-// Distances of a batch of several units, its letters streamed: the letters go up in pieces on the upload
-// stream while earlier units run, each unit (its first thresholds, then its band doubling) starting once
-// its letters are there, the units round the context and its partners (each its own lane, stream and
-// scratch), so that a unit's upload overlaps others' rounds and one unit's last long pairs overlap
-// another's bulk. Every distance is the one band doubling gives the whole batch: a pair's rounds depend on
+// Distances of a batch of several units (kDistanceUnits at most), its letters streamed: the letters go up
+// in pieces on the upload stream while the first unit runs, each unit (its first thresholds, then its band
+// doubling) starting once its letters are there, on a lane of its own (the context or its partner, each
+// with its stream and scratch). A unit's rounds are bound by its longest pairs' chains of word steps, so
+// the call takes about the last unit's upload and its chains; on the uneven batch (1.5 GB, 27 ms to
+// upload) two units on two lanes measured 65 ms against 78 unstreamed, and more units or lanes no
+// better (six lanes 85 ms: their predictions and rounds crowd each other). Every distance is the one band doubling gives the whole batch: a pair's rounds depend on
 // that pair alone.
 void streamed_distances(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
                         const std::vector<int64_t> &relative, const dinara_band_plan *plan,
@@ -995,8 +1000,8 @@ void streamed_distances(dinara_gpu *gpu, int64_t pairs, const char *letters, con
         given = gpu->predictions.ensure<int64_t>(size_t(pairs));
         to_device(gpu, given, plan->start_thresholds, size_t(pairs) * sizeof(int64_t), gpu->pinned_small);
     }
-    const size_t lanes = std::min(kLanes, units.size());
-    dinara_gpu *contexts[kMaxLanes] = {gpu};
+    const size_t lanes = std::min(size_t(kDistanceUnits), units.size());
+    dinara_gpu *contexts[kDistanceUnits] = {gpu};
     for (size_t l = 1; l < lanes; ++l) {
         contexts[l] = partner_of(contexts[l - 1]);
         share_band_state(gpu, contexts[l]);
@@ -1006,7 +1011,7 @@ void streamed_distances(dinara_gpu *gpu, int64_t pairs, const char *letters, con
     DINARA_CUDA(cudaEventRecord(inputs_ready, gpu->stream));
     std::vector<dinara_band_report> unit_reports(units.size());
     for (dinara_band_report &r : unit_reports) std::memset(&r, 0, sizeof r);
-    std::exception_ptr failures[kMaxLanes];
+    std::exception_ptr failures[kDistanceUnits];
     {
         LetterUpload upload(gpu, letters_device, reinterpret_cast<const uint8_t *>(letters) + first_letter,
                             size_t(total));
@@ -1034,7 +1039,7 @@ void streamed_distances(dinara_gpu *gpu, int64_t pairs, const char *letters, con
                 failures[l] = std::current_exception();
             }
         };
-        std::thread helpers[kMaxLanes];
+        std::thread helpers[kDistanceUnits];
         for (size_t l = 1; l < lanes; ++l) helpers[l] = std::thread(lane, l);
         lane(0);
         for (size_t l = 1; l < lanes; ++l) helpers[l].join();
@@ -1519,7 +1524,8 @@ int64_t dinara_gpu_distances_tape(dinara_gpu *gpu, int64_t pairs, const char *le
         for (int64_t k = 0; k <= 2 * pairs; ++k) relative[size_t(k)] = offsets[k] - first;
         uint8_t *letters_device = gpu->letters.ensure<uint8_t>(size_t(total) + 16);
         int64_t *offsets_device = gpu->offsets.ensure<int64_t>(size_t(2 * pairs + 1));
-        const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
+        const auto units =
+            plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0, kDistanceUnits);
         if (units.size() > 1) {
             streamed_distances(gpu, pairs, letters, offsets, relative, plan, units, results, report);
             return 0;
