@@ -176,7 +176,7 @@ def _cigar_score(reference, query, cigar, scoring):
     return score, r, q
 
 
-@pytest.mark.parametrize("scoring_name", ["config2", "dna"])
+@pytest.mark.parametrize("scoring_name", ["config2", "dna", "steep", "wide"])
 def test_long_cigars_over_a_proven_band(da, oracle, scoring_name):
     """Global CIGARs of long pairs (4,096 x 2,048 letters and more) recorded strip by strip over the band
     their widening band proved: few and many errors, a long deletion and a long insertion that take the

@@ -183,3 +183,34 @@ def test_extension_refusals(da):
         da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(0, zdrop=0))
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(1))
+
+
+def test_five_letter_alphabet(da, oracle):
+    """A table of five letters puts pairs on the 8-bit tape and the shared-memory table: free-end scores and
+    alignments (INFIX and a few letters each end) and extensions from both anchors against the oracle."""
+    rng = np.random.default_rng(59)
+    cells = [[6 if r == c else (-2 if 4 in (r, c) else -4) for c in range(5)] for r in range(5)]
+    scoring = da.Scoring.tabulated("ACGTN", [v for row in cells for v in row], -5, -2)
+    refs, queries = [], []
+    for trial in range(120):
+        n = int(rng.integers(0, 300 if trial % 20 else 900))
+        ref = "".join(rng.choice(list("ACGTN"), size=n))
+        start = int(rng.integers(0, n // 3 + 1))
+        piece = ref[start:start + int(rng.integers(0, n - start + 1))]
+        query = "".join(ch if rng.random() > 0.05 else rng.choice(list("ACGTN")) for ch in piece)
+        if trial % 9 == 0:
+            query = "".join(rng.choice(list("ACGTN"), size=int(rng.integers(0, 80))))
+        refs.append(ref)
+        queries.append(query)
+    for mode in (da.Mode.INFIX, da.Mode.ends_free(reference_start=6, reference_end=9, query_start=2, query_end=4)):
+        assert da.scores(refs, queries, scoring, mode) == _expected(oracle, scoring, refs, queries, mode)
+        found = da.alignments(refs, queries, scoring, mode)
+        expected = _expected_alignments(oracle, scoring, refs, queries, mode)
+        assert [(a.score, a.cigar, (a.reference_start, a.reference_end, a.query_start, a.query_end))
+                for a in found] == [tuple(e) for e in expected]
+    for from_end in (False, True):
+        mode = da.Mode.extension(0, da.Anchor.END if from_end else da.Anchor.START, end_bonus=9)
+        found = da.alignments(refs, queries, scoring, mode)
+        expected = _expected_extensions(oracle, scoring, refs, queries, from_end, 9)
+        assert [(a.score, a.cigar, (a.reference_start, a.reference_end, a.query_start, a.query_end))
+                for a in found] == [tuple(e) for e in expected]
