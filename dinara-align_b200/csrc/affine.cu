@@ -894,19 +894,70 @@ __global__ void extents_kernel(const PairShape *__restrict__ shapes, int64_t fir
     extents[k] = (int64_t(sh.rows) << 32) | int64_t(sh.columns);
 }
 
-// An extension's span from its stop: from the origin to the stop, or (swept from the ends) from the stop,
-// counted back from the ends, to the ends.
-__global__ void extension_spans_kernel(const PairShape *__restrict__ shapes, int64_t first, const int64_t *__restrict__ stops,
-                                       int64_t count, bool from_end, int64_t *__restrict__ spans) {
+// Each pair's anti-diagonals kept for an extension's Z-drop: rows + columns + 1 (none for an empty side).
+__global__ void diagonal_counts_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count,
+                                       int64_t *__restrict__ counts) {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const PairShape sh = shapes[first + k];
-    const int64_t row = stops[k] >> 32, column = stops[k] & 0xffffffff;
-    int64_t *span = spans + 4 * k;
-    span[0] = from_end ? int64_t(sh.rows) - row : 0;
-    span[1] = from_end ? int64_t(sh.rows) : row;
-    span[2] = from_end ? int64_t(sh.columns) - column : 0;
-    span[3] = from_end ? int64_t(sh.columns) : column;
+    counts[k] = sh.rows > 0 && sh.columns > 0 ? int64_t(sh.rows) + sh.columns + 1 : 0;
+}
+
+// An extension's result from its sweep, one thread a pair. With a Z-drop (`diagonals`), the stop is read
+// from the anti-diagonals' bests in order as scored.mojo:272-300 reads them: a best above zero at or
+// above the best so far is the new stop (later anti-diagonals win ties); one below it ends the sweep when
+// it lies more than `zdrop` plus `slack` a diagonal between them (each's reference less query letters)
+// below it. Otherwise the sweep's best cell is the stop. The span runs from the origin to the stop, or
+// (swept from the ends) from the stop counted back to the ends. With an end bonus and no early end, the
+// alignment reaching the query's far end wins when its score plus the bonus passes the stop's
+// (scoring.mojo:704-710), compared without the sum: the bonus may be near 2^63.
+__global__ void extension_finish_kernel(const PairShape *__restrict__ shapes, int64_t first, int64_t count,
+                                        bool from_end, const int64_t *__restrict__ stops,
+                                        const unsigned long long *__restrict__ diagonals,
+                                        const int64_t *__restrict__ diagonal_offsets, int64_t zdrop, int64_t slack,
+                                        int64_t end_bonus, const int32_t *__restrict__ reach_scores,
+                                        const int64_t *__restrict__ reach_spans, int32_t *__restrict__ scores,
+                                        int64_t *__restrict__ spans) {
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int64_t pair = first + k;
+    const PairShape sh = shapes[pair];
+    const int64_t rows = sh.rows, columns = sh.columns;
+    int64_t best = scores[pair], row = stops[k] >> 32, column = stops[k] & 0xffffffff;
+    bool dropped = false;
+    if (diagonals && rows > 0 && columns > 0) {
+        const unsigned long long *kept = diagonals + diagonal_offsets[k];
+        int64_t best_row = 0, best_diagonal = 0;
+        best = 0;
+        for (int64_t d = 2; d <= rows + columns; ++d) {
+            const unsigned long long key = kept[d];
+            const int64_t most = int64_t(int32_t(uint32_t(key >> 32) ^ 0x80000000u));
+            const int64_t furthest = int64_t(key & 0xffffffffu);
+            if (most > 0 && most >= best) {
+                best = most;
+                best_row = furthest;
+                best_diagonal = d;
+            } else if (most < best) {
+                const int64_t lean = 2 * furthest - d, best_lean = 2 * best_row - best_diagonal;
+                const int64_t apart = lean > best_lean ? lean - best_lean : best_lean - lean;
+                if (best - most > zdrop + slack * apart) {
+                    dropped = true;
+                    break;
+                }
+            }
+        }
+        row = best_row;
+        column = best_diagonal - best_row;
+    }
+    int64_t span[4] = {from_end ? rows - row : 0, from_end ? rows : row, from_end ? columns - column : 0,
+                       from_end ? columns : column};
+    if (end_bonus > 0 && !dropped && end_bonus > best - int64_t(reach_scores[pair])) {
+        best = reach_scores[pair];
+        for (int j = 0; j < 4; ++j) span[j] = reach_spans[4 * k + j];
+    }
+    scores[pair] = int32_t(best);
+    if (spans)
+        for (int j = 0; j < 4; ++j) spans[4 * k + j] = span[j];
 }
 
 // Global scores with free ends: every pair over its whole matrix in 32 bits, one shape (32 lanes of 16
@@ -920,6 +971,20 @@ __global__ void extension_spans_kernel(const PairShape *__restrict__ shapes, int
 // the origin or, read backwards, from the ends; its span runs from its anchor to the stop.
 void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
                      int64_t first, int64_t count, int64_t *spans) {
+    // An extension's end bonus weighs the alignment reaching the query's far end (from the same anchor, the
+    // whole query against the reference, whose far end is free): its score and span first.
+    int32_t *reach_scores = nullptr;
+    int64_t *reach_spans = nullptr;
+    if (batch.extension && batch.end_bonus > 0) {
+        AffineBatch reaching = batch;
+        reaching.extension = false;
+        reaching.free_reference_start = batch.from_end ? INT32_MAX : 0;
+        reaching.free_reference_end = batch.from_end ? 0 : INT32_MAX;
+        reaching.free_query_start = reaching.free_query_end = 0;
+        reach_scores = gpu->reach_scores.ensure<int32_t>(size_t(batch.pairs));
+        reach_spans = gpu->reach_spans.ensure<int64_t>(4 * size_t(count));
+        free_end_scores(gpu, reaching, table, reach_scores, first, count, reach_spans);
+    }
     const Schedule order = dinara::schedule(gpu, batch.shapes, nullptr, first, count, false, false, PairLimits());
     int32_t *table32 = nullptr;
     upload_table32(gpu, table, false, &table32);
@@ -959,6 +1024,26 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
             gpu->launches += 1;
             args.extents = extents;
         }
+        if (batch.zdrop >= 0) {
+            // Room for every pair's anti-diagonals, by a scan of their counts, zeroed (below every key).
+            int64_t *counts = gpu->diagonal_offsets.ensure<int64_t>(2 * (size_t(count) + 1));
+            int64_t *offsets = counts + (count + 1);
+            diagonal_counts_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(batch.shapes, first, count,
+                                                                                         counts);
+            DINARA_CUDA(cudaGetLastError());
+            gpu->launches += 1;
+            DINARA_CUDA(cudaMemsetAsync(counts + count, 0, sizeof(int64_t), gpu->stream));
+            size_t scratch = 0;
+            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, counts, offsets, int(count + 1), gpu->stream));
+            void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
+            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, counts, offsets, int(count + 1), gpu->stream));
+            int64_t kept = 0;
+            read_back(gpu, &kept, offsets + count, sizeof kept);
+            unsigned long long *diagonals = gpu->diagonals.ensure<unsigned long long>(size_t(kept) + 1);
+            DINARA_CUDA(cudaMemsetAsync(diagonals, 0, (size_t(kept) + 1) * sizeof(unsigned long long), gpu->stream));
+            args.diagonals = diagonals;
+            args.diagonal_offsets = offsets;
+        }
     }
     int64_t total = 0;
     for (int cls = 0; cls < kClasses; ++cls) total += order.counts[cls];
@@ -977,12 +1062,11 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
     clock.stop();
     gpu->launches += 1;
     if (batch.extension) {
-        if (spans) {
-            extension_spans_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(
-                batch.shapes, first, ends, count, batch.from_end, spans);
-            DINARA_CUDA(cudaGetLastError());
-            gpu->launches += 1;
-        }
+        extension_finish_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(
+            batch.shapes, first, count, batch.from_end, ends, args.diagonals, args.diagonal_offsets, batch.zdrop,
+            -int64_t(table.extend), batch.end_bonus, reach_scores, reach_spans, scores, spans);
+        DINARA_CUDA(cudaGetLastError());
+        gpu->launches += 1;
     } else if (spans) {
         // The sweep back: each pair's prefixes to its end, backwards, the start's free letters free at the
         // (backward) end and none at its start; its scores, the same, go to scratch.

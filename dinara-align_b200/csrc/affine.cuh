@@ -54,8 +54,11 @@ struct AffineBatch {
     int32_t free_reference_start = 0, free_reference_end = 0, free_query_start = 0, free_query_end = 0;
     // An extension's stop (scoring.mojo:673-688 extension_span): from the origin, or with `from_end` from
     // both sequences' ends (read backwards), to the best cell anywhere; `free_ends` is then set too, with no
-    // letters free.
+    // letters free. A Z-drop of `zdrop` (0 or more; negative: none) ends the sweep early
+    // (scored.mojo:272-300); an `end_bonus` above zero takes the alignment reaching the query's far end when
+    // its score plus the bonus passes the stop's and the sweep was not ended early (scoring.mojo:704-710).
     bool extension = false, from_end = false;
+    int64_t zdrop = -1, end_bonus = -1;
 };
 
 // The flag value a failed walk leaves (1 is a letter outside the alphabet).

@@ -66,6 +66,11 @@ struct KernelArgs {
     int64_t *free_ends_out;
     const int64_t *extents;
     int32_t free_highest;
+    // An extension's Z-drop (affine_kernel<..., ORIGIN>): each anti-diagonal's best cell, its true score
+    // (offset by 2^31) in the high 32 bits and its row in the low, kept by atomic maximum at
+    // diagonals[diagonal_offsets[pair - first_pair] + row + column].
+    unsigned long long *diagonals;
+    const int64_t *diagonal_offsets;
 };
 
 // The lowest diagonal (column less row) of a band of `width` diagonals holding a pair's main and end
@@ -238,6 +243,7 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
         }
         int64_t strip_base = 0;
         int previous_last = rows;
+        const int64_t diagonal_base = ORIGIN && p.diagonals && work ? p.diagonal_offsets[pair - p.first_pair] : -1;
 
         for (int s = 0; s < warp_strips; ++s) {
             const bool strip_live = s < strips;
@@ -393,10 +399,19 @@ __global__ void __launch_bounds__(kBlock) affine_kernel(KernelArgs p, TableArgs 
                                 }
                             }
                             if (ORIGIN) {
-                                // An extension may stop at any cell, as a true score.
+                                // An extension may stop at any cell, as a true score; with a Z-drop each
+                                // anti-diagonal's best is kept too, for the stop to be read in their order.
 #pragma unroll
                                 for (int k = 0; k < C; ++k)
-                                    if (k < owned) offer(H[k] + (row + first_col + k + 1) * extend, row, first_col + k + 1);
+                                    if (k < owned) {
+                                        const int column = first_col + k + 1;
+                                        const int32_t value = H[k] + (row + column) * extend;
+                                        offer(value, row, column);
+                                        if (diagonal_base >= 0)
+                                            atomicMax(p.diagonals + diagonal_base + row + column,
+                                                      (static_cast<unsigned long long>(uint32_t(value) ^ 0x80000000u)
+                                                       << 32) | uint32_t(row));
+                                    }
                             } else if (FREE) {
                                 // Ends on the last row within free_qe letters of the last column, and on the
                                 // last column within free_re letters of the last row, as true scores.

@@ -124,16 +124,16 @@ bool check_scores_mode(const dinara_mode *mode, AffineBatch &batch) {
     batch.extension = false;
     if (mode && mode->kind == DINARA_EXTENSION) {
         // An extension (scoring.mojo:673-688): from the starts or the ends, no match score of the mode's own
-        // beside the table's. A Z-drop judges whole anti-diagonals, which a row sweep does not see in
-        // order; one too large ever to stop the sweep (scores stay within 2^28 of zero) is taken as none.
+        // beside the table's. A Z-drop too large ever to end the sweep (scores stay within 2^28 of zero) is
+        // taken as none, which spares reading the anti-diagonals in order.
         if (mode->match_score > 0)
             throw Failure(DINARA_INVALID_MODE, "a match score in the mode as well as in the Scoring's table");
         if (mode->anchor != 0 && mode->anchor != 1) throw Failure(DINARA_INVALID_MODE, "an anchor at neither end");
-        if (mode->zdrop >= 0 && mode->zdrop < (int64_t(1) << 29))
-            throw Failure(DINARA_INVALID_MODE, "a Z-drop on the GPU, which sweeps by rows, not anti-diagonals");
         batch.free_ends = true;
         batch.extension = true;
         batch.from_end = mode->anchor == 1;
+        batch.zdrop = mode->zdrop >= 0 && mode->zdrop < (int64_t(1) << 29) ? mode->zdrop : -1;
+        batch.end_bonus = mode->end_bonus;
         batch.free_reference_start = batch.free_reference_end = batch.free_query_start = batch.free_query_end = 0;
         return false;
     }
@@ -1175,6 +1175,8 @@ void run_scores(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64
     batch.free_query_end = ends.free_query_end;
     batch.extension = ends.extension;
     batch.from_end = ends.from_end;
+    batch.zdrop = ends.zdrop;
+    batch.end_bonus = ends.end_bonus;
     int32_t *scores_device = streamed.scores;
     const auto units = plan_units(pairs, offsets, true, [](int64_t) { return int64_t(0); }, false, 0);
     UnitFinisher finisher(gpu, units.size(), [&](const StagedUnit &unit) {
@@ -1215,38 +1217,11 @@ bool free_end_mode(const dinara_mode *mode) {
            (mode->reference_start | mode->reference_end | mode->query_start | mode->query_end) != 0;
 }
 
-// Scores (and, with `spans`, spans) of a batch under a mode run_scores takes, and for an extension with an
-// end bonus the reference's choice (scoring.mojo:704-710): the extension that reaches the query's far end
-// (from the same anchor, the whole query against the reference whose far end is free) wins when its score
-// plus the bonus passes the best extension's. Without a Z-drop the sweep is never given up, so the bonus
-// always applies.
-void run_placed(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
-                const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores, int64_t *statuses,
-                int64_t *spans) {
-    run_scores(gpu, pairs, letters, offsets, scoring, mode, scores, statuses, spans);
-    if (!mode || mode->kind != DINARA_EXTENSION || mode->end_bonus <= 0 || pairs == 0) return;
-    const bool from_end = mode->anchor == 1;
-    const int64_t unbounded = int64_t(1) << 62;
-    dinara_mode reaching = {DINARA_ENDS_FREE, from_end ? unbounded : 0, from_end ? 0 : unbounded, 0, 0,
-                            mode->match_score, 0, -1, -1};
-    const size_t room = size_t(pairs);
-    std::vector<int32_t> reach_scores(room);
-    std::vector<int64_t> reach_statuses(room), reach_spans(spans ? 4 * room : 0);
-    run_scores(gpu, pairs, letters, offsets, scoring, &reaching, reach_scores.data(), reach_statuses.data(),
-               spans ? reach_spans.data() : nullptr);
-    for (int64_t p = 0; p < pairs; ++p) {
-        // reach + bonus > best, without the sum: the bonus may be near 2^63.
-        if (mode->end_bonus > int64_t(scores[p]) - int64_t(reach_scores[size_t(p)])) {
-            scores[p] = reach_scores[size_t(p)];
-            if (spans) std::memcpy(spans + 4 * p, reach_spans.data() + 4 * p, 4 * sizeof(int64_t));
-        }
-    }
-}
-
 // Alignments with free ends or as extensions under a Scoring, as the reference's host path makes them
-// (scoring.mojo:800-813): each pair's score and span from the free-end or extension sweeps (run_placed),
-// then the span's letters aligned globally (dinara_gpu_alignments_tape), whose CIGAR is the alignment's. A pair whose span's global score
-// differs from its free-end score, or whose span is out of its letters, reports a device failure.
+// (scoring.mojo:800-813): each pair's score and span from the free-end or extension sweeps (run_scores;
+// an extension's Z-drop and end bonus on the device), then the span's letters aligned globally
+// (dinara_gpu_alignments_tape), whose CIGAR is the alignment's. A pair whose span's global score differs
+// from its free-end score, or whose span is out of its letters, reports a device failure.
 void free_end_alignments(dinara_gpu *gpu, int64_t pairs, const char *letters, const int64_t *offsets,
                          const dinara_scoring *scoring, const dinara_mode *mode, int64_t eqx, int32_t *scores,
                          int64_t *spans, int64_t *cigar_offsets, char **cigar_bytes, int64_t *statuses) {
@@ -1254,7 +1229,7 @@ void free_end_alignments(dinara_gpu *gpu, int64_t pairs, const char *letters, co
     std::vector<int64_t> own_spans(spans ? 0 : 4 * room);
     int64_t *placed = spans ? spans : own_spans.data();
     std::vector<int64_t> first_statuses(room, 0);
-    run_placed(gpu, pairs, letters, offsets, scoring, mode, scores, first_statuses.data(), placed);
+    run_scores(gpu, pairs, letters, offsets, scoring, mode, scores, first_statuses.data(), placed);
     // The spans' letters as a tape of their own.
     std::vector<int64_t> inner_offsets(size_t(2 * pairs + 1), 0);
     std::vector<int64_t> failed(room, 0);
@@ -1310,7 +1285,7 @@ int64_t dinara_gpu_scores_tape(dinara_gpu *gpu, int64_t pairs, const char *lette
                                const dinara_scoring *scoring, const dinara_mode *mode, int32_t *scores,
                                int64_t *statuses) {
     return guard(gpu, [&]() -> int64_t {
-        run_placed(gpu, pairs, letters, offsets, scoring, mode, scores, statuses, nullptr);
+        run_scores(gpu, pairs, letters, offsets, scoring, mode, scores, statuses, nullptr);
         return 0;
     });
 }
@@ -1635,8 +1610,6 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         if (!r.scoring) throw Failure(DINARA_INVALID_MODE, "the resident batch was loaded for distances");
         AffineBatch ends;
         const bool local = cigars ? check_mode(mode) : check_scores_mode(mode, ends);
-        if (ends.extension && mode->end_bonus > 0)
-            throw Failure(DINARA_INVALID_MODE, "an extension's end bonus on a resident batch");
         if (r.pairs == 0) return 0;
         DINARA_CUDA(cudaSetDevice(gpu->device));
         Timer timer(gpu);
@@ -1649,6 +1622,8 @@ int64_t dinara_gpu_resident_align(dinara_gpu *gpu, const dinara_mode *mode, int6
         batch.free_query_end = ends.free_query_end;
         batch.extension = ends.extension;
         batch.from_end = ends.from_end;
+        batch.zdrop = ends.zdrop;
+        batch.end_bonus = ends.end_bonus;
         int32_t *scores_device = r.results.ensure<int32_t>(size_t(r.pairs));
         const int64_t *offsets = r.offsets.data();
         if (!cigars) {

@@ -172,7 +172,7 @@ struct dinara_gpu {
     // Outputs and per-launch scratch.
     dinara::DeviceBuffer scores, carry, decisions, decision_offsets, walk_out, cigar_slots, cigar_lengths,
         cigar_offsets, cigar_bytes, spans, wide_pending, narrow_leftovers, record_widths, long_pairs, free_spans,
-        free_scores, walk_order;
+        free_scores, walk_order, reach_scores, reach_spans, diagonals, diagonal_offsets;
     // The host copies of what code_table and table32 hold.
     uint8_t codes_host[256] = {0};
     std::vector<int32_t> table32_host;
@@ -220,7 +220,7 @@ struct dinara_gpu {
             &letters,   &offsets,      &code_table, &tape,          &shapes,        &flags,         &keys,
             &keys_sorted, &order,      &order_sorted, &sort_scratch, &ranges,       &class_counts,  &layouts,
             &leftovers, &decisions_extra, &scores,  &carry,         &decisions,     &decision_offsets, &walk_out,
-            &cigar_slots, &cigar_lengths, &cigar_offsets, &cigar_bytes, &spans,      &wide_pending,  &narrow_leftovers, &record_widths, &long_pairs, &free_spans, &free_scores, &walk_order, &planes,
+            &cigar_slots, &cigar_lengths, &cigar_offsets, &cigar_bytes, &spans,      &wide_pending,  &narrow_leftovers, &record_widths, &long_pairs, &free_spans, &free_scores, &walk_order, &reach_scores, &reach_spans, &diagonals, &diagonal_offsets, &planes,
             &plane_offsets,
             &thresholds, &distances,   &pending,    &pending_next,  &counters,      &table32,       &features,
             &weights,   &gradients,    &optimizer,  &predictions,   &targets,       &activations,   &sketches,

@@ -169,7 +169,7 @@ class Mode:
     def extension(match_score: int, anchor: int = Anchor.START, *, zdrop: int = -1, end_bonus: int = -1) -> "Mode":
         """A seed's extension from both starts (or `anchor` END, both ends), a match earning
         `match_score`. Under a `Scoring` (match score 0: the table's own) the GPU serves it, scores and
-        alignments, with an end bonus; a Z-drop that could stop the sweep it refuses."""
+        alignments, with a Z-drop and an end bonus."""
         return Mode(_EXTENSION, match_score=match_score, anchor=anchor, zdrop=zdrop, end_bonus=end_bonus)
 
     @staticmethod

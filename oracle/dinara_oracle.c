@@ -297,6 +297,83 @@ int32_t oracle_gotoh_extension(const uint8_t *first, int64_t rows, const uint8_t
     return best;
 }
 
+/* An extension with a Z-drop, scored.mojo:272-300 (FROM_ORIGIN in one strip): the anti-diagonals
+ * (row + column) in order, each's best cell (its score; of equal ones the furthest along the reference);
+ * a best above zero at or above the best so far is the new stop, and a best below it ends the sweep when
+ * it lies more than `zdrop` plus `slack` a diagonal between them (each's reference less query letters)
+ * below it. A Z-drop leaves every cell's score as it is, so the scores come from the row sweep and the
+ * anti-diagonals' bests are read after it. *dropped says whether the sweep ended early. */
+int32_t oracle_gotoh_extension_zdrop(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                                     const int8_t *table, int32_t size, int32_t open, int32_t extend, int64_t zdrop,
+                                     int64_t slack, int64_t *end_row, int64_t *end_column, int32_t *dropped) {
+    *end_row = 0;
+    *end_column = 0;
+    *dropped = 0;
+    if (rows == 0 || columns == 0) return 0;
+    const int64_t diagonals = rows + columns + 1;
+    int32_t *most = (int32_t *)malloc((size_t)diagonals * sizeof(int32_t));
+    int64_t *furthest = (int64_t *)malloc((size_t)diagonals * sizeof(int64_t));
+    for (int64_t d = 0; d < diagonals; ++d) {
+        most[d] = INT32_MIN;
+        furthest[d] = 0;
+    }
+    const int32_t opening = open + extend;
+    const int64_t stride = columns + 1;
+    int32_t *s = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *dl = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    int32_t *il = (int32_t *)malloc((size_t)(2 * stride) * sizeof(int32_t));
+    for (int64_t c = 0; c <= columns; ++c) {
+        const int32_t border = c == 0 ? 0 : gap_run(open, extend, c);
+        s[c] = border;
+        dl[c] = border + opening;
+        il[c] = 0;
+    }
+    for (int64_t r = 1; r <= rows; ++r) {
+        int32_t *ps = s + ((r - 1) & 1) * stride, *pd = dl + ((r - 1) & 1) * stride;
+        int32_t *cs = s + (r & 1) * stride, *cd = dl + (r & 1) * stride, *ci = il + (r & 1) * stride;
+        const int32_t border = gap_run(open, extend, r);
+        cs[0] = border;
+        cd[0] = border;
+        ci[0] = border + opening;
+        const int8_t *table_row = table + (int64_t)first[r - 1] * size;
+        for (int64_t c = 1; c <= columns; ++c) {
+            int32_t del = max32(ps[c] + open, pd[c] + extend);
+            int32_t ins = max32(cs[c - 1] + open, ci[c - 1] + extend);
+            cs[c] = max32(ps[c - 1] + table_row[second[c - 1]], max32(del, ins));
+            cd[c] = del;
+            ci[c] = ins;
+            const int64_t d = r + c;
+            if (cs[c] > most[d] || (cs[c] == most[d] && r > furthest[d])) {
+                most[d] = cs[c];
+                furthest[d] = r;
+            }
+        }
+    }
+    int64_t best = 0, best_row = 0, best_diagonal = 0;
+    for (int64_t d = 2; d <= rows + columns; ++d) {
+        if (most[d] > 0 && most[d] >= best) {
+            best = most[d];
+            best_row = furthest[d];
+            best_diagonal = d;
+        } else if (most[d] < best) {
+            const int64_t lean = 2 * furthest[d] - d, best_lean = 2 * best_row - best_diagonal;
+            const int64_t apart = lean > best_lean ? lean - best_lean : best_lean - lean;
+            if (best - most[d] > zdrop + slack * apart) {
+                *dropped = 1;
+                break;
+            }
+        }
+    }
+    *end_row = best_row;
+    *end_column = best_diagonal - best_row;
+    free(most);
+    free(furthest);
+    free(s);
+    free(dl);
+    free(il);
+    return (int32_t)best;
+}
+
 int32_t oracle_gotoh_score_free(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                                 const int8_t *table, int32_t size, int32_t open, int32_t extend,
                                 int64_t reference_start, int64_t reference_end, int64_t query_start,

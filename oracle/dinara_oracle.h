@@ -46,6 +46,11 @@ int32_t oracle_gotoh_end_free(const uint8_t *first, int64_t rows, const uint8_t 
 int32_t oracle_gotoh_extension(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                                const int8_t *table, int32_t size, int32_t open, int32_t extend, int64_t *end_row,
                                int64_t *end_column);
+/* The same with a Z-drop of `zdrop` (and `slack`, the cheapest a gap grows a letter, a diagonal between two
+ * bests), its anti-diagonals read in order (scored.mojo:272-300); *dropped set when the sweep ended early. */
+int32_t oracle_gotoh_extension_zdrop(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
+                                     const int8_t *table, int32_t size, int32_t open, int32_t extend, int64_t zdrop,
+                                     int64_t slack, int64_t *end_row, int64_t *end_column, int32_t *dropped);
 int32_t oracle_gotoh_score(const uint8_t *first, int64_t rows, const uint8_t *second, int64_t columns,
                            const int8_t *table, int32_t size, int32_t open, int32_t extend, int32_t mode,
                            int64_t *end_row, int64_t *end_column);

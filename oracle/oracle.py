@@ -48,6 +48,10 @@ def lib() -> ctypes.CDLL:
         handle.oracle_gotoh_score.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i32, i64p, i64p]
         handle.oracle_gotoh_score_free.restype = i32
         handle.oracle_gotoh_score_free.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64, i64, i64]
+        handle.oracle_gotoh_extension_zdrop.restype = i32
+        handle.oracle_gotoh_extension_zdrop.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, i64, i64,
+                                                        ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                                        ctypes.POINTER(ctypes.c_int32)]
         handle.oracle_gotoh_extension.restype = i32
         handle.oracle_gotoh_extension.argtypes = [u8p, i64, u8p, i64, i8p, i32, i32, i32, ctypes.POINTER(i64),
                                                   ctypes.POINTER(i64)]
@@ -185,22 +189,38 @@ def gotoh_extension(a, b, table, size, open_, extend) -> tuple:
     return int(score), row.value, column.value
 
 
-def extension_alignment(a, b, table, size, open_, extend, from_end=False, end_bonus=-1, eqx=True) -> tuple:
+def gotoh_extension_zdrop(a, b, table, size, open_, extend, zdrop) -> tuple:
+    """(score, stop_row, stop_column, dropped) of an extension from the origin with a Z-drop (scored.mojo:272-300),
+    its slack a diagonal the cheapest a gap grows a letter, -extend."""
+    first, pa = _u8(a)
+    second, pb = _u8(b)
+    t, pt = _i8(table)
+    row, column, dropped = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    score = lib().oracle_gotoh_extension_zdrop(pa, len(first), pb, len(second), pt, size, open_, extend, zdrop,
+                                               -extend, ctypes.byref(row), ctypes.byref(column),
+                                               ctypes.byref(dropped))
+    return int(score), row.value, column.value, bool(dropped.value)
+
+
+def extension_alignment(a, b, table, size, open_, extend, from_end=False, end_bonus=-1, eqx=True,
+                        zdrop=-1) -> tuple:
     """(score, cigar, (reference start, reference end, query start, query end)) of an extension under a
-    Scoring with no Z-drop, as the reference's host path makes it (scoring.mojo:673-722 extension_span and
-    mode_span, 800-813): the best stop from the starts, or from the ends over both sequences reversed; with
-    an end bonus, the alignment reaching the query's far end (free ends: the reference's far end free) when
-    its score plus the bonus passes the stop's; then the span's letters aligned globally."""
+    Scoring, as the reference's host path makes it (scoring.mojo:673-722 extension_span and mode_span,
+    800-813): the best stop from the starts, or from the ends over both sequences reversed, with a Z-drop
+    when `zdrop` is 0 or more; with an end bonus and no drop, the alignment reaching the query's far end
+    (free ends: the reference's far end free) when its score plus the bonus passes the stop's; then the
+    span's letters aligned globally."""
     a = np.asarray(a, dtype=np.uint8)
     b = np.asarray(b, dtype=np.uint8)
     n, m = len(a), len(b)
-    if from_end:
-        score, row, column = gotoh_extension(a[::-1].copy(), b[::-1].copy(), table, size, open_, extend)
-        span = (n - row, n, m - column, m)
+    x, y = (a[::-1].copy(), b[::-1].copy()) if from_end else (a, b)
+    dropped = False
+    if zdrop >= 0:
+        score, row, column, dropped = gotoh_extension_zdrop(x, y, table, size, open_, extend, zdrop)
     else:
-        score, row, column = gotoh_extension(a, b, table, size, open_, extend)
-        span = (0, row, 0, column)
-    if end_bonus > 0:
+        score, row, column = gotoh_extension(x, y, table, size, open_, extend)
+    span = (n - row, n, m - column, m) if from_end else (0, row, 0, column)
+    if end_bonus > 0 and not dropped:
         big = 1 << 62
         counts = (big, 0, 0, 0) if from_end else (0, big, 0, 0)
         reach, _cigar, reach_span = free_ends_alignment(a, b, table, size, open_, extend, *counts, eqx=eqx)

@@ -175,14 +175,54 @@ def test_extensions_against_the_oracle(da, oracle, anchor):
 
 
 def test_extension_refusals(da):
-    """A Z-drop that could stop the sweep needs whole anti-diagonals, which the GPU's row sweep does not
-    take in order, and an extension's match score beside the table's is the reference's own refusal."""
-    with pytest.raises(ValueError):
-        da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(0, zdrop=100))
-    with pytest.raises(ValueError):
-        da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(0, zdrop=0))
+    """An extension's match score beside the table's is the reference's own refusal."""
     with pytest.raises(ValueError):
         da.scores(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(1))
+    with pytest.raises(ValueError):
+        da.alignments(["ACGT"], ["ACG"], da.Scoring.dna(), da.Mode.extension(2, zdrop=5))
+
+
+def _expected_zdrop(oracle, scoring, refs, queries, from_end, bonus, zdrop):
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    size = len(scoring.alphabet)
+    return [oracle.extension_alignment(oracle.codes(r, scoring.alphabet), oracle.codes(q, scoring.alphabet), table,
+                                       size, op, ex, from_end, bonus, zdrop=zdrop) for r, q in zip(refs, queries)]
+
+
+@pytest.mark.parametrize("anchor", ["start", "end"])
+def test_extension_zdrops_against_the_oracle(da, oracle, anchor):
+    """Extensions with Z-drops small enough to end the sweep (0, 5, 20, 60): each anti-diagonal's best kept on
+    the device and read in order, the stop, the span and the CIGAR equal the oracle's, with and without an
+    end bonus (a sweep ended early keeps its stop), on reads that share their anchor with the reference and
+    then run into unrelated letters, under two tables; scores alone agree."""
+    from_end = anchor == "end"
+    rng = np.random.default_rng(131 + from_end)
+    refs, queries = [], []
+    for trial in range(120):
+        n = int(rng.integers(0, 300 if trial % 30 else 1200))
+        ref = "".join(rng.choice(list("ACGT"), size=n))
+        shared = int(rng.integers(0, n + 1))
+        piece = ref[n - shared:] if from_end else ref[:shared]
+        piece = "".join(ch if rng.random() >= 0.04 else rng.choice(list("ACGT")) for ch in piece)
+        tail = "".join(rng.choice(list("ACGT"), size=int(rng.integers(0, 150))))
+        refs.append(ref)
+        queries.append(tail + piece if from_end else piece + tail)
+    refs += ["", "ACGT"]
+    queries += ["ACG", ""]
+    anchor_value = da.Anchor.END if from_end else da.Anchor.START
+    tabulated = da.Scoring.tabulated("ACGT", [5, -1, -2, -1, -1, 5, -3, -2, -2, -3, 5, -1, -1, -2, -1, 5], -6, -1)
+    for scoring in (da.Scoring.dna(), tabulated):
+        for zdrop in (0, 5, 20, 60):
+            for bonus in (-1, 30):
+                mode = da.Mode.extension(0, anchor_value, zdrop=zdrop, end_bonus=bonus)
+                found = da.alignments(refs, queries, scoring, mode)
+                expected = _expected_zdrop(oracle, scoring, refs, queries, from_end, bonus, zdrop)
+                for k, (alignment, (score, cigar, span)) in enumerate(zip(found, expected)):
+                    got = (alignment.score, alignment.cigar, (alignment.reference_start, alignment.reference_end,
+                                                              alignment.query_start, alignment.query_end))
+                    assert got == (score, cigar, span), (k, refs[k], queries[k], zdrop, bonus)
+                assert da.scores(refs, queries, scoring, mode) == [score for score, _c, _s in expected]
 
 
 def test_five_letter_alphabet(da, oracle):

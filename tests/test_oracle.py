@@ -518,3 +518,44 @@ def test_extensions_by_brute_force(oracle):
                     reach, reach_cigar, reach_span = oracle.free_ends_alignment(a, b, table, 4, op, ex, *counts)
                     want = (reach, reach_cigar, reach_span) if reach + bonus > best else (best, cigar, span)
                     assert oracle.extension_alignment(a, b, table, 4, op, ex, from_end, bonus) == want
+
+
+def test_extension_zdrop_by_brute_force(oracle):
+    """An extension's Z-drop against a brute force: every prefix pair scored by its global alignment, each
+    anti-diagonal's best (of equal ones the furthest along the reference), then the anti-diagonals in order
+    as the reference reads them (scored.mojo:272-300): a best above zero at or above the best so far is
+    the stop, one below it by more than the Z-drop plus the gap extension a diagonal apart ends the sweep.
+    A Z-drop of 2^40 never ends it; with an end bonus a dropped sweep keeps its stop."""
+    rng = np.random.default_rng(83)
+    big = 1 << 40
+    for match, mismatch, opening, extension in ((2, -4, -4, -2), (1, -3, -5, -1)):
+        table = oracle.dna_table(match, mismatch)
+        op, ex = oracle.kernel_gaps(opening, extension)
+        for trial in range(40):
+            n, m = int(rng.integers(0, 14)), int(rng.integers(0, 14))
+            a = rng.integers(0, 4, size=n).astype(np.uint8)
+            keep = int(rng.integers(0, n + 1))
+            b = np.concatenate([a[:keep], rng.integers(0, 4, size=max(0, m - keep)).astype(np.uint8)])[:m]
+            for zdrop in (0, 3, 7, big):
+                most, furthest = {}, {}
+                for r in range(1, n + 1):
+                    for c in range(1, len(b) + 1):
+                        value = oracle.gotoh_score(a[:r], b[:c], table, 4, op, ex)[0]
+                        d = r + c
+                        if d not in most or value > most[d] or (value == most[d] and r > furthest[d]):
+                            most[d], furthest[d] = value, r
+                best, best_row, best_d, dropped = 0, 0, 0, False
+                for d in range(2, n + len(b) + 1) if n and len(b) else ():
+                    if most[d] > 0 and most[d] >= best:
+                        best, best_row, best_d = most[d], furthest[d], d
+                    elif most[d] < best:
+                        if best - most[d] > zdrop + (-ex) * abs((2 * furthest[d] - d) - (2 * best_row - best_d)):
+                            dropped = True
+                            break
+                got = oracle.gotoh_extension_zdrop(a, b, table, 4, op, ex, zdrop)
+                assert got == (best, best_row, best_d - best_row, dropped), (a, b, zdrop)
+                if zdrop == big:
+                    assert got[:3] == oracle.gotoh_extension(a, b, table, 4, op, ex)
+                score, _cigar, span = oracle.extension_alignment(a, b, table, 4, op, ex, False, 1 << 61, zdrop=zdrop)
+                if dropped:
+                    assert (score, span) == (best, (0, best_row, 0, best_d - best_row))
