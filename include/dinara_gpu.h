@@ -35,8 +35,8 @@ extern "C" {
 #define DINARA_DEVICE_TIMEOUT (-9)      /* a bounded wait (device flag or host wait) ran out */
 
 /* dinara_mode kinds (c/dinara.h:69-76); under a Scoring the GPU serves ENDS_FREE (global, or with free
- * letters at the ends), EXTENSION (no match score of the mode's own; a Z-drop that could stop the sweep
- * refused, DINARA_INVALID_MODE) and LOCAL. */
+ * letters at the ends), EXTENSION (no match score of the mode's own; either anchor, Z-drop and end bonus)
+ * and LOCAL. */
 #define DINARA_ENDS_FREE 0
 #define DINARA_EXTENSION 1
 #define DINARA_LOCAL 2
