@@ -971,6 +971,32 @@ __global__ void extension_finish_kernel(const PairShape *__restrict__ shapes, in
 // the origin or, read backwards, from the ends; its span runs from its anchor to the stop.
 void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTable &table, int32_t *scores,
                      int64_t first, int64_t count, int64_t *spans) {
+    // A Z-drop keeps rows + columns + 1 words a pair: a range whose words pass the budget goes in halves.
+    constexpr int64_t kDiagonalBudget = int64_t(1) << 28;  // 2 GiB of 8-byte words
+    int64_t *diagonal_counts = nullptr, *diagonal_offsets = nullptr;
+    if (batch.extension && batch.zdrop >= 0) {
+        diagonal_counts = gpu->diagonal_offsets.ensure<int64_t>(2 * (size_t(count) + 1));
+        diagonal_offsets = diagonal_counts + (count + 1);
+        diagonal_counts_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(batch.shapes, first, count,
+                                                                                     diagonal_counts);
+        DINARA_CUDA(cudaGetLastError());
+        gpu->launches += 1;
+        DINARA_CUDA(cudaMemsetAsync(diagonal_counts + count, 0, sizeof(int64_t), gpu->stream));
+        size_t scratch = 0;
+        DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, diagonal_counts, diagonal_offsets, int(count + 1),
+                                                  gpu->stream));
+        void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
+        DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, diagonal_counts, diagonal_offsets, int(count + 1),
+                                                  gpu->stream));
+        int64_t kept = 0;
+        read_back(gpu, &kept, diagonal_offsets + count, sizeof kept);
+        if (kept > kDiagonalBudget && count > 1) {
+            const int64_t half = count / 2;
+            free_end_scores(gpu, batch, table, scores, first, half, spans);
+            free_end_scores(gpu, batch, table, scores, first + half, count - half, spans ? spans + 4 * half : nullptr);
+            return;
+        }
+    }
     // An extension's end bonus weighs the alignment reaching the query's far end (from the same anchor, the
     // whole query against the reference, whose far end is free): its score and span first.
     int32_t *reach_scores = nullptr;
@@ -1025,24 +1051,16 @@ void free_end_scores(dinara_gpu *gpu, const AffineBatch &batch, const AffineTabl
             args.extents = extents;
         }
         if (batch.zdrop >= 0) {
-            // Room for every pair's anti-diagonals, by a scan of their counts, zeroed (below every key).
-            int64_t *counts = gpu->diagonal_offsets.ensure<int64_t>(2 * (size_t(count) + 1));
-            int64_t *offsets = counts + (count + 1);
-            diagonal_counts_kernel<<<unsigned((count + 255) / 256), 256, 0, gpu->stream>>>(batch.shapes, first, count,
-                                                                                         counts);
-            DINARA_CUDA(cudaGetLastError());
-            gpu->launches += 1;
-            DINARA_CUDA(cudaMemsetAsync(counts + count, 0, sizeof(int64_t), gpu->stream));
-            size_t scratch = 0;
-            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scratch, counts, offsets, int(count + 1), gpu->stream));
-            void *space = gpu->sort_scratch.ensure<uint8_t>(scratch + 256);
-            DINARA_CUDA(cub::DeviceScan::ExclusiveSum(space, scratch, counts, offsets, int(count + 1), gpu->stream));
-            int64_t kept = 0;
-            read_back(gpu, &kept, offsets + count, sizeof kept);
+            // Room for every pair's anti-diagonals (their offsets scanned above), zeroed: below every key.
+            const int64_t kept = [&] {
+                int64_t total = 0;
+                read_back(gpu, &total, diagonal_offsets + count, sizeof total);
+                return total;
+            }();
             unsigned long long *diagonals = gpu->diagonals.ensure<unsigned long long>(size_t(kept) + 1);
             DINARA_CUDA(cudaMemsetAsync(diagonals, 0, (size_t(kept) + 1) * sizeof(unsigned long long), gpu->stream));
             args.diagonals = diagonals;
-            args.diagonal_offsets = offsets;
+            args.diagonal_offsets = diagonal_offsets;
         }
     }
     int64_t total = 0;
