@@ -181,3 +181,55 @@ def test_reference_shaped_distances(da, oracle):
     banded = da._native.COptions(-10, 10, -1, 1, 0, 0)
     assert lib.dinara_gpu_distances(context, count - 1, ref_ptrs, ref_lens, q_ptrs, q_lens, None, None,
                                     ctypes.byref(banded), results) == da._native.INVALID_MODE
+
+
+@pytest.mark.parametrize("kind", ["infix", "extension"])
+def test_reference_shaped_free_ends_and_extensions(da, oracle, kind):
+    """The pointer-array entry point (the reference's batch shape) with free ends and with an extension (from
+    the ends, a Z-drop and an end bonus): each alignment's score, span and CIGAR as the oracle places and
+    aligns it, a pair with a letter outside the alphabet refused alone, the CIGARs freed by dinara_free."""
+    lib = da._native.lib()
+    vp, i64, i64p = ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)
+    charpp = ctypes.POINTER(ctypes.c_char_p)
+    lib.dinara_gpu_alignments.restype = i64
+    lib.dinara_gpu_alignments.argtypes = [vp, i64, charpp, i64p, charpp, i64p, ctypes.POINTER(da._native.CScoring),
+                                          ctypes.POINTER(da._native.CMode), i64, ctypes.POINTER(CAlignment), i64p]
+    rng = np.random.default_rng(61 + (kind == "extension"))
+    refs, queries = _reference_batch(rng, 300)
+    count = len(refs)
+    scoring = da.Scoring.dna()
+    mode = da.Mode.INFIX if kind == "infix" else da.Mode.extension(0, da.Anchor.END, zdrop=10, end_bonus=5)
+    struct, _table, _alphabet = scoring._struct()
+    mode_struct = mode._struct()
+    ref_ptrs, ref_lens = _pointer_arrays(refs)
+    q_ptrs, q_lens = _pointer_arrays(queries)
+    context = da._native.context(0)
+    statuses = (ctypes.c_int64 * count)()
+    alignments = (CAlignment * count)()
+    code = lib.dinara_gpu_alignments(context, count, ref_ptrs, ref_lens, q_ptrs, q_lens, ctypes.byref(struct),
+                                     ctypes.byref(mode_struct), 1, alignments, statuses)
+    assert code == 0
+    refused = count - 3
+    assert statuses[refused] == da._native.UNSUPPORTED_SYMBOLS and not alignments[refused].cigar
+    table = np.asarray(scoring.table, dtype=np.int8)
+    op, ex = oracle.kernel_gaps(scoring.opening, scoring.extension)
+    big = 1 << 40
+    try:
+        for k in range(count):
+            if k == refused:
+                continue
+            assert statuses[k] == 0
+            a, b = oracle.codes(refs[k]), oracle.codes(queries[k])
+            if kind == "infix":
+                want = oracle.free_ends_alignment(a, b, table, 4, op, ex, big, big, 0, 0)
+            else:
+                want = oracle.extension_alignment(a, b, table, 4, op, ex, True, 5, zdrop=10)
+            got = alignments[k]
+            cigar = ctypes.string_at(got.cigar, got.cigar_length).decode() if got.cigar_length else ""
+            assert (got.score, cigar, (got.reference_start, got.reference_end, got.query_start, got.query_end)) == (
+                want[0], want[1], want[2]), k
+            assert got.cost == -got.score
+    finally:
+        for k in range(count):
+            if alignments[k].cigar:
+                lib.dinara_free(alignments[k].cigar)
