@@ -5,7 +5,7 @@ log-uniform 100 bp-20 kbp, per-pair error rate uniform 0.5-15% (substitutions/in
 50/25/25), global unit-cost edit distances by band doubling. The learned band (a 258-64-64-1 network over
 4-mer count differences and a 6-mer sketch, trained first on the GPU on 1,000,000 pairs of the same distribution, whose exact
 distances plain band doubling measures) sets each pair's first threshold; plain band doubling from the
-default band is run beside it as the judge, and both must give the same distance on every pair.
+default band is run beside it as the check, and both must give the same distance on every pair.
 
 A step is one pass of the path over the batch with the letters resident in HBM (`value`, device time on
 the context's stream); `e2e` times the same batch through the library's public call from page-locked host
