@@ -398,18 +398,25 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
     from dinara_align import learned, tuning
 
     placement = da.Placement.on_gpu(ranks.local_rank)
-    # The band autotuner first: both arms then sweep with the shapes it measured, and the predictor's
-    # margins are calibrated against the windows those shapes give.
+    # The band autotuner first: both arms then sweep with the shapes it measured, each with the chain bound
+    # it measured fastest for that arm's starts (plain doubling's, or near each distance as a learned start
+    # is), and the predictor's margins are calibrated against the windows the learned arm's tuning gives.
     tuning_file = ctx.get("tuning", "")
     if tuning_file and os.path.exists(tuning_file):
-        tuning.load(tuning_file, placement)
-        kept = tuning.tuning(placement)
-        tuned = {"chain_words": kept["chain_words"], "chain_share": kept["chain_share"], "chain_ms": {},
-                 "seconds": 0.0, "words_per_ms": {}, "loaded": tuning_file}
+        with open(tuning_file) as source:
+            kept = json.load(source)
+        arm_tunings = kept if "learned" in kept else {"learned": kept, "plain": kept}
+        tuned = {"chain_words": arm_tunings["learned"]["chain_words"], "chain_share": arm_tunings["learned"]["chain_share"],
+                 "chain_ms": {}, "seconds": 0.0, "words_per_ms": {}, "loaded": tuning_file}
     else:
         tuned = tuning.autotune(placement, pairs=tape.pairs)
+        measured = tuning.tuning(placement)
+        arm_tunings = {"learned": tuning.tuning_for_starts(tuned, measured, near=True),
+                       "plain": tuning.tuning_for_starts(tuned, measured, near=False)}
         if tuning_file:
-            tuning.save(tuning_file, placement)
+            with open(tuning_file, "w") as out_file:
+                json.dump(arm_tunings, out_file)
+    tuning.install(arm_tunings["learned"], placement)
     predictor = learned.Predictor(placement)
     blob = ctx.get("predictor", "")
     if blob and os.path.exists(blob):
@@ -439,6 +446,7 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
     arms = [(name, policy) for name, policy in (("learned", native.BAND_LEARNED), ("plain", native.BAND_PLAIN))
             if ctx.get("arms", "both") in ("both", name)]
     for name, policy in arms:
+        tuning.install(arm_tunings[name], placement)
         timings, begin, end = timed_steps(stepper(policy, name), steps, warmup, ranks)
         device_ms = ranks.max(sum(t.total_ms for t in timings))
         result = np.zeros(tape.pairs, dtype=np.int64)
@@ -451,6 +459,7 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
                      "band_ms_per_step": sum(t.class_ms[CLASS_UNIT_BAND] for t in timings) / steps,
                      "predict_ms_per_step": sum(t.class_ms[CLASS_PREDICT] for t in timings) / steps,
                      "report": reports[name], "timed_region": [begin, end]}
+    tuning.install(arm_tunings["learned"], placement)  # the end-to-end calls run the learned band
     if len(out) == 1:
         # One arm alone (a profiling run): its own figures, no comparison.
         (name, only), = out.items()
@@ -466,7 +475,9 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
             "gcups": out["learned"]["gcups_full_matrix"], "plain_gcups": out["plain"]["gcups_full_matrix"],
             "learned": out["learned"], "plain": out["plain"], "training": training,
             "autotune": {"chain_words": tuned["chain_words"], "chain_share": tuned["chain_share"],
-                         "chain_ms": tuned["chain_ms"],
+                         "chain_ms": tuned["chain_ms"], "chain_ms_near": tuned.get("chain_ms_near", {}),
+                         "learned_chain": {k: arm_tunings["learned"][k] for k in ("chain_words", "chain_share", "reach")},
+                         "plain_chain": {k: arm_tunings["plain"][k] for k in ("chain_words", "chain_share", "reach")},
                          "seconds": tuned["seconds"], "words_per_ms": tuned["words_per_ms"]}}
     # The dominant kernel: every round's band kernels. A Myers/Hyyro word step is about 20 u64 operations
     # (bit_parallel.mojo:10-11), 40 in int32 terms, over the words the rounds swept.

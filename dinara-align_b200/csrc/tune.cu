@@ -129,6 +129,7 @@ void band_autotune(dinara_gpu *gpu, const dinara_band_tune_options &options, din
                 if (repeat == 0 || band.kernel_ms < fastest_run) fastest_run = band.kernel_ms;
             }
             total += fastest_run;
+            if (start) out.chain_ms_near[c] = fastest_run;
         }
         out.chain_words_tried[c] = kFloorCandidates[c];
         out.chain_share_tried[c] = kShareCandidates[c];

@@ -26,7 +26,8 @@ class TuneReport(ctypes.Structure):
                 ("chain_tried", ctypes.c_int64), ("chain_words_tried", ctypes.c_int64 * 8),
                 ("chain_share_tried", ctypes.c_double * 8), ("reach_tried", ctypes.c_int64 * 8),
                 ("chain_ms", ctypes.c_double * 8), ("chain_words", ctypes.c_int64), ("chain_share", ctypes.c_double),
-                ("reach", ctypes.c_int64), ("full_grids", ctypes.c_int64), ("seconds", ctypes.c_double)]
+                ("reach", ctypes.c_int64), ("full_grids", ctypes.c_int64), ("seconds", ctypes.c_double),
+                ("chain_ms_near", ctypes.c_double * 8)]
 
 
 class Tuning(ctypes.Structure):
@@ -62,12 +63,24 @@ def autotune(placement: Placement | None = None, *, pairs: int = 50_000, length=
     report = TuneReport()
     native.check(lib.dinara_gpu_band_autotune(handle, ctypes.byref(options), ctypes.byref(report)), handle)
     rates = {f"{g}x{k}": report.words_per_ms[s] for s in range(report.shapes) for g, k in [shape_of(s)]}
-    # Keyed "floor/share/reach": the device time of plain doubling and of near starts together.
-    chains = {f"{report.chain_words_tried[c]}/{report.chain_share_tried[c]:g}/{report.reach_tried[c]}":
-              report.chain_ms[c] for c in range(report.chain_tried)}
-    return {"words_per_ms": rates, "chain_ms": chains, "chain_words": int(report.chain_words),
+    # Keyed "floor/share/reach": the device time of plain doubling and of near starts together, and the near
+    # starts' part alone (first thresholds near each distance, as a learned start gives them).
+    keys = [f"{report.chain_words_tried[c]}/{report.chain_share_tried[c]:g}/{report.reach_tried[c]}"
+            for c in range(report.chain_tried)]
+    chains = {key: report.chain_ms[c] for c, key in enumerate(keys)}
+    near = {key: report.chain_ms_near[c] for c, key in enumerate(keys)}
+    return {"words_per_ms": rates, "chain_ms": chains, "chain_ms_near": near, "chain_words": int(report.chain_words),
             "chain_share": report.chain_share, "reach": int(report.reach), "full_grids": int(report.full_grids),
             "seconds": report.seconds}
+
+
+def tuning_for_starts(report: dict, values: dict, near: bool) -> dict:
+    """The tuning `values` (as `tuning()` returns it) with the chain bound an autotune `report` measured
+    fastest for near starts (a learned start's rounds) or, without `near`, for plain doubling's."""
+    times = {key: (report["chain_ms_near"][key] if near else report["chain_ms"][key] - report["chain_ms_near"][key])
+             for key in report["chain_ms"]}
+    floor, share, reach = min(times, key=times.get).split("/")
+    return dict(values, chain_words=int(floor), chain_share=float(share), reach=int(reach))
 
 
 def tuning(placement: Placement | None = None) -> dict:

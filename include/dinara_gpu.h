@@ -263,6 +263,7 @@ typedef struct {
     int64_t reach;                   /* the reach chosen */
     int64_t full_grids;              /* 1 when the chosen launches each fill the GPU, 0 when they share it */
     double seconds;                  /* wall time of the whole tuning */
+    double chain_ms_near[8];         /* of chain_ms, the near starts' part (the rest is plain doubling's) */
 } dinara_band_tune_report;
 
 /* Measures and installs the context's band tuning; `options` may be null for the defaults. */
