@@ -76,3 +76,18 @@ def test_band_tuning_needs_a_context():
     assert handle.dinara_gpu_band_tuning(None, 0, values) == -6
     handle.dinara_gpu_band_autotune.restype = ctypes.c_int64
     assert handle.dinara_gpu_band_autotune(None, None, None) == -6
+
+
+def test_tuning_for_each_start():
+    """An autotune report's per-candidate times split into plain doubling's and the near starts' parts: each
+    start takes the bound fastest for it, the measured word costs and grid scheme kept."""
+    from dinara_align import tuning
+
+    report = {"chain_ms": {"24000/0/5": 120.0, "48000/0/5": 113.0, "24000/1/8": 118.0},
+              "chain_ms_near": {"24000/0/5": 41.5, "48000/0/5": 40.6, "24000/1/8": 48.2}}
+    values = {"chain_words": 48000, "chain_share": 0.0, "reach": 5, "full_grids": 0, "word_costs": [40.0] * 39}
+    near = tuning.tuning_for_starts(report, values, near=True)
+    plain = tuning.tuning_for_starts(report, values, near=False)
+    assert (near["chain_words"], near["chain_share"], near["reach"]) == (48000, 0.0, 5)
+    assert (plain["chain_words"], plain["chain_share"], plain["reach"]) == (24000, 1.0, 8)
+    assert plain["word_costs"] == values["word_costs"] and plain["full_grids"] == 0
