@@ -3,9 +3,10 @@
 Headline workload (default `uneven`, the metric's own comparison): 200,000 synthetic pairs, lengths
 log-uniform 100 bp-20 kbp, per-pair error rate uniform 0.5-15% (substitutions/insertions/deletions
 50/25/25), global unit-cost edit distances by band doubling. The learned band (a 258-64-64-1 network over
-4-mer count differences and a 6-mer sketch, trained first on the GPU on 1,000,000 pairs of the same distribution, whose exact
-distances plain band doubling measures) sets each pair's first threshold; plain band doubling from the
-default band is run beside it as the check, and both must give the same distance on every pair.
+4-mer count differences and a 6-mer sketch, trained first on the GPU on 1,000,000 pairs of the same
+distribution, whose exact distances plain band doubling measures) sets each pair's first threshold; plain
+band doubling from the default band is run beside it as the check, and both must give the same distance on
+every pair. Each arm sweeps with the band tuning's chain bound measured fastest for its own starts.
 
 A step is one pass of the path over the batch with the letters resident in HBM (`value`, device time on
 the context's stream); `e2e` times the same batch through the library's public call from page-locked host
@@ -47,6 +48,9 @@ WORKLOADS = {
              "8% errors 50/25/25",
     "unit250": "global unit-cost distances, 10,000 pairs of 250 bp, 2% errors in thirds",
 }
+
+# The band tuning's chain bound, as the bench reports each arm's.
+CHAIN_KEYS = ("chain_words", "chain_share", "reach")
 
 # The host work the CPU legs sample, sized for roughly 10-30 s of CPU work on a 16-core host.
 CPU_SAMPLE = {"uneven": 40_000, "affine": 400_000, "local": 20_000, "unit250": 10_000}
@@ -406,7 +410,8 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
         with open(tuning_file) as source:
             kept = json.load(source)
         arm_tunings = kept if "learned" in kept else {"learned": kept, "plain": kept}
-        tuned = {"chain_words": arm_tunings["learned"]["chain_words"], "chain_share": arm_tunings["learned"]["chain_share"],
+        learned_tuning = arm_tunings["learned"]
+        tuned = {"chain_words": learned_tuning["chain_words"], "chain_share": learned_tuning["chain_share"],
                  "chain_ms": {}, "seconds": 0.0, "words_per_ms": {}, "loaded": tuning_file}
     else:
         tuned = tuning.autotune(placement, pairs=tape.pairs)
@@ -476,8 +481,8 @@ def run_uneven(ctx, tape, steps, warmup) -> dict:
             "learned": out["learned"], "plain": out["plain"], "training": training,
             "autotune": {"chain_words": tuned["chain_words"], "chain_share": tuned["chain_share"],
                          "chain_ms": tuned["chain_ms"], "chain_ms_near": tuned.get("chain_ms_near", {}),
-                         "learned_chain": {k: arm_tunings["learned"][k] for k in ("chain_words", "chain_share", "reach")},
-                         "plain_chain": {k: arm_tunings["plain"][k] for k in ("chain_words", "chain_share", "reach")},
+                         "learned_chain": {k: arm_tunings["learned"][k] for k in CHAIN_KEYS},
+                         "plain_chain": {k: arm_tunings["plain"][k] for k in CHAIN_KEYS},
                          "seconds": tuned["seconds"], "words_per_ms": tuned["words_per_ms"]}}
     # The dominant kernel: every round's band kernels. A Myers/Hyyro word step is about 20 u64 operations
     # (bit_parallel.mojo:10-11), 40 in int32 terms, over the words the rounds swept.
